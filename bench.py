@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Benchmark of the plain LBVH build on B200: Mprims/s and fraction of the HBM roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload clustered16M|sphere2M|uniform64K]
+
+One step = one complete build (scene box, Morton keys, 4-pass onesweep sort, Karras tree,
+refit + rearrange) of the workload's triangle soup.  Default workload: the 16,777,216-triangle
+Gaussian-mixture scene (seeded synthetic data; the reference publishes no scene set).  The
+805 MB input soup is larger than the 126 MB L2, so steps run back to back without a flush.
+
+Prints one JSON line (rank 0).  Fields beyond the base contract:
+  roofline      dominant kernel's algorithmic bytes / its CUDA-event duration vs measured HBM
+  stage_ms      per-stage device times (CUDA events on the build stream, profiled steps)
+  cpu_baseline  the CPU restatement of the reference build timed on this host's cores
+  e2e           through the public C ABI from pinned host memory: H2D of the soup, the build,
+                D2H of the root node record, every step
+Under torchrun (N > 1) each rank builds its own replica (the build has no shardable exchange).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "webgpu-lvbh-demo_b200")
+for _p in (REPO, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "LBVH build Mprims/s"
+UNIT = "Mprims/s"
+
+# Algorithmic HBM bytes per triangle of each stage (fixed traffic model): bounds read 48;
+# Morton read 48 + key 4; sort 48 (3 LSD passes of 30-bit keys: histogram read 4, pass 1 read 4
+# write 8, passes 2-3 read 8 write 8); tree keys 4 + parents 8 + child links 8; refit +
+# rearrange perm 4 + gather 48 + write 48 + node words 56 + parent reads 8 + flag atomics 8.
+MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "tree": 20, "refit": 172}
+MODEL_TOTAL = sum(MODEL_BYTES.values())  # 340 B per triangle
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_workload(name: str):
+    from lvbh import scenes
+    if name == "clustered16M":
+        return scenes.clustered_soup(1 << 24, seed=2), "clustered_soup_16M"
+    if name == "sphere2M":
+        return scenes.sphere_mesh(1024, seed=1), "sphere_mesh_2M"
+    if name == "uniform64K":
+        return scenes.uniform_soup(65_536, seed=0), "uniform_soup_64K"
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    """Largest value of x over all ranks (the slowest rank's time)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(tri, bounds=None):
+    """The oracle (CPU restatement of the reference build) on all host cores."""
+    import oracle
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    oracle.build(tri, bounds, threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": tri.shape[0] / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"one full build of the {tri.shape[0]:,}-triangle workload "
+                      f"({dt:.2f} s wall, OpenMP over {cores} threads)"}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the CPU restatement of the reference's build, each step a bounded
+    sample (the first 2^22 triangles) of the workload, all host threads."""
+    if rank != 0:
+        return
+    import oracle
+    tri, wname = make_workload(args.workload)
+    sample = tri[: min(tri.shape[0], 1 << 22)]
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.build(sample, None, threads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.build(sample, None, threads=cores)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = sample.shape[0] / dt / 1e6
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/u32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": wname, "num_tris": int(tri.shape[0]), "parallelism": "replicas",
+                       "bounds": "reduced over all vertices"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"first {sample.shape[0]:,} triangles of the workload per step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's WGSL build needs browser WebGPU (unavailable on this box); "
+                    "this arm times its C++ restatement, which produces the same output"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import lvbh
+    from lvbh import empty_outputs
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    tri, wname = make_workload(args.workload)
+    n = tri.shape[0]
+    builder = lvbh.BVHBuilder(local, reserve_tris=n)
+    stream = torch.cuda.Stream(dev)
+    dtri = torch.from_numpy(tri).to(dev)
+    outs = empty_outputs(n, dev)
+    peak, peak_kind = load_peaks()
+
+    def step(profile=False, sync=False):
+        return builder.build_soup(dtri, None, outputs=outs, stream=stream, sync=sync, profile=profile)
+
+    # warm-up (graph capture happens on the first call)
+    for _ in range(args.warmup):
+        step(sync=True)
+    torch.cuda.synchronize(dev)
+
+    # timed region: K graph-replayed builds back to back on `stream`
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step(sync=False)
+        ev1.record(stream)
+        builder.sync()
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ms, world)
+    value = world * n / (ms * 1e-3) / 1e6
+
+    # per-stage CUDA events on the build stream, K profiled builds
+    stages = {k: [] for k in lvbh.STAGE_NAMES}
+    for _ in range(args.steps):
+        res = step(profile=True, sync=True)
+        for k, v in res.stage_ms.items():
+            stages[k].append(v)
+    stage_ms = {k: statistics.mean(v) for k, v in stages.items() if k != "upload"}
+    dom = max(("bounds", "morton", "sort", "tree", "refit"), key=lambda k: stage_ms[k])
+    dom_bytes = MODEL_BYTES[dom] * n
+    achieved = dom_bytes / (stage_ms[dom] * 1e-3) / 1e9
+    traffic = load_traffic(dom, n)
+    roofline = {"bound": "hbm", "kernel": {"refit": "k_refit", "sort": "k_onesweep x4",
+                                          "morton": "k_morton", "bounds": "k_bounds",
+                                          "tree": "k_tree"}[dom],
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes": dom_bytes,
+                "whole_build": {"model_bytes_per_tri": MODEL_TOTAL,
+                                "achieved_gbs": MODEL_TOTAL * n / (ms * 1e-3) / 1e9,
+                                "frac_of_measured": MODEL_TOTAL * n / (ms * 1e-3) / 1e9 / peak,
+                                "frac_of_8tbs": MODEL_TOTAL * n / (ms * 1e-3) / 1e9 / 8000.0}}
+
+    # end to end through the public API from pinned host memory
+    htri = torch.from_numpy(tri).pin_memory()
+    hroot = torch.empty(16, dtype=torch.int32).pin_memory()
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        builder.build_soup(htri.numpy(), None, outputs=outs, stream=stream, sync=True)
+        with torch.cuda.stream(stream):
+            hroot.copy_(outs["nodes"][0], non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e = max_over_ranks(statistics.mean(e2e_ms), world)
+    e2e_line = {"value": world * n / (e2e * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": e2e,
+                "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 64}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(tri)
+
+    builder.close()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32/u32", "data": "synthetic",
+            "config": {"workload": wname, "num_tris": n, "parallelism": "replicas" if world > 1 else "single",
+                       "bounds": "reduced on the device over all vertices",
+                       "l2": "input soup 805 MB > 126 MB L2; no flush", "graph": True},
+            "gpu_launches": 8 * args.steps,
+            "roofline": roofline, "stage_ms": stage_ms, "cpu_baseline": cpu, "e2e": e2e_line,
+            "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def load_traffic(stage: str, n: int):
+    """dram read+write bytes per launch of the stage's kernel from the committed ncu summary
+    (profiles/traffic.json, scaled to n triangles), or None."""
+    try:
+        with open(os.path.join(REPO, "profiles", "traffic.json")) as f:
+            t = json.load(f)[stage]
+        return t["bytes_per_tri"] * n
+    except Exception:
+        return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="clustered16M")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,171 @@
+/*
+ * lvbh.h - C ABI of the B200 (sm_100a) LBVH builder.
+ *
+ * This library is a drop-in for the BVH build path of AddisonPrairie/WebGPU-LVBH-demo:
+ *
+ *   initBVHBuild(device) -> { build }                        scripts/bvh/build-bvh.js:1-10
+ *   async build(TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS)
+ *       -> { BVH_BUFFER, O_TRIANGLE_BUFFER }                 scripts/bvh/build-bvh.js:12-66
+ *
+ * Every entry point takes plain pointers and sizes; no C++ or framework type crosses
+ * the boundary, and no exception escapes it.  Status codes replace the reference's
+ * `console.warn(...); return undefined` (scripts/bvh/kernels/aabb-z-idx.js:58-61,
+ * radix-tree.js:51-54, rearrange.js:58-66).
+ *
+ * Layouts (identical to what scripts/pathtracer/pathtracer.js:441-459 traverses):
+ *
+ *   Triangle (input and output), 48 B:  float v0[3], pad, v1[3], pad, v2[3], pad
+ *        (WGSL vec3f members at 16-byte alignment, scripts/bvh/kernels/aabb-z-idx.js:153-157;
+ *         pad words are ignored on input and copied unchanged into the output).
+ *
+ *   BVHNode, 64 B (scripts/bvh/kernels/bvh-up-pass.js:161-178):
+ *        word  0- 2  left  box min      word  3  l_child
+ *        word  4- 6  left  box max      word  7  f_1
+ *        word  8-10  right box min      word 11  r_child
+ *        word 12-14  right box max      word 15  f_2
+ *     A child >= 0 is an internal node index; a child < 0 is the leaf -(sorted_pos + 1),
+ *     i.e. triangle `sorted_pos` of the output triangle buffer.  Node 0 is the root.  The
+ *     buffer holds N records and record N-1 is all zero, as in the reference.
+ *     Canonical form: the left slot holds the Karras left child (the lower key range),
+ *     f_1 = 2 and f_2 = 0 for every internal node (f_1 = 1 for the single node of an N = 1
+ *     build).  The reference fills the slots in arrival order and leaves an arrival/spin
+ *     count in f_1; a tree of it equals this one after sorting each node's two slots by
+ *     child range and masking words 7 and 15.
+ *
+ *   parents, int32 x 2N (scripts/bvh/kernels/radix-tree.js:57-60,146-156):
+ *        [0, N-2]  parent of internal node i      [N, 2N-1]  parent of leaf (sorted pos) i-N
+ *        slots 0 and N-1 hold 0.
+ *   leaf_index, uint32 x N: sorted position -> input triangle index (the reference's IDX_BUFFER).
+ *   morton, uint32 x N: the sorted Morton keys (the reference's Z_IDX_BUFFER after the sort).
+ *
+ * Memory: all result buffers are device memory of the context's device.  Input may be host
+ * or device memory (LVBH_INPUT_HOST).
+ */
+#ifndef LVBH_H
+#define LVBH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LVBH_API __attribute__((visibility("default")))
+#else
+#define LVBH_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define LVBH_OK        0
+#define LVBH_EINVAL    1  /* bad argument: NULL pointer, size out of range, non-finite vertex */
+#define LVBH_ENOMEM    2  /* device or pinned allocation failed, or the memory budget is exceeded */
+#define LVBH_ETIMEOUT  3  /* a device-side wait gave up after its bound (error word set by a kernel) */
+#define LVBH_ECUDA     4  /* a CUDA runtime call failed; lvbh_last_error() has the text */
+#define LVBH_EBUSY     5  /* serving: queue full / request not finished yet */
+#define LVBH_EDEVICE   6  /* a kernel reported an inconsistent structure (bounded climb exceeded) */
+
+/* ---- build flags ------------------------------------------------------------------- */
+#define LVBH_INPUT_HOST    0x1u  /* input pointers are host memory: copied to the device inside the call */
+#define LVBH_ASYNC         0x2u  /* return after enqueueing; call lvbh_sync() before reading results/status */
+#define LVBH_OUT_CALLER    0x4u  /* result pointers in *out are caller-owned device buffers to fill */
+#define LVBH_PROFILE       0x8u  /* record per-stage CUDA events; read them with lvbh_stage_times() */
+#define LVBH_NO_GRAPH      0x10u /* launch stage by stage instead of replaying a cached CUDA graph */
+
+/* Largest triangle count one build accepts (2^29: keeps every index sum of the tree search
+ * inside int32 and the look-back counts inside their 30-bit field; a build this size needs
+ * about 100 GB of device memory). */
+#define LVBH_MAX_TRIS  ((uint32_t)1 << 29)
+
+/* Stage indices for lvbh_stage_times(). */
+#define LVBH_STAGE_UPLOAD  0  /* host->device copy of the input (LVBH_INPUT_HOST only) */
+#define LVBH_STAGE_BOUNDS  1  /* scene box reduction (skipped when bounds are supplied) */
+#define LVBH_STAGE_MORTON  2  /* triangle centroid -> 30-bit Morton key + digit histograms */
+#define LVBH_STAGE_SORT    3  /* onesweep stable radix sort of (key, triangle index) */
+#define LVBH_STAGE_TREE    4  /* Karras radix tree -> parent links */
+#define LVBH_STAGE_REFIT   5  /* leaf gather + triangle rearrange + bottom-up box refit */
+#define LVBH_NUM_STAGES    6
+
+typedef struct lvbh_ctx lvbh_ctx;
+
+typedef struct lvbh_config {
+    int      device;        /* CUDA device ordinal; -1 = the calling thread's current device */
+    uint32_t reserve_tris;  /* pre-size the scratch arena for this many triangles (0 = on demand) */
+    uint64_t reserved[4];   /* must be zero */
+} lvbh_config;
+
+typedef struct lvbh_result {
+    uint32_t  num_tris;     /* N */
+    uint32_t  num_nodes;    /* N: BVHNode records in `nodes` (record N-1 is zero) */
+    void     *nodes;        /* BVH_BUFFER: 64 B x N */
+    void     *tris;         /* O_TRIANGLE_BUFFER: 48 B x N, sorted order */
+    int32_t  *parents;      /* 2N */
+    uint32_t *leaf_index;   /* N */
+    uint32_t *morton;       /* N */
+    float     bounds[6];    /* scene min xyz, max xyz used for quantisation (filled at sync) */
+    uint32_t  owned;        /* 1 when the library allocated the buffers (free with lvbh_release) */
+} lvbh_result;
+
+/* Replaces initBVHBuild(device) (scripts/bvh/build-bvh.js:1-10): binds a context to a device.
+ * `cfg` may be NULL (current device, no reservation). */
+LVBH_API int  lvbh_create(lvbh_ctx **ctx, const lvbh_config *cfg);
+/* Frees the context and its scratch arena.  Results it allocated stay valid until released. */
+LVBH_API void lvbh_destroy(lvbh_ctx *ctx);
+
+/* Replaces build(TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS) (scripts/bvh/build-bvh.js:12-66).
+ *   tri_array    12 floats per triangle (48 B stride), host memory when LVBH_INPUT_HOST is set.
+ *   num_tris     N; 0 gives an empty result, as in the reference.
+ *   model_bounds 6 host floats {min x,y,z, max x,y,z} used for quantisation exactly as the
+ *                reference's uniform (aabb-z-idx.js:113-132); NULL = reduce min/max over all
+ *                vertices on the device (what parse-obj.js:27-53 computes on the host).
+ *   flags        LVBH_* build flags.
+ *   out          receives the result.  Without LVBH_OUT_CALLER the library allocates the
+ *                buffers (stream-ordered) and the caller frees them with lvbh_release().
+ *   stream       cudaStream_t to run on (NULL = the legacy default stream).
+ * Synchronous unless LVBH_ASYNC: the call returns once results are ready and device-side
+ * checks (non-finite input, bounded waits) have been read back. */
+LVBH_API int  lvbh_build_soup(lvbh_ctx *ctx, const float *tri_array, uint32_t num_tris,
+                     const float *model_bounds, uint32_t flags, lvbh_result *out, void *stream);
+
+/* Indexed-mesh form of lvbh_build_soup (vertex and index buffers in): vertices are packed
+ * float3 (12 B), indices are uint32 triples.  The triangles are gathered on the
+ * device into the same 48 B layout (pad words = 0), then built exactly as lvbh_build_soup. */
+LVBH_API int  lvbh_build_indexed(lvbh_ctx *ctx, const float *xyz, uint32_t num_verts,
+                        const uint32_t *idx3, uint32_t num_tris, const float *model_bounds,
+                        uint32_t flags, lvbh_result *out, void *stream);
+
+/* Waits for the context's last build and returns its device-side status (LVBH_OK,
+ * LVBH_EINVAL for non-finite vertices, LVBH_ETIMEOUT, LVBH_EDEVICE).  Fills out->bounds
+ * of the result passed to that build when it is still reachable. */
+LVBH_API int  lvbh_sync(lvbh_ctx *ctx);
+
+/* Frees library-allocated result buffers (no-op for LVBH_OUT_CALLER results). */
+LVBH_API int  lvbh_release(lvbh_ctx *ctx, lvbh_result *res);
+
+/* Per-stage device times (ms) of the last build made with LVBH_PROFILE, LVBH_NUM_STAGES
+ * entries, after lvbh_sync(). */
+LVBH_API int  lvbh_stage_times(lvbh_ctx *ctx, float *ms_out);
+
+/* Bytes of device scratch a build of `num_tris` triangles needs beyond its inputs/outputs. */
+LVBH_API size_t lvbh_scratch_bytes(uint32_t num_tris);
+
+/* Text of the last error on this context (never NULL). */
+LVBH_API const char *lvbh_last_error(const lvbh_ctx *ctx);
+/* Library version string. */
+LVBH_API const char *lvbh_version(void);
+
+/* ---- validation consumer: closest-hit traversal ------------------------------------
+ * Restates intersect_bvh / aabb_intersect / tri_intersect of scripts/pathtracer/pathtracer.js
+ * (:495-584, :621-628, :587-619) over a built tree and returns per ray the hit triangle's
+ * sorted position (-1 = miss), the hit distance t (-1 = miss, as the reference returns) and
+ * the deepest stack the ray used.  rays: 8 floats per ray {ox,oy,oz,pad,dx,dy,dz,pad},
+ * device memory. */
+LVBH_API int  lvbh_trace(lvbh_ctx *ctx, const void *nodes, const void *tris, uint32_t num_tris,
+                const float *rays, uint32_t num_rays, int32_t *hit_prim, float *hit_t,
+                uint32_t *max_stack, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LVBH_H */

@@ -1,0 +1,157 @@
+"""CPU oracle for the LBVH build - TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper over oracle/liblvbh_oracle.so, the C++ restatement of the reference's WGSL
+build (scripts/bvh/kernels/*.js) and traversal (scripts/pathtracer/pathtracer.js).  Only the
+tests, the smoke check and the benchmark's CPU-baseline / reference arm use it, as the
+checker; the product library never does.
+
+Parity status: unpinned against a run of the reference (it has no tests or golden vectors
+and cannot run here); cross-checked against the literal WGSL simulation in
+tests/golden/make_golden.py and its committed fixtures.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liblvbh_oracle.so")
+_lib = None
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def build_lib() -> str:
+    """Compile the oracle (make -C oracle)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(_HERE, "lvbh_oracle.cpp")
+        if not os.path.exists(_LIB_PATH) or (
+                os.path.exists(src) and os.path.getmtime(src) > os.path.getmtime(_LIB_PATH)):
+            build_lib()
+        L = ctypes.CDLL(_LIB_PATH)
+        vp = ctypes.c_void_p
+        u32 = ctypes.c_uint32
+        L.oracle_scene_bounds.argtypes = [_f32p, u32, _f32p]
+        L.oracle_aabb_zidx.argtypes = [_f32p, u32, _f32p, vp, _u32p, ctypes.c_int]
+        L.oracle_radix_sort.argtypes = [_u32p, u32, _i32p, ctypes.c_int]
+        L.oracle_radix_tree.argtypes = [_u32p, u32, _i32p, ctypes.c_int]
+        L.oracle_up_pass.argtypes = [_i32p, _f32p, _i32p, u32, _u32p, ctypes.c_int]
+        L.oracle_canonicalize.argtypes = [_u32p, u32]
+        L.oracle_rearrange.argtypes = [_f32p, _i32p, u32, _f32p, ctypes.c_int]
+        L.oracle_gather_indexed.argtypes = [_f32p, _u32p, u32, _f32p]
+        L.oracle_build.argtypes = [_f32p, u32, vp, ctypes.c_int, vp, vp, vp, vp, vp, vp]
+        L.oracle_build.restype = ctypes.c_int
+        L.oracle_trace.argtypes = [_u32p, _f32p, u32, _f32p, u32, _i32p, _f32p, _u32p, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def scene_bounds(tri: np.ndarray) -> np.ndarray:
+    tri = np.ascontiguousarray(tri, dtype=np.float32).reshape(-1, 12)
+    b = np.empty(6, dtype=np.float32)
+    lib().oracle_scene_bounds(tri, tri.shape[0], b)
+    return b
+
+
+def aabb_zidx(tri: np.ndarray, bounds6, threads: int = 1):
+    """(aabb (N, 8) float32, keys (N,) uint32) in input order."""
+    tri = np.ascontiguousarray(tri, dtype=np.float32).reshape(-1, 12)
+    n = tri.shape[0]
+    b = np.ascontiguousarray(bounds6, dtype=np.float32)
+    aabb = np.empty((n, 8), dtype=np.float32)
+    keys = np.empty(n, dtype=np.uint32)
+    lib().oracle_aabb_zidx(tri, n, b, _ptr(aabb), keys, threads)
+    return aabb, keys
+
+
+def radix_sort(keys: np.ndarray, threads: int = 1):
+    """(sorted keys, permutation) of the reference's 2-bit x 16-pass stable radix sort."""
+    k = np.array(keys, dtype=np.uint32, copy=True)
+    perm = np.empty(k.size, dtype=np.int32)
+    lib().oracle_radix_sort(k, k.size, perm, threads)
+    return k, perm
+
+
+def radix_tree(sorted_keys: np.ndarray, threads: int = 1) -> np.ndarray:
+    k = np.ascontiguousarray(sorted_keys, dtype=np.uint32)
+    parents = np.empty(2 * k.size, dtype=np.int32)
+    lib().oracle_radix_tree(k, k.size, parents, threads)
+    return parents
+
+
+def up_pass(perm, aabb, parents, threads: int = 1, canonical: bool = True) -> np.ndarray:
+    perm = np.ascontiguousarray(perm, dtype=np.int32)
+    n = perm.size
+    nodes = np.empty((n, 16), dtype=np.uint32)
+    lib().oracle_up_pass(perm, np.ascontiguousarray(aabb, dtype=np.float32),
+                         np.ascontiguousarray(parents, dtype=np.int32), n, nodes, threads)
+    if canonical:
+        lib().oracle_canonicalize(nodes, n)
+    return nodes
+
+
+def canonicalize(nodes: np.ndarray) -> np.ndarray:
+    nodes = np.array(nodes, dtype=np.uint32, copy=True).reshape(-1, 16)
+    lib().oracle_canonicalize(nodes, nodes.shape[0])
+    return nodes
+
+
+def rearrange(tri, perm, threads: int = 1) -> np.ndarray:
+    tri = np.ascontiguousarray(tri, dtype=np.float32).reshape(-1, 12)
+    perm = np.ascontiguousarray(perm, dtype=np.int32)
+    out = np.empty((perm.size, 12), dtype=np.float32)
+    lib().oracle_rearrange(tri, perm, perm.size, out, threads)
+    return out
+
+
+def gather_indexed(xyz, idx3) -> np.ndarray:
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+    idx3 = np.ascontiguousarray(idx3, dtype=np.uint32).reshape(-1, 3)
+    out = np.empty((idx3.shape[0], 12), dtype=np.float32)
+    lib().oracle_gather_indexed(xyz, idx3, idx3.shape[0], out)
+    return out
+
+
+def build(tri: np.ndarray, bounds6=None, threads: int = 1) -> dict:
+    """The whole build in canonical form: nodes (N, 16) uint32 words, tris (N, 12) float32,
+    parents (2N,) int32, leaf_index (N,) uint32, morton (N,) uint32, bounds (6,) float32."""
+    tri = np.ascontiguousarray(tri, dtype=np.float32).reshape(-1, 12)
+    n = tri.shape[0]
+    out = dict(nodes=np.empty((n, 16), dtype=np.uint32), tris=np.empty((n, 12), dtype=np.float32),
+               parents=np.empty(2 * n, dtype=np.int32), leaf_index=np.empty(n, dtype=np.int32),
+               morton=np.empty(n, dtype=np.uint32), bounds=np.empty(6, dtype=np.float32))
+    b = None if bounds6 is None else np.ascontiguousarray(bounds6, dtype=np.float32)
+    rc = lib().oracle_build(tri, n, _ptr(b), threads, _ptr(out["nodes"]), _ptr(out["tris"]),
+                            _ptr(out["parents"]), _ptr(out["leaf_index"]), _ptr(out["morton"]),
+                            _ptr(out["bounds"]))
+    assert rc == 0
+    out["leaf_index"] = out["leaf_index"].view(np.uint32)
+    return out
+
+
+def trace(nodes, tris, rays, threads: int = 0):
+    """(hit_prim int32, hit_t float32, max_stack uint32) per ray; rays (R, 8) float32."""
+    nodes = np.ascontiguousarray(nodes, dtype=np.uint32).reshape(-1, 16)
+    tris = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 12)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    r = rays.shape[0]
+    prim = np.empty(r, dtype=np.int32)
+    t = np.empty(r, dtype=np.float32)
+    st = np.empty(r, dtype=np.uint32)
+    lib().oracle_trace(nodes, tris, tris.shape[0], rays, r, prim, t, st, threads)
+    return prim, t, st

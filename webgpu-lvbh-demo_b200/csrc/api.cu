@@ -1,0 +1,487 @@
+// api.cu - the C ABI (include/lvbh.h): context, scratch arena, build orchestration.
+//
+// Replaces the reference's host orchestration (scripts/bvh/build-bvh.js:12-66 and each kernel
+// module's execute(): 69 queue submits and 20 host waits per build) with one stream-ordered
+// chain of 8 kernels and a memset, replayed as a cached CUDA graph when the same build shape
+// repeats, and a single host wait at the end (none with LVBH_ASYNC).
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "lvbh.h"
+#include "lvbh_device.cuh"
+#include "lvbh_internal.h"
+
+namespace lvbh {
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cached[dev]) {
+        int v = 148;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) v = 148;
+        cached[dev] = v;
+    }
+    return cached[dev];
+}
+
+}  // namespace lvbh
+
+using namespace lvbh;
+
+namespace {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+size_t control_bytes(uint32_t n) {
+    return align_up(sizeof(Control)) + (size_t)kSortPasses * sort_tiles(n) * kDigits * sizeof(uint32_t);
+}
+
+struct GraphKey {
+    const void *tri = nullptr;
+    uint32_t n = 0;
+    HostBounds hb{};
+    void *outs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
+};
+
+}  // namespace
+
+struct lvbh_ctx {
+    int device = 0;
+    std::string err;
+    // scratch arena (sized for `cap` triangles)
+    uint32_t cap = 0;
+    void *arena = nullptr;
+    uint32_t *keys_b = nullptr, *vals_b = nullptr, *arrive = nullptr, *epoch = nullptr;
+    Control *ctl = nullptr;
+    uint32_t *lookback = nullptr;
+    // staging for host input
+    size_t stage_bytes = 0;
+    void *stage = nullptr;
+    // pinned readback of the control block head
+    uint32_t *host_ctl = nullptr;
+    cudaEvent_t ev[LVBH_NUM_STAGES + 1] = {};
+    bool ev_valid = false;
+    // cached graph of the last build shape
+    cudaStream_t cap_stream = nullptr;
+    GraphKey gkey;
+    cudaGraphExec_t gexec = nullptr;
+    // last build, for lvbh_sync
+    cudaStream_t last_stream = nullptr;
+    lvbh_result *last_out = nullptr;
+    HostBounds last_hb{};
+    bool pending = false;
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int fail(lvbh_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(lvbh_ctx *ctx, cudaError_t e, const char *what) {
+    const int code = (e == cudaErrorMemoryAllocation) ? LVBH_ENOMEM : LVBH_ECUDA;
+    cudaGetLastError();  // clear the sticky-free error state
+    return fail(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define LVBH_CUDA(ctx, call)                                              \
+    do {                                                                  \
+        cudaError_t e_ = (call);                                          \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);        \
+    } while (0)
+
+void free_arena(lvbh_ctx *ctx) {
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    if (ctx->arena) cudaFree(ctx->arena);
+    ctx->arena = nullptr;
+    ctx->cap = 0;
+}
+
+int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
+    if (n <= ctx->cap && ctx->arena) return LVBH_OK;
+    if (ctx->pending) cudaStreamSynchronize(ctx->last_stream);
+    free_arena(ctx);
+    const uint32_t cap = n < 4096 ? 4096 : n;
+    const size_t kb = align_up((size_t)cap * 4);
+    const size_t total = 3 * kb + align_up(sizeof(uint32_t)) + control_bytes(cap);
+    void *p = nullptr;
+    LVBH_CUDA(ctx, cudaMalloc(&p, total));
+    char *c = static_cast<char *>(p);
+    ctx->arena = p;
+    ctx->keys_b = reinterpret_cast<uint32_t *>(c); c += kb;
+    ctx->vals_b = reinterpret_cast<uint32_t *>(c); c += kb;
+    ctx->arrive = reinterpret_cast<uint32_t *>(c); c += kb;
+    ctx->epoch = reinterpret_cast<uint32_t *>(c); c += align_up(sizeof(uint32_t));
+    ctx->ctl = reinterpret_cast<Control *>(c);
+    ctx->lookback = reinterpret_cast<uint32_t *>(c + align_up(sizeof(Control)));
+    // arrival words and the epoch start at zero; after that the epoch keeps them valid
+    LVBH_CUDA(ctx, cudaMemset(ctx->arrive, 0, kb + align_up(sizeof(uint32_t))));
+    ctx->cap = cap;
+    return LVBH_OK;
+}
+
+int ensure_stage(lvbh_ctx *ctx, size_t bytes) {
+    if (bytes <= ctx->stage_bytes && ctx->stage) return LVBH_OK;
+    if (ctx->pending) cudaStreamSynchronize(ctx->last_stream);
+    if (ctx->stage) cudaFree(ctx->stage);
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    LVBH_CUDA(ctx, cudaMalloc(&ctx->stage, bytes));
+    ctx->stage_bytes = bytes;
+    return LVBH_OK;
+}
+
+// The build proper: every launch on `s`, nothing synchronous.
+void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
+                   const lvbh_result *out, cudaStream_t s, bool profile) {
+    if (profile) cudaEventRecord(ctx->ev[1], s);
+    cudaMemsetAsync(reinterpret_cast<char *>(ctx->ctl) + offsetof(Control, err), 0,
+                    control_bytes(n) - offsetof(Control, err), s);
+    if (!hb.use) launch_bounds(tri, n, ctx->ctl, s);
+    if (profile) cudaEventRecord(ctx->ev[2], s);
+    launch_morton(tri, n, hb, ctx->ctl, out->morton, s);
+    if (profile) cudaEventRecord(ctx->ev[3], s);
+    // ping-pong so that the last pass lands in the result buffers
+    launch_onesweep(out->morton, nullptr, ctx->keys_b, ctx->vals_b, n, 0, ctx->ctl, ctx->lookback, s);
+    launch_onesweep(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 1, ctx->ctl, ctx->lookback, s);
+    launch_onesweep(out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, n, 2, ctx->ctl, ctx->lookback, s);
+    launch_onesweep(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 3, ctx->ctl, ctx->lookback, s);
+    if (profile) cudaEventRecord(ctx->ev[4], s);
+    if (n == 1) cudaMemsetAsync(out->parents, 0, 2 * sizeof(int32_t), s);
+    launch_tree(out->morton, n, out->parents, ctx->epoch, s);
+    if (profile) cudaEventRecord(ctx->ev[5], s);
+    launch_refit(tri, out->leaf_index, out->morton, out->parents, n,
+                 static_cast<float4 *>(out->tris), static_cast<float4 *>(out->nodes), ctx->arrive,
+                 ctx->epoch, ctx->ctl, s);
+    if (profile) cudaEventRecord(ctx->ev[6], s);
+}
+
+int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
+                 const lvbh_result *out, cudaStream_t s) {
+    GraphKey key;
+    std::memset(static_cast<void *>(&key), 0, sizeof key);  // padding takes part in the compare
+    key.tri = tri;
+    key.n = n;
+    key.hb = hb;
+    key.outs[0] = out->nodes; key.outs[1] = out->tris; key.outs[2] = out->parents;
+    key.outs[3] = out->leaf_index; key.outs[4] = out->morton;
+    if (!ctx->gexec || !(key == ctx->gkey)) {
+        if (!ctx->cap_stream) LVBH_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+        LVBH_CUDA(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_build(ctx, tri, n, hb, out, ctx->cap_stream, false);
+        cudaGraph_t g = nullptr;
+        LVBH_CUDA(ctx, cudaStreamEndCapture(ctx->cap_stream, &g));
+        bool updated = false;
+        if (ctx->gexec) {
+            cudaGraphExecUpdateResultInfo info;
+            updated = cudaGraphExecUpdate(ctx->gexec, g, &info) == cudaSuccess;
+            if (!updated) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(ctx->gexec);
+                ctx->gexec = nullptr;
+            }
+        }
+        cudaError_t e = cudaSuccess;
+        if (!updated) e = cudaGraphInstantiate(&ctx->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { ctx->gexec = nullptr; return cuda_fail(ctx, e, "cudaGraphInstantiate"); }
+        ctx->gkey = key;
+    }
+    LVBH_CUDA(ctx, cudaGraphLaunch(ctx->gexec, s));
+    return LVBH_OK;
+}
+
+int alloc_outputs(lvbh_ctx *ctx, uint32_t n, lvbh_result *out) {
+    out->nodes = out->tris = nullptr;
+    out->parents = nullptr;
+    out->leaf_index = out->morton = nullptr;
+    out->owned = 0;
+    if (n == 0) return LVBH_OK;
+    void *p[5] = {};
+    const size_t sz[5] = {64ull * n, 48ull * n, 8ull * n, 4ull * n, 4ull * n};
+    for (int i = 0; i < 5; ++i) {
+        cudaError_t e = cudaMalloc(&p[i], sz[i]);
+        if (e != cudaSuccess) {
+            for (int j = 0; j < i; ++j) cudaFree(p[j]);
+            return cuda_fail(ctx, e, "cudaMalloc(result)");
+        }
+    }
+    out->nodes = p[0];
+    out->tris = p[1];
+    out->parents = static_cast<int32_t *>(p[2]);
+    out->leaf_index = static_cast<uint32_t *>(p[3]);
+    out->morton = static_cast<uint32_t *>(p[4]);
+    out->owned = 1;
+    return LVBH_OK;
+}
+
+int build_common(lvbh_ctx *ctx, const float4 *tri_dev, uint32_t n, const float *model_bounds,
+                 uint32_t flags, lvbh_result *out, cudaStream_t s, bool profile_upload) {
+    HostBounds hb{};
+    if (model_bounds) {
+        std::memcpy(hb.v, model_bounds, sizeof hb.v);
+        hb.use = 1;
+    }
+    const bool profile = (flags & LVBH_PROFILE) != 0;
+    if (n == 0) {
+        ctx->pending = false;
+        ctx->ev_valid = false;
+        if (model_bounds) std::memcpy(out->bounds, model_bounds, sizeof out->bounds);
+        return LVBH_OK;
+    }
+    int rc = LVBH_OK;
+    if (profile && !profile_upload) cudaEventRecord(ctx->ev[0], s);
+    if (profile || (flags & LVBH_NO_GRAPH)) {
+        enqueue_build(ctx, tri_dev, n, hb, out, s, profile);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+    } else {
+        rc = launch_graph(ctx, tri_dev, n, hb, out, s);
+        if (rc) return rc;
+    }
+    ctx->ev_valid = profile;
+    // fetch the error words and the device-reduced bounds with the build
+    LVBH_CUDA(ctx, cudaMemcpyAsync(ctx->host_ctl, ctx->ctl, offsetof(Control, pad1),
+                                   cudaMemcpyDeviceToHost, s));
+    ctx->last_stream = s;
+    ctx->last_out = out;
+    ctx->last_hb = hb;
+    ctx->pending = true;
+    if (flags & LVBH_ASYNC) return LVBH_OK;
+    return lvbh_sync(ctx);
+}
+
+int check_out(lvbh_ctx *ctx, uint32_t n, uint32_t flags, lvbh_result *out) {
+    if (!out) return fail(ctx, LVBH_EINVAL, "out is NULL");
+    if (flags & LVBH_OUT_CALLER) {
+        if (n && (!out->nodes || !out->tris || !out->parents || !out->leaf_index || !out->morton))
+            return fail(ctx, LVBH_EINVAL, "LVBH_OUT_CALLER with a NULL result buffer");
+        if (n && (((uintptr_t)out->nodes | (uintptr_t)out->tris) & 15u))
+            return fail(ctx, LVBH_EINVAL, "result nodes/tris must be 16-byte aligned");
+        if (n && (((uintptr_t)out->parents | (uintptr_t)out->leaf_index | (uintptr_t)out->morton) & 3u))
+            return fail(ctx, LVBH_EINVAL, "result parents/leaf_index/morton must be 4-byte aligned");
+        out->owned = 0;
+        return LVBH_OK;
+    }
+    return alloc_outputs(ctx, n, out);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *lvbh_version(void) { return "lvbh-b200 0.1 (sm_100a)"; }
+
+int lvbh_create(lvbh_ctx **out, const lvbh_config *cfg) {
+    if (!out) return LVBH_EINVAL;
+    *out = nullptr;
+    int dev = cfg ? cfg->device : -1;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return LVBH_ECUDA; }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || dev >= count) { cudaGetLastError(); return LVBH_EINVAL; }
+    lvbh_ctx *ctx = new (std::nothrow) lvbh_ctx();
+    if (!ctx) return LVBH_ENOMEM;
+    ctx->device = dev;
+    DeviceGuard g(dev);
+    if (cudaMallocHost(&ctx->host_ctl, 64) != cudaSuccess) { cudaGetLastError(); delete ctx; return LVBH_ENOMEM; }
+    for (auto &e : ctx->ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); lvbh_destroy(ctx); return LVBH_ECUDA; }
+    }
+    if (cfg && cfg->reserve_tris) {
+        if (cfg->reserve_tris > LVBH_MAX_TRIS) { lvbh_destroy(ctx); return LVBH_EINVAL; }
+        if (int rc = ensure_arena(ctx, cfg->reserve_tris)) { lvbh_destroy(ctx); return rc; }
+    }
+    *out = ctx;
+    return LVBH_OK;
+}
+
+void lvbh_destroy(lvbh_ctx *ctx) {
+    if (!ctx) return;
+    DeviceGuard g(ctx->device);
+    if (ctx->pending) cudaStreamSynchronize(ctx->last_stream);
+    free_arena(ctx);
+    if (ctx->stage) cudaFree(ctx->stage);
+    for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
+    if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    if (ctx->host_ctl) cudaFreeHost(ctx->host_ctl);
+    cudaGetLastError();
+    delete ctx;
+}
+
+int lvbh_build_soup(lvbh_ctx *ctx, const float *tri_array, uint32_t num_tris,
+                    const float *model_bounds, uint32_t flags, lvbh_result *out, void *stream) {
+    if (!ctx) return LVBH_EINVAL;
+    if (!out) return fail(ctx, LVBH_EINVAL, "out is NULL");
+    if (num_tris > LVBH_MAX_TRIS) return fail(ctx, LVBH_EINVAL, "num_tris exceeds LVBH_MAX_TRIS");
+    if (num_tris && !tri_array) return fail(ctx, LVBH_EINVAL, "tri_array is NULL");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (int rc = check_out(ctx, num_tris, flags, out)) return rc;
+    out->num_tris = out->num_nodes = num_tris;
+    std::memset(out->bounds, 0, sizeof out->bounds);
+    if (num_tris) {
+        if (int rc = ensure_arena(ctx, num_tris)) return rc;
+        LVBH_CUDA(ctx, cudaMemsetAsync(&ctx->ctl->aux_err, 0, sizeof(uint32_t), s));
+    }
+    const float4 *tri = reinterpret_cast<const float4 *>(tri_array);
+    bool profile_upload = false;
+    if ((flags & LVBH_INPUT_HOST) && num_tris) {
+        if (int rc = ensure_stage(ctx, 48ull * num_tris)) return rc;
+        if (flags & LVBH_PROFILE) { cudaEventRecord(ctx->ev[0], s); profile_upload = true; }
+        LVBH_CUDA(ctx, cudaMemcpyAsync(ctx->stage, tri_array, 48ull * num_tris, cudaMemcpyHostToDevice, s));
+        tri = static_cast<const float4 *>(ctx->stage);
+    } else if (num_tris && (reinterpret_cast<uintptr_t>(tri_array) & 15u)) {
+        return fail(ctx, LVBH_EINVAL, "device tri_array must be 16-byte aligned");
+    }
+    return build_common(ctx, tri, num_tris, model_bounds, flags, out, s, profile_upload);
+}
+
+int lvbh_build_indexed(lvbh_ctx *ctx, const float *xyz, uint32_t num_verts, const uint32_t *idx3,
+                       uint32_t num_tris, const float *model_bounds, uint32_t flags,
+                       lvbh_result *out, void *stream) {
+    if (!ctx) return LVBH_EINVAL;
+    if (!out) return fail(ctx, LVBH_EINVAL, "out is NULL");
+    if (num_tris > LVBH_MAX_TRIS) return fail(ctx, LVBH_EINVAL, "num_tris exceeds LVBH_MAX_TRIS");
+    if (num_tris && (!xyz || !idx3 || !num_verts)) return fail(ctx, LVBH_EINVAL, "NULL vertex or index buffer");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (int rc = check_out(ctx, num_tris, flags, out)) return rc;
+    out->num_tris = out->num_nodes = num_tris;
+    std::memset(out->bounds, 0, sizeof out->bounds);
+    if (!num_tris) return build_common(ctx, nullptr, 0, model_bounds, flags, out, s, false);
+    if (flags & LVBH_INPUT_HOST) {
+        // indices are validated on the host when they are host memory
+        for (uint64_t i = 0; i < 3ull * num_tris; ++i)
+            if (idx3[i] >= num_verts) return fail(ctx, LVBH_EINVAL, "vertex index out of range");
+    }
+    const size_t soup = align_up(48ull * num_tris);
+    const size_t vb = align_up(12ull * num_verts), ib = align_up(12ull * num_tris);
+    const bool host = (flags & LVBH_INPUT_HOST) != 0;
+    if (int rc = ensure_arena(ctx, num_tris)) return rc;
+    if (int rc = ensure_stage(ctx, soup + (host ? vb + ib : 0))) return rc;
+    LVBH_CUDA(ctx, cudaMemsetAsync(&ctx->ctl->aux_err, 0, sizeof(uint32_t), s));
+    char *st = static_cast<char *>(ctx->stage);
+    bool profile_upload = false;
+    if (flags & LVBH_PROFILE) { cudaEventRecord(ctx->ev[0], s); profile_upload = true; }
+    if (host) {
+        LVBH_CUDA(ctx, cudaMemcpyAsync(st + soup, xyz, 12ull * num_verts, cudaMemcpyHostToDevice, s));
+        LVBH_CUDA(ctx, cudaMemcpyAsync(st + soup + vb, idx3, 12ull * num_tris, cudaMemcpyHostToDevice, s));
+        xyz = reinterpret_cast<const float *>(st + soup);
+        idx3 = reinterpret_cast<const uint32_t *>(st + soup + vb);
+    }
+    launch_gather_indexed(xyz, num_verts, idx3, num_tris, reinterpret_cast<float4 *>(st),
+                          &ctx->ctl->aux_err, s);
+    return build_common(ctx, reinterpret_cast<const float4 *>(st), num_tris, model_bounds, flags,
+                        out, s, profile_upload);
+}
+
+int lvbh_sync(lvbh_ctx *ctx) {
+    if (!ctx) return LVBH_EINVAL;
+    if (!ctx->pending) return LVBH_OK;
+    DeviceGuard g(ctx->device);
+    ctx->pending = false;
+    cudaError_t e = cudaStreamSynchronize(ctx->last_stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamSynchronize");
+    const uint32_t err = ctx->host_ctl[0] | ctx->host_ctl[1];
+    if (ctx->last_out) {
+        if (ctx->last_hb.use) {
+            std::memcpy(ctx->last_out->bounds, ctx->last_hb.v, sizeof ctx->last_hb.v);
+        } else {
+            const uint32_t *b = ctx->host_ctl + offsetof(Control, bounds_ord) / 4;
+            for (int a = 0; a < 3; ++a) {
+                uint32_t lo = ~b[a], hi = b[3 + a];
+                auto inv = [](uint32_t o) {
+                    uint32_t u = (o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o;
+                    float f;
+                    std::memcpy(&f, &u, 4);
+                    return f;
+                };
+                ctx->last_out->bounds[a] = inv(lo);
+                ctx->last_out->bounds[3 + a] = inv(hi);
+            }
+        }
+    }
+    if (err & ERR_BAD_INDEX) return fail(ctx, LVBH_EINVAL, "vertex index out of range");
+    if (err & ERR_NONFINITE) return fail(ctx, LVBH_EINVAL, "non-finite vertex coordinate in the input");
+    if (err & ERR_LOOKBACK_TIMEOUT) return fail(ctx, LVBH_ETIMEOUT, "radix sort look-back wait exceeded its bound");
+    if (err & ERR_CLIMB) return fail(ctx, LVBH_EDEVICE, "refit climb exceeded the maximum tree depth");
+    return LVBH_OK;
+}
+
+int lvbh_release(lvbh_ctx *ctx, lvbh_result *res) {
+    if (!res) return LVBH_EINVAL;
+    if (!res->owned) return LVBH_OK;
+    DeviceGuard g(ctx ? ctx->device : 0);
+    if (ctx && ctx->pending && ctx->last_out == res) lvbh_sync(ctx);
+    cudaFree(res->nodes);
+    cudaFree(res->tris);
+    cudaFree(res->parents);
+    cudaFree(res->leaf_index);
+    cudaFree(res->morton);
+    res->nodes = res->tris = nullptr;
+    res->parents = nullptr;
+    res->leaf_index = res->morton = nullptr;
+    res->owned = 0;
+    return LVBH_OK;
+}
+
+int lvbh_stage_times(lvbh_ctx *ctx, float *ms_out) {
+    if (!ctx || !ms_out) return LVBH_EINVAL;
+    for (int i = 0; i < LVBH_NUM_STAGES; ++i) ms_out[i] = 0.0f;
+    if (!ctx->ev_valid) return fail(ctx, LVBH_EINVAL, "no profiled build to report");
+    DeviceGuard g(ctx->device);
+    for (int i = 0; i < LVBH_NUM_STAGES; ++i) {
+        float ms = 0.0f;
+        cudaError_t e = cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]);
+        if (e != cudaSuccess) { cudaGetLastError(); ms = 0.0f; }
+        ms_out[i] = ms;
+    }
+    return LVBH_OK;
+}
+
+size_t lvbh_scratch_bytes(uint32_t num_tris) {
+    const uint32_t cap = num_tris < 4096 ? 4096 : num_tris;
+    return 3 * align_up((size_t)cap * 4) + align_up(sizeof(uint32_t)) + control_bytes(cap);
+}
+
+const char *lvbh_last_error(const lvbh_ctx *ctx) {
+    if (!ctx) return "no context";
+    return ctx->err.c_str();
+}
+
+int lvbh_trace(lvbh_ctx *ctx, const void *nodes, const void *tris, uint32_t num_tris,
+               const float *rays, uint32_t num_rays, int32_t *hit_prim, float *hit_t,
+               uint32_t *max_stack, void *stream) {
+    if (!ctx) return LVBH_EINVAL;
+    if (num_rays && (!rays || !hit_prim || !hit_t)) return fail(ctx, LVBH_EINVAL, "NULL ray buffer");
+    if (num_tris && (!nodes || !tris)) return fail(ctx, LVBH_EINVAL, "NULL tree buffer");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    launch_trace(static_cast<const float4 *>(nodes), static_cast<const float4 *>(tris), num_tris,
+                 reinterpret_cast<const float4 *>(rays), num_rays, hit_prim, hit_t, max_stack, s);
+    LVBH_CUDA(ctx, cudaGetLastError());
+    LVBH_CUDA(ctx, cudaStreamSynchronize(s));
+    return LVBH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,89 @@
+// lvbh_device.cuh - device helpers shared by the LBVH build kernels (sm_100a).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lvbh {
+
+// Bits of the per-build device error word.
+enum : uint32_t {
+    ERR_NONFINITE = 1u,         // a vertex coordinate is NaN or +-Inf
+    ERR_LOOKBACK_TIMEOUT = 2u,  // a decoupled look-back wait exceeded its bound
+    ERR_CLIMB = 4u,             // a refit climb exceeded the depth any valid tree has
+    ERR_BAD_INDEX = 8u,         // an indexed-mesh vertex index is out of range
+};
+
+// Largest number of cycles a device-side wait spins before it records an error and gives up
+// (about a second at B200 clocks); every wait in this library is bounded by it.
+constexpr long long kSpinLimitCycles = 2000000000ll;
+
+// split_3 / morton_code of scripts/bvh/kernels/aabb-z-idx.js:197-209: 10 bits per axis
+// spread three apart, x in bit 0, y in bit 1, z in bit 2 of each triple.  Inputs above 1023
+// keep the bits the masks let through, exactly as the reference's u32 arithmetic does.
+__device__ __forceinline__ uint32_t split3(uint32_t x) {
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+__device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+    return split3(x) | (split3(y) << 1) | (split3(z) << 2);
+}
+
+// One axis of the quantisation in the reference's operation order (aabb-z-idx.js:191-194):
+//   cen = (max + min) * .5f;  rel = (cen - umin) / (umax - umin);  q = u32(rel * 1023.99f)
+// Every operation is rounded on its own (no contraction), division is correctly rounded,
+// and the float->u32 conversion truncates and saturates (NaN -> 0).
+__device__ __forceinline__ uint32_t quantise(float bmin, float bmax, float umin, float umax) {
+    const float cen = __fmul_rn(__fadd_rn(bmax, bmin), 0.5f);
+    const float rel = __fdiv_rn(__fsub_rn(cen, umin), __fsub_rn(umax, umin));
+    return __float2uint_rz(__fmul_rn(rel, 1023.99f));
+}
+
+// Common-prefix length delta(i, j) of the sorted keys (radix-tree.js:160-185): -1 when j is
+// out of range, clz(k_i ^ k_j) when the keys differ, else 32 + clz(i ^ j) (index tie-break).
+// i must be in range.
+__device__ __forceinline__ int delta(const uint32_t *__restrict__ keys, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    const uint32_t a = __ldg(keys + i), b = __ldg(keys + j);
+    return a != b ? __clz(a ^ b) : 32 + __clz(i ^ j);
+}
+
+// Monotone float <-> uint32 maps for atomic min/max reductions.  `ord_lo` orders floats
+// ascending; atomicMax on ord_hi(x) = ~ord_lo(x) keeps the minimum, atomicMax on ord_lo(x)
+// keeps the maximum, so an all-zero word is the identity of both.
+__device__ __forceinline__ uint32_t ord_lo(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord_lo_inv(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+
+__device__ __forceinline__ bool finite3(float4 v) {
+    return isfinite(v.x) && isfinite(v.y) && isfinite(v.z);
+}
+
+// Relaxed gpu-scope load / store of a 32-bit word another CTA publishes.
+__device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu(uint32_t *p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Streaming (evict-first) 16-byte load and store.
+__device__ __forceinline__ float4 ld_stream(const float4 *p) { return __ldcs(p); }
+__device__ __forceinline__ void st_stream(float4 *p, float4 v) { __stcs(p, v); }
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+}  // namespace lvbh

@@ -1,0 +1,67 @@
+// lvbh_internal.h - launch wrappers shared between the kernel files and the C-ABI layer.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lvbh {
+
+// Radix sort geometry: 8-bit digits, four passes cover every bit of a 32-bit key (Morton keys
+// use 30 bits; keys of triangles outside host-supplied bounds may use all 32).
+constexpr int kDigitBits = 8;
+constexpr int kDigits = 1 << kDigitBits;
+constexpr int kSortPasses = 4;
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;                       // keys per thread
+constexpr int kSortTile = kSortThreads * kSortItems; // keys per tile (4096)
+
+inline uint32_t sort_tiles(uint32_t n) { return (n + kSortTile - 1) / kSortTile; }
+
+// Per-build control block in device memory.  Everything from `err` on is zeroed by one memset
+// at the start of a build; `aux_err` collects errors of steps that run before that memset (the
+// indexed-mesh gather) and is cleared by the host before them.
+struct Control {
+    uint32_t aux_err;
+    uint32_t err;
+    uint32_t tile_counter[kSortPasses];
+    uint32_t pad0[2];
+    uint32_t bounds_ord[6];            // scene min (ord_hi) and max (ord_lo), see lvbh_device.cuh
+    uint32_t pad1[2];
+    uint32_t hist[kSortPasses][kDigits]; // global digit counts of the unsorted keys
+};
+
+struct HostBounds {
+    float v[6];
+    int use;  // 1 = quantise with v; 0 = with the device reduction in Control::bounds_ord
+};
+
+int sm_count();
+
+// K1a: scene box over every vertex of the 48-byte triangle soup.
+void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s);
+// K1b: triangle box centroid -> Morton key (input order) + the four digit histograms; flags
+// non-finite vertices in ctl->err.
+void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl,
+                   uint32_t *keys_out, cudaStream_t s);
+// K2: one onesweep pass over digit `pass`.  vals_in == nullptr generates the identity.
+void launch_onesweep(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
+                     uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *lookback,
+                     cudaStream_t s);
+// K3: Karras radix tree -> parent links (2N).
+void launch_tree(const uint32_t *keys, uint32_t n, int32_t *parents, uint32_t *epoch,
+                 cudaStream_t s);
+// K4: leaf gather + rearrange + bottom-up refit -> BVH nodes.
+void launch_refit(const float4 *tri, const uint32_t *perm, const uint32_t *keys,
+                  const int32_t *parents, uint32_t n, float4 *otri, float4 *nodes,
+                  uint32_t *arrive, const uint32_t *epoch, Control *ctl, cudaStream_t s);
+// Indexed mesh -> 48-byte soup (pad 0).  An index >= num_verts sets ERR_BAD_INDEX in
+// *err and gathers zeros instead of reading out of bounds.
+void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,
+                           uint32_t n, float4 *tri, uint32_t *err, cudaStream_t s);
+// K5: closest-hit traversal (validation consumer).
+void launch_trace(const float4 *nodes, const float4 *tris, uint32_t n, const float4 *rays,
+                  uint32_t num_rays, int32_t *hit_prim, float *hit_t, uint32_t *max_stack,
+                  cudaStream_t s);
+
+}  // namespace lvbh

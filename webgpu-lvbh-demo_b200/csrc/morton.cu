@@ -1,0 +1,175 @@
+// morton.cu - K1a scene-box reduction and K1b Morton keys (sm_100a).
+//
+// Restates compute_aabb_z_idx (scripts/bvh/kernels/aabb-z-idx.js:177-209) and, for the box,
+// the host-side min/max of parse-obj.js:27-53.  Both kernels stream the 48-byte triangle soup
+// once with 16-byte loads: a warp reads 32 triangles as 96 consecutive float4 (three fully
+// coalesced 512-byte loads), transposes them through 1.5 KB of shared memory, and each lane
+// then owns one triangle.  HBM-bound: 48 B read per triangle (+4 B key written by K1b).
+#include "lvbh_device.cuh"
+#include "lvbh_internal.h"
+
+namespace lvbh {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+__device__ __forceinline__ void warp_minmax(float (&mn)[3], float (&mx)[3]) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = fminf(mn[a], __shfl_xor_sync(0xFFFFFFFFu, mn[a], o));
+            mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xFFFFFFFFu, mx[a], o));
+        }
+    }
+}
+
+// K1a: min / max of every vertex coordinate.  Vertices are the float4 of the soup; the pad
+// word is ignored.  fminf/fmaxf skip NaN (K1b reports non-finite input separately).
+__global__ void __launch_bounds__(kThreads) k_bounds(const float4 *__restrict__ v, uint64_t nv,
+                                                     Control *__restrict__ ctl) {
+    float mn[3] = {INFINITY, INFINITY, INFINITY};
+    float mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const uint64_t stride = (uint64_t)gridDim.x * kThreads;
+    uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
+    for (; i + 3 * stride < nv; i += 4 * stride) {
+        float4 p[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) p[u] = ld_stream(v + i + u * stride);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            mn[0] = fminf(mn[0], p[u].x); mx[0] = fmaxf(mx[0], p[u].x);
+            mn[1] = fminf(mn[1], p[u].y); mx[1] = fmaxf(mx[1], p[u].y);
+            mn[2] = fminf(mn[2], p[u].z); mx[2] = fmaxf(mx[2], p[u].z);
+        }
+    }
+    for (; i < nv; i += stride) {
+        const float4 p = ld_stream(v + i);
+        mn[0] = fminf(mn[0], p.x); mx[0] = fmaxf(mx[0], p.x);
+        mn[1] = fminf(mn[1], p.y); mx[1] = fmaxf(mx[1], p.y);
+        mn[2] = fminf(mn[2], p.z); mx[2] = fmaxf(mx[2], p.z);
+    }
+    warp_minmax(mn, mx);
+    __shared__ float s[kWarps][6];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { s[warp][a] = mn[a]; s[warp][3 + a] = mx[a]; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int a = threadIdx.x;
+        float r = s[0][a];
+        for (int w = 1; w < kWarps; ++w) r = a < 3 ? fminf(r, s[w][a]) : fmaxf(r, s[w][a]);
+        if (a < 3) atomicMax(&ctl->bounds_ord[a], ~ord_lo(r));
+        else atomicMax(&ctl->bounds_ord[a], ord_lo(r));
+    }
+}
+
+// K1b: per triangle box, centroid, quantisation and 30-bit Morton key, written in input order;
+// the digit histograms of all four sort passes are accumulated on the way.
+__global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ tri, uint32_t n,
+                                                     HostBounds hb, Control *__restrict__ ctl,
+                                                     uint32_t *__restrict__ keys) {
+    __shared__ float4 stage[kWarps][96];
+    __shared__ uint32_t hist[kSortPasses][kDigits];
+    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) (&hist[0][0])[i] = 0;
+
+    float umin[3], umax[3];
+    if (hb.use) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { umin[a] = hb.v[a]; umax[a] = hb.v[3 + a]; }
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            umin[a] = ord_lo_inv(~ctl->bounds_ord[a]);
+            umax[a] = ord_lo_inv(ctl->bounds_ord[3 + a]);
+        }
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t nv = 3ull * n;
+    const uint32_t chunks = (n + 31) / 32;
+    const uint32_t warps_total = gridDim.x * kWarps;
+    bool bad = false;
+    for (uint32_t c = blockIdx.x * kWarps + warp; c < chunks; c += warps_total) {
+        const uint64_t base = 96ull * c;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const uint64_t e = base + 32 * r + lane;
+            stage[warp][32 * r + lane] = e < nv ? ld_stream(tri + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncwarp();
+        const float4 v0 = stage[warp][3 * lane], v1 = stage[warp][3 * lane + 1],
+                     v2 = stage[warp][3 * lane + 2];
+        __syncwarp();
+        const uint32_t t = 32u * c + lane;
+        if (t < n) {
+            bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
+            // box.min = min(v0, min(v1, v2)); box.max = max(v0, max(v1, v2))   (:186-187)
+            const uint32_t qx = quantise(fminf(v0.x, fminf(v1.x, v2.x)), fmaxf(v0.x, fmaxf(v1.x, v2.x)), umin[0], umax[0]);
+            const uint32_t qy = quantise(fminf(v0.y, fminf(v1.y, v2.y)), fmaxf(v0.y, fmaxf(v1.y, v2.y)), umin[1], umax[1]);
+            const uint32_t qz = quantise(fminf(v0.z, fminf(v1.z, v2.z)), fmaxf(v0.z, fmaxf(v1.z, v2.z)), umin[2], umax[2]);
+            const uint32_t key = morton3(qx, qy, qz);
+            keys[t] = key;
+#pragma unroll
+            for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (kDigitBits * p)) & (kDigits - 1)], 1u);
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) {
+        const uint32_t c = (&hist[0][0])[i];
+        if (c) atomicAdd(&ctl->hist[0][0] + i, c);
+    }
+}
+
+__global__ void k_gather_indexed(const float *__restrict__ xyz, uint32_t num_verts,
+                                 const uint32_t *__restrict__ idx3, uint32_t n,
+                                 float4 *__restrict__ tri, uint32_t *__restrict__ err) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const uint32_t vi = __ldg(idx3 + 3ull * t + v);
+        if (vi >= num_verts) {
+            atomicOr(err, ERR_BAD_INDEX);
+            tri[3ull * t + v] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        const float *p = xyz + 3ull * vi;
+        tri[3ull * t + v] = make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), 0.0f);
+    }
+}
+
+}  // namespace
+
+void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s) {
+    const uint64_t nv = 3ull * n;
+    uint64_t blocks = (nv + kThreads * 4 - 1) / (kThreads * 4);
+    const uint64_t cap = (uint64_t)sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_bounds<<<(unsigned)blocks, kThreads, 0, s>>>(tri, nv, ctl);
+}
+
+void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl, uint32_t *keys,
+                   cudaStream_t s) {
+    const uint64_t chunks = (n + 31) / 32;
+    uint64_t blocks = (chunks + kWarps - 1) / kWarps;
+    const uint64_t cap = (uint64_t)sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_morton<<<(unsigned)blocks, kThreads, 0, s>>>(tri, n, hb, ctl, keys);
+}
+
+void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,
+                           uint32_t n, float4 *tri, uint32_t *err, cudaStream_t s) {
+    if (n == 0) return;
+    k_gather_indexed<<<(n + 255) / 256, 256, 0, s>>>(xyz, num_verts, idx3, n, tri, err);
+}
+
+}  // namespace lvbh

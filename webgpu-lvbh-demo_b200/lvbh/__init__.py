@@ -1,0 +1,263 @@
+"""B200-native LBVH builder - Python host side of the C ABI in include/lvbh.h.
+
+Mirrors the reference's build entry (scripts/bvh/build-bvh.js):
+
+    BVH = initBVHBuild(device)                                   # build-bvh.js:1-10
+    out = BVH.build(TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS)           # build-bvh.js:12-66
+    out["BVH_BUFFER"], out["O_TRIANGLE_BUFFER"]
+
+with the same argument meaning: TRI_ARRAY holds 12 floats per triangle (the pad slot is
+ignored), MODEL_BOUNDS is {"min": [x, y, z], "max": [x, y, z]} (parse-obj.js:80-87) or None to
+reduce the scene box on the device.  As in the reference, a TRI_ARRAY longer than
+12 * NUM_TRIS is an error (Float32Array.set throws a RangeError, build-bvh.js:20) and a shorter
+one leaves the remaining floats zero.  Results stay on the GPU as torch tensors; the reference
+returns GPU buffers the same way (build-bvh.js:65).
+
+torch provides device memory and streams only; every byte of the build is computed by the
+sm_100a kernels in liblvbh.so.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _native
+from ._native import (ASYNC, INPUT_HOST, NO_GRAPH, OUT_CALLER, PROFILE, STAGE_NAMES, LvbhError,
+                      version)
+
+__all__ = ["initBVHBuild", "BVHBuilder", "BuildResult", "LvbhError", "version", "trace"]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_ptr(stream, device):
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream(device)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def bounds_from_model(model_bounds) -> Optional[np.ndarray]:
+    """MODEL_BOUNDS ({min, max} dict, 6 floats, or None) -> float32[6] or None."""
+    if model_bounds is None:
+        return None
+    if isinstance(model_bounds, dict):
+        b = list(model_bounds["min"]) + list(model_bounds["max"])
+    else:
+        b = list(np.asarray(model_bounds, dtype=np.float64).ravel())
+    if len(b) != 6:
+        raise ValueError("MODEL_BOUNDS needs 3 min and 3 max values")
+    return np.asarray(b, dtype=np.float32)  # DataView.setFloat32 rounding (aabb-z-idx.js:116-122)
+
+
+def soup_from_tri_array(tri_array, num_tris: int):
+    """TRI_ARRAY -> (N, 12) float32 host array or CUDA tensor, with the reference's length rule."""
+    torch = _torch()
+    need = 12 * int(num_tris)
+    if isinstance(tri_array, torch.Tensor):
+        t = tri_array.reshape(-1)
+        if t.numel() > need:
+            raise ValueError(f"RangeError: TRI_ARRAY holds {t.numel()} floats, NUM_TRIS*12 = {need}")
+        if t.dtype != torch.float32:
+            t = t.to(torch.float32)
+        if t.numel() < need:
+            t = torch.cat([t, torch.zeros(need - t.numel(), dtype=torch.float32, device=t.device)])
+        return t.contiguous().reshape(int(num_tris), 12)
+    a = np.asarray(tri_array, dtype=np.float32).reshape(-1)
+    if a.size > need:
+        raise ValueError(f"RangeError: TRI_ARRAY holds {a.size} floats, NUM_TRIS*12 = {need}")
+    if a.size < need:
+        a = np.concatenate([a, np.zeros(need - a.size, dtype=np.float32)])
+    return np.ascontiguousarray(a).reshape(int(num_tris), 12)
+
+
+@dataclass
+class BuildResult:
+    """Device-resident result.  nodes: int32 (N, 16) BVHNode words (box words are float32 bits,
+    view with .view(torch.float32)); tris: float32 (N, 12); parents: int32 (2N,);
+    leaf_index: int32 (N,) (the reference's IDX_BUFFER); morton: int32 (N,) key bits;
+    bounds: float32 (6,) quantisation box; stage_ms: per-stage device times when profiled."""
+    nodes: object
+    tris: object
+    parents: object
+    leaf_index: object
+    morton: object
+    bounds: np.ndarray
+    stage_ms: Optional[dict] = None
+
+    def as_reference(self) -> dict:
+        """{BVH_BUFFER, O_TRIANGLE_BUFFER} as the reference's build() returns them."""
+        return {"BVH_BUFFER": self.nodes, "O_TRIANGLE_BUFFER": self.tris}
+
+    def to_numpy(self) -> dict:
+        return {"nodes": self.nodes.cpu().numpy().view(np.uint32),
+                "tris": self.tris.cpu().numpy(),
+                "parents": self.parents.cpu().numpy(),
+                "leaf_index": self.leaf_index.cpu().numpy().view(np.uint32),
+                "morton": self.morton.cpu().numpy().view(np.uint32),
+                "bounds": self.bounds.copy()}
+
+
+def empty_outputs(n: int, device):
+    torch = _torch()
+    return dict(nodes=torch.empty((n, 16), dtype=torch.int32, device=device),
+                tris=torch.empty((n, 12), dtype=torch.float32, device=device),
+                parents=torch.empty(2 * n, dtype=torch.int32, device=device),
+                leaf_index=torch.empty(n, dtype=torch.int32, device=device),
+                morton=torch.empty(n, dtype=torch.int32, device=device))
+
+
+def _result_struct(outs, n) -> _native.Result:
+    r = _native.Result()
+    r.num_tris = n
+    r.num_nodes = n
+    for k in ("nodes", "tris", "parents", "leaf_index", "morton"):
+        setattr(r, k, outs[k].data_ptr() if n else None)
+    return r
+
+
+class BVHBuilder:
+    """One library context bound to a CUDA device (initBVHBuild(device), build-bvh.js:1-10)."""
+
+    def __init__(self, device=0, reserve_tris: int = 0):
+        torch = _torch()
+        self.device = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
+        cfg = _native.Config(device=self.device.index or 0, reserve_tris=int(reserve_tris))
+        ctx = ctypes.c_void_p()
+        rc = _native.lib.lvbh_create(ctypes.byref(ctx), ctypes.byref(cfg))
+        if rc != _native.OK:
+            raise LvbhError(rc, "lvbh_create failed")
+        self._ctx = ctx
+        self._pending = None
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            _native.lib.lvbh_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def ctx(self):
+        return self._ctx
+
+    # -- reference-shaped entry -------------------------------------------------------------
+    def build(self, TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS=None) -> dict:  # noqa: N803
+        """build(TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS) -> {BVH_BUFFER, O_TRIANGLE_BUFFER, ...}."""
+        res = self.build_soup(soup_from_tri_array(TRI_ARRAY, NUM_TRIS), bounds_from_model(MODEL_BOUNDS))
+        out = res.as_reference()
+        out.update(PARENT_BUFFER=res.parents, IDX_BUFFER=res.leaf_index, Z_IDX_BUFFER=res.morton,
+                   BOUNDS=res.bounds)
+        return out
+
+    # -- full-control entries ---------------------------------------------------------------
+    def build_soup(self, tri, bounds=None, outputs=None, stream=None, sync=True, profile=False,
+                   graph=True) -> BuildResult:
+        """tri: (N, 12) float32 numpy array (host, copied inside the call) or CUDA tensor."""
+        torch = _torch()
+        host = not isinstance(tri, torch.Tensor)
+        if host:
+            tri = np.ascontiguousarray(tri, dtype=np.float32).reshape(-1, 12)
+            n = tri.shape[0]
+            ptr = tri.ctypes.data_as(ctypes.c_void_p)
+        else:
+            if tri.device.type != "cuda":
+                tri = tri.to(self.device)
+            tri = tri.contiguous().reshape(-1, 12)
+            if tri.dtype != torch.float32:
+                raise TypeError("device triangle soup must be float32")
+            n = tri.shape[0]
+            ptr = ctypes.c_void_p(tri.data_ptr())
+        flags = OUT_CALLER | (INPUT_HOST if host else 0) | (0 if sync else ASYNC) \
+            | (PROFILE if profile else 0) | (0 if graph else NO_GRAPH)
+        return self._run(_native.lib.lvbh_build_soup, (ptr, n), n, bounds, flags, outputs,
+                         stream, sync, profile, keep=(tri,))
+
+    def build_indexed(self, xyz, idx3, bounds=None, outputs=None, stream=None, sync=True,
+                      profile=False) -> BuildResult:
+        """xyz: (V, 3) float32, idx3: (N, 3) uint32 - both host arrays or both CUDA tensors."""
+        torch = _torch()
+        host = not isinstance(xyz, torch.Tensor)
+        if host:
+            xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+            idx3 = np.ascontiguousarray(idx3, dtype=np.uint32).reshape(-1, 3)
+            pv, pi = xyz.ctypes.data_as(ctypes.c_void_p), idx3.ctypes.data_as(ctypes.c_void_p)
+        else:
+            xyz = xyz.contiguous().reshape(-1, 3)
+            idx3 = idx3.contiguous().reshape(-1, 3)
+            pv, pi = ctypes.c_void_p(xyz.data_ptr()), ctypes.c_void_p(idx3.data_ptr())
+        n, nv = idx3.shape[0], xyz.shape[0]
+        flags = OUT_CALLER | (INPUT_HOST if host else 0) | (0 if sync else ASYNC) \
+            | (PROFILE if profile else 0)
+        return self._run(_native.lib.lvbh_build_indexed, (pv, nv, pi, n), n, bounds, flags,
+                         outputs, stream, sync, profile, keep=(xyz, idx3))
+
+    def _run(self, fn, head, n, bounds, flags, outputs, stream, sync, profile, keep):
+        if self._pending is not None:
+            self.sync()
+        outs = outputs if outputs is not None else empty_outputs(n, self.device)
+        r = _result_struct(outs, n)
+        b = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float32).reshape(6)
+        bp = None if b is None else b.ctypes.data_as(ctypes.c_void_p)
+        sp = _stream_ptr(stream, self.device)
+        rc = fn(self._ctx, *head, bp, flags, ctypes.byref(r), sp)
+        res = BuildResult(bounds=np.zeros(6, np.float32), **outs)
+        if rc != _native.OK:
+            _native.check(self._ctx, rc)
+        if sync:
+            res.bounds = np.array(r.bounds[:], dtype=np.float32)
+            if profile:
+                res.stage_ms = self.stage_times()
+        else:
+            self._pending = (r, res, keep, profile)
+        return res
+
+    def sync(self):
+        """Wait for an asynchronous build and raise its device-side status."""
+        if self._pending is None:
+            return
+        r, res, _, profile = self._pending
+        self._pending = None
+        _native.check(self._ctx, _native.lib.lvbh_sync(self._ctx))
+        res.bounds = np.array(r.bounds[:], dtype=np.float32)
+        if profile:
+            res.stage_ms = self.stage_times()
+
+    def stage_times(self) -> dict:
+        arr = (ctypes.c_float * _native.NUM_STAGES)()
+        _native.check(self._ctx, _native.lib.lvbh_stage_times(self._ctx, arr))
+        return dict(zip(STAGE_NAMES, [float(x) for x in arr]))
+
+    def trace(self, res: BuildResult, rays, stream=None):
+        """Closest-hit traversal (scripts/pathtracer/pathtracer.js:495-628) of rays (R, 8)
+        float32 CUDA tensor -> (hit_prim int32, hit_t float32, max_stack int32)."""
+        torch = _torch()
+        rays = rays.contiguous().reshape(-1, 8)
+        nr = rays.shape[0]
+        prim = torch.empty(nr, dtype=torch.int32, device=self.device)
+        t = torch.empty(nr, dtype=torch.float32, device=self.device)
+        st = torch.empty(nr, dtype=torch.int32, device=self.device)
+        n = res.tris.shape[0]
+        rc = _native.lib.lvbh_trace(self._ctx, ctypes.c_void_p(res.nodes.data_ptr() if n else 0),
+                                    ctypes.c_void_p(res.tris.data_ptr() if n else 0), n,
+                                    ctypes.c_void_p(rays.data_ptr()), nr,
+                                    ctypes.c_void_p(prim.data_ptr()), ctypes.c_void_p(t.data_ptr()),
+                                    ctypes.c_void_p(st.data_ptr()), _stream_ptr(stream, self.device))
+        _native.check(self._ctx, rc)
+        return prim, t, st
+
+
+def initBVHBuild(device=0) -> BVHBuilder:  # noqa: N802
+    """initBVHBuild(device) -> object with .build (scripts/bvh/build-bvh.js:1-10)."""
+    return BVHBuilder(device)
+
+
+def trace(builder: BVHBuilder, res: BuildResult, rays):
+    return builder.trace(res, rays)

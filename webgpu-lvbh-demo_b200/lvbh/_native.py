@@ -1,0 +1,88 @@
+"""ctypes binding of the C ABI declared in include/lvbh.h (liblvbh.so, built in-tree).
+
+There is no fallback: when the compiled library is missing, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblvbh.so")
+
+# status codes (include/lvbh.h)
+OK, EINVAL, ENOMEM, ETIMEOUT, ECUDA, EBUSY, EDEVICE = 0, 1, 2, 3, 4, 5, 6
+STATUS_NAMES = {OK: "LVBH_OK", EINVAL: "LVBH_EINVAL", ENOMEM: "LVBH_ENOMEM",
+                ETIMEOUT: "LVBH_ETIMEOUT", ECUDA: "LVBH_ECUDA", EBUSY: "LVBH_EBUSY",
+                EDEVICE: "LVBH_EDEVICE"}
+
+# build flags
+INPUT_HOST, ASYNC, OUT_CALLER, PROFILE, NO_GRAPH = 0x1, 0x2, 0x4, 0x8, 0x10
+MAX_TRIS = 1 << 29
+NUM_STAGES = 6
+STAGE_NAMES = ("upload", "bounds", "morton", "sort", "tree", "refit")
+
+
+class LvbhError(RuntimeError):
+    """A non-zero status returned through the C ABI."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("reserve_tris", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint64 * 4)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("num_tris", ctypes.c_uint32), ("num_nodes", ctypes.c_uint32),
+                ("nodes", ctypes.c_void_p), ("tris", ctypes.c_void_p),
+                ("parents", ctypes.c_void_p), ("leaf_index", ctypes.c_void_p),
+                ("morton", ctypes.c_void_p), ("bounds", ctypes.c_float * 6),
+                ("owned", ctypes.c_uint32)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {os.path.dirname(HERE)}` "
+                          "(or __graft_entry__.build()); there is no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, u32, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int
+    L.lvbh_version.restype = ctypes.c_char_p
+    L.lvbh_version.argtypes = []
+    L.lvbh_create.restype = i32
+    L.lvbh_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(Config)]
+    L.lvbh_destroy.restype = None
+    L.lvbh_destroy.argtypes = [vp]
+    L.lvbh_build_soup.restype = i32
+    L.lvbh_build_soup.argtypes = [vp, vp, u32, vp, u32, ctypes.POINTER(Result), vp]
+    L.lvbh_build_indexed.restype = i32
+    L.lvbh_build_indexed.argtypes = [vp, vp, u32, vp, u32, vp, u32, ctypes.POINTER(Result), vp]
+    L.lvbh_sync.restype = i32
+    L.lvbh_sync.argtypes = [vp]
+    L.lvbh_release.restype = i32
+    L.lvbh_release.argtypes = [vp, ctypes.POINTER(Result)]
+    L.lvbh_stage_times.restype = i32
+    L.lvbh_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.lvbh_scratch_bytes.restype = ctypes.c_size_t
+    L.lvbh_scratch_bytes.argtypes = [u32]
+    L.lvbh_last_error.restype = ctypes.c_char_p
+    L.lvbh_last_error.argtypes = [vp]
+    L.lvbh_trace.restype = i32
+    L.lvbh_trace.argtypes = [vp, vp, vp, u32, vp, u32, vp, vp, vp, vp]
+    return L
+
+
+lib = _load()
+
+
+def version() -> str:
+    return lib.lvbh_version().decode()
+
+
+def check(ctx, rc: int):
+    if rc != OK:
+        msg = lib.lvbh_last_error(ctx).decode() if ctx else "no context"
+        raise LvbhError(rc, msg)
