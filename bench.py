@@ -58,6 +58,8 @@ def make_workload(name: str):
     from lvbh import scenes
     if name == "clustered16M":
         return scenes.clustered_soup(1 << 24, seed=2), "clustered_soup_16M"
+    if name == "clustered4M":  # the same distribution at 2^22 triangles (profiling captures)
+        return scenes.clustered_soup(1 << 22, seed=2), "clustered_soup_4M"
     if name == "sphere2M":
         return scenes.sphere_mesh(1024, seed=1), "sphere_mesh_2M"
     if name == "uniform64K":
@@ -74,14 +76,21 @@ class ClockSampler:
 
     def __init__(self, index: int):
         self.index = index
+        self.ident = None
+        try:
+            import torch
+            self.ident = "GPU-" + str(torch.cuda.get_device_properties(index).uuid)
+        except Exception:
+            pass
         self.proc = None
         self.lines = []
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+            ident = ["--id=" + self.ident] if self.ident else []
+            self.proc = subprocess.Popen(["nvidia-smi", *ident, f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                         stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
         except Exception:
@@ -116,7 +125,8 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0,
+                    "raw": self.lines[:3]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm)}
 
