@@ -4,8 +4,9 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload clustered16M|sphere2M|uniform64K]
 
-One step = one complete build (scene box, Morton keys, 4-pass onesweep sort, Karras tree,
-refit + rearrange) of the workload's triangle soup.  Default workload: the 16,777,216-triangle
+One step = one complete build (scene box, Morton keys, 4-pass onesweep sort, and one pass that
+emits the radix tree, gathers and rearranges the triangles and refits the boxes) of the
+workload's triangle soup.  Default workload: the 16,777,216-triangle
 Gaussian-mixture scene (seeded synthetic data; the reference publishes no scene set).  The
 805 MB input soup is larger than the 126 MB L2, so steps run back to back without a flush.
 
@@ -39,9 +40,12 @@ UNIT = "Mprims/s"
 
 # Algorithmic HBM bytes per triangle of each stage (fixed traffic model): bounds read 48;
 # Morton read 48 + key 4; sort 48 (3 LSD passes of 30-bit keys: histogram read 4, pass 1 read 4
-# write 8, passes 2-3 read 8 write 8); tree keys 4 + parents 8 + child links 8; refit +
-# rearrange perm 4 + gather 48 + write 48 + node words 56 + parent reads 8 + flag atomics 8.
-MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "tree": 20, "refit": 172}
+# write 8, passes 2-3 read 8 write 8); emit = tree (keys 4 + parents 8 + child links 8) +
+# refit and rearrange (perm 4 + gather 48 + write 48 + node words 56 + parent reads 8 + flag
+# atomics 8) = 20 + 172.
+MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "emit": 192}
+KERNELS = {"bounds": "k_bounds", "morton": "k_morton", "sort": "k_onesweep x4", "emit": "k_emit"}
+LAUNCHES_PER_BUILD = 7  # bounds, morton, 4 onesweep passes, emit
 MODEL_TOTAL = sum(MODEL_BYTES.values())  # 340 B per triangle
 
 
@@ -99,7 +103,15 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def wait_ready(self, timeout=5.0):
+        t0 = time.perf_counter()
+        while self.proc and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.05)
+
+    def count(self, t0, t1):
+        return sum(1 for t, _ in self.lines if t0 <= t <= t1)
 
     def __exit__(self, *a):
         if self.proc:
@@ -109,10 +121,12 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, t0=None, t1=None):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ts, ln in self.lines:
+            if t0 is not None and not (t0 <= ts <= t1):
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -126,7 +140,7 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0,
-                    "raw": self.lines[:3]}
+                    "raw": [ln for _, ln in self.lines[:3]]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm)}
 
@@ -226,6 +240,8 @@ def run_ours(args, world, rank, local):
     def step(profile=False, sync=False):
         return builder.build_soup(dtri, None, outputs=outs, stream=stream, sync=sync, profile=profile)
 
+    clocks = ClockSampler(local).__enter__()
+    clocks.wait_ready()
     # warm-up (graph capture happens on the first call)
     for _ in range(args.warmup):
         step(sync=True)
@@ -235,13 +251,26 @@ def run_ours(args, world, rank, local):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(world)
     torch.cuda.synchronize(dev)
-    with ClockSampler(local) as clocks:
-        ev0.record(stream)
-        for _ in range(args.steps):
+    h0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(sync=False)
+    ev1.record(stream)
+    builder.sync()
+    torch.cuda.synchronize(dev)
+    h1 = time.perf_counter()
+    # The sampler ticks every 200 ms; when the timed region was shorter than a few ticks, the
+    # same builds keep running (untimed) until three samples are in, and those are reported.
+    h2 = h1
+    while clocks.count(h0, h2) < 3 and h2 - h1 < 3.0:
+        for _ in range(20):
             step(sync=False)
-        ev1.record(stream)
         builder.sync()
-        torch.cuda.synchronize(dev)
+        h2 = time.perf_counter()
+    clock_summary = clocks.summary(h0, h2)
+    clock_summary["window_s"] = round(h2 - h0, 3)
+    clock_summary["timed_region_s"] = round(h1 - h0, 3)
+    clocks.__exit__()
     barrier(world)
     ms = ev0.elapsed_time(ev1) / args.steps
     ms = max_over_ranks(ms, world)
@@ -254,13 +283,11 @@ def run_ours(args, world, rank, local):
         for k, v in res.stage_ms.items():
             stages[k].append(v)
     stage_ms = {k: statistics.mean(v) for k, v in stages.items() if k != "upload"}
-    dom = max(("bounds", "morton", "sort", "tree", "refit"), key=lambda k: stage_ms[k])
+    dom = max(MODEL_BYTES, key=lambda k: stage_ms[k])
     dom_bytes = MODEL_BYTES[dom] * n
     achieved = dom_bytes / (stage_ms[dom] * 1e-3) / 1e9
     traffic = load_traffic(dom, n)
-    roofline = {"bound": "hbm", "kernel": {"refit": "k_refit", "sort": "k_onesweep x4",
-                                          "morton": "k_morton", "bounds": "k_bounds",
-                                          "tree": "k_tree"}[dom],
+    roofline = {"bound": "hbm", "kernel": KERNELS[dom],
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes": dom_bytes,
@@ -301,9 +328,9 @@ def run_ours(args, world, rank, local):
             "config": {"workload": wname, "num_tris": n, "parallelism": "replicas" if world > 1 else "single",
                        "bounds": "reduced on the device over all vertices",
                        "l2": "input soup 805 MB > 126 MB L2; no flush", "graph": True},
-            "gpu_launches": 8 * args.steps,
+            "gpu_launches": LAUNCHES_PER_BUILD * args.steps,
             "roofline": roofline, "stage_ms": stage_ms, "cpu_baseline": cpu, "e2e": e2e_line,
-            "clocks": clocks.summary()}
+            "clocks": clock_summary}
     print(json.dumps(line), flush=True)
 
 

@@ -83,9 +83,8 @@ extern "C" {
 #define LVBH_STAGE_BOUNDS  1  /* scene box reduction (skipped when bounds are supplied) */
 #define LVBH_STAGE_MORTON  2  /* triangle centroid -> 30-bit Morton key + digit histograms */
 #define LVBH_STAGE_SORT    3  /* onesweep stable radix sort of (key, triangle index) */
-#define LVBH_STAGE_TREE    4  /* Karras radix tree -> parent links */
-#define LVBH_STAGE_REFIT   5  /* leaf gather + triangle rearrange + bottom-up box refit */
-#define LVBH_NUM_STAGES    6
+#define LVBH_STAGE_EMIT    4  /* radix tree + leaf gather + triangle rearrange + box refit */
+#define LVBH_NUM_STAGES    5
 
 typedef struct lvbh_ctx lvbh_ctx;
 

@@ -41,6 +41,15 @@ size_t control_bytes(uint32_t n) {
     return align_up(sizeof(Control)) + (size_t)kSortPasses * sort_tiles(n) * kDigits * sizeof(uint32_t);
 }
 
+// Scratch of a context sized for `cap` triangles: sort ping-pong keys and values, the tree
+// pass's open-node buffers, the control block and the look-back words.
+size_t arena_bytes(uint32_t cap) {
+    const size_t groups = emit_groups(cap);
+    return 3 * align_up((size_t)cap * 4) + align_up((size_t)cap * 24) + align_up((size_t)cap * 32) +
+           align_up(groups * kOpenCap * sizeof(OpenItem)) + align_up(groups * sizeof(uint32_t)) +
+           align_up(sizeof(uint32_t)) + control_bytes(cap);
+}
+
 struct GraphKey {
     const void *tri = nullptr;
     uint32_t n = 0;
@@ -57,7 +66,11 @@ struct lvbh_ctx {
     // scratch arena (sized for `cap` triangles)
     uint32_t cap = 0;
     void *arena = nullptr;
-    uint32_t *keys_b = nullptr, *vals_b = nullptr, *arrive = nullptr, *epoch = nullptr;
+    uint32_t *keys_b = nullptr, *vals_b = nullptr;
+    float2 *lbox = nullptr;
+    OpenItem *items = nullptr;
+    uint32_t *counts = nullptr, *arrive = nullptr, *epoch = nullptr;
+    float4 *pend = nullptr;
     Control *ctl = nullptr;
     uint32_t *lookback = nullptr;
     // staging for host input
@@ -121,20 +134,25 @@ int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
     if (ctx->pending) cudaStreamSynchronize(ctx->last_stream);
     free_arena(ctx);
     const uint32_t cap = n < 4096 ? 4096 : n;
-    const size_t kb = align_up((size_t)cap * 4);
-    const size_t total = 3 * kb + align_up(sizeof(uint32_t)) + control_bytes(cap);
     void *p = nullptr;
-    LVBH_CUDA(ctx, cudaMalloc(&p, total));
+    LVBH_CUDA(ctx, cudaMalloc(&p, arena_bytes(cap)));
     char *c = static_cast<char *>(p);
     ctx->arena = p;
+    const size_t kb = align_up((size_t)cap * 4);
+    const size_t groups = emit_groups(cap);
     ctx->keys_b = reinterpret_cast<uint32_t *>(c); c += kb;
     ctx->vals_b = reinterpret_cast<uint32_t *>(c); c += kb;
     ctx->arrive = reinterpret_cast<uint32_t *>(c); c += kb;
+    ctx->lbox = reinterpret_cast<float2 *>(c); c += align_up((size_t)cap * 24);
+    ctx->pend = reinterpret_cast<float4 *>(c); c += align_up((size_t)cap * 32);
+    ctx->items = reinterpret_cast<OpenItem *>(c); c += align_up(groups * kOpenCap * sizeof(OpenItem));
+    ctx->counts = reinterpret_cast<uint32_t *>(c); c += align_up(groups * sizeof(uint32_t));
     ctx->epoch = reinterpret_cast<uint32_t *>(c); c += align_up(sizeof(uint32_t));
     ctx->ctl = reinterpret_cast<Control *>(c);
     ctx->lookback = reinterpret_cast<uint32_t *>(c + align_up(sizeof(Control)));
-    // arrival words and the epoch start at zero; after that the epoch keeps them valid
-    LVBH_CUDA(ctx, cudaMemset(ctx->arrive, 0, kb + align_up(sizeof(uint32_t))));
+    // arrival words and the epoch start at zero; from then on the epoch keeps them valid
+    LVBH_CUDA(ctx, cudaMemset(ctx->arrive, 0, kb));
+    LVBH_CUDA(ctx, cudaMemset(ctx->epoch, 0, sizeof(uint32_t)));
     ctx->cap = cap;
     return LVBH_OK;
 }
@@ -159,7 +177,7 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
                     control_bytes(n) - offsetof(Control, err), s);
     if (!hb.use) launch_bounds(tri, n, ctx->ctl, s);
     if (profile) cudaEventRecord(ctx->ev[2], s);
-    launch_morton(tri, n, hb, ctx->ctl, out->morton, s);
+    launch_morton(tri, n, hb, ctx->ctl, out->morton, ctx->epoch, s);
     if (profile) cudaEventRecord(ctx->ev[3], s);
     // ping-pong so that the last pass lands in the result buffers
     launch_onesweep(out->morton, nullptr, ctx->keys_b, ctx->vals_b, n, 0, ctx->ctl, ctx->lookback, s);
@@ -167,13 +185,10 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
     launch_onesweep(out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, n, 2, ctx->ctl, ctx->lookback, s);
     launch_onesweep(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 3, ctx->ctl, ctx->lookback, s);
     if (profile) cudaEventRecord(ctx->ev[4], s);
-    if (n == 1) cudaMemsetAsync(out->parents, 0, 2 * sizeof(int32_t), s);
-    launch_tree(out->morton, n, out->parents, ctx->epoch, s);
+    launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
+                static_cast<float4 *>(out->nodes), out->parents, ctx->lbox, ctx->items, ctx->counts,
+                ctx->arrive, ctx->pend, ctx->epoch, ctx->ctl, s);
     if (profile) cudaEventRecord(ctx->ev[5], s);
-    launch_refit(tri, out->leaf_index, out->morton, out->parents, n,
-                 static_cast<float4 *>(out->tris), static_cast<float4 *>(out->nodes), ctx->arrive,
-                 ctx->epoch, ctx->ctl, s);
-    if (profile) cudaEventRecord(ctx->ev[6], s);
 }
 
 int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
@@ -307,6 +322,7 @@ int lvbh_create(lvbh_ctx **out, const lvbh_config *cfg) {
     for (auto &e : ctx->ev) {
         if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); lvbh_destroy(ctx); return LVBH_ECUDA; }
     }
+    if (emit_init() != cudaSuccess) { cudaGetLastError(); lvbh_destroy(ctx); return LVBH_ECUDA; }
     if (cfg && cfg->reserve_tris) {
         if (cfg->reserve_tris > LVBH_MAX_TRIS) { lvbh_destroy(ctx); return LVBH_EINVAL; }
         if (int rc = ensure_arena(ctx, cfg->reserve_tris)) { lvbh_destroy(ctx); return rc; }
@@ -460,8 +476,7 @@ int lvbh_stage_times(lvbh_ctx *ctx, float *ms_out) {
 }
 
 size_t lvbh_scratch_bytes(uint32_t num_tris) {
-    const uint32_t cap = num_tris < 4096 ? 4096 : num_tris;
-    return 3 * align_up((size_t)cap * 4) + align_up(sizeof(uint32_t)) + control_bytes(cap);
+    return arena_bytes(num_tris < 4096 ? 4096 : num_tris);
 }
 
 const char *lvbh_last_error(const lvbh_ctx *ctx) {

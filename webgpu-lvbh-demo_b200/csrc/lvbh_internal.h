@@ -18,6 +18,19 @@ constexpr int kSortTile = kSortThreads * kSortItems; // keys per tile (4096)
 
 inline uint32_t sort_tiles(uint32_t n) { return (n + kSortTile - 1) / kSortTile; }
 
+// Tree/refit pass: leaves per block of the in-block tree pass (one thread each); open nodes a
+// block can leave to the straddling pass (at most 2 x the tree depth 64).
+constexpr int kEmitBlock = 256;
+constexpr int kOpenCap = 128;
+
+// A complete subtree handed from one level of the tree pass to the next: box min + link,
+// box max + the separator d after it, and its leaf range.
+struct __align__(16) OpenItem {
+    float4 lo;
+    float4 hi;
+    int xl, xr, pad0, pad1;
+};
+
 // Per-build control block in device memory.  Everything from `err` on is zeroed by one memset
 // at the start of a build; `aux_err` collects errors of steps that run before that memset (the
 // indexed-mesh gather) and is cleared by the host before them.
@@ -41,20 +54,23 @@ int sm_count();
 // K1a: scene box over every vertex of the 48-byte triangle soup.
 void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s);
 // K1b: triangle box centroid -> Morton key (input order) + the four digit histograms; flags
-// non-finite vertices in ctl->err.
+// non-finite vertices in ctl->err and advances the build epoch *epoch used by K3c.
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl,
-                   uint32_t *keys_out, cudaStream_t s);
+                   uint32_t *keys_out, uint32_t *epoch, cudaStream_t s);
 // K2: one onesweep pass over digit `pass`.  vals_in == nullptr generates the identity.
 void launch_onesweep(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
                      uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *lookback,
                      cudaStream_t s);
-// K3: Karras radix tree -> parent links (2N).
-void launch_tree(const uint32_t *keys, uint32_t n, int32_t *parents, uint32_t *epoch,
-                 cudaStream_t s);
-// K4: leaf gather + rearrange + bottom-up refit -> BVH nodes.
-void launch_refit(const float4 *tri, const uint32_t *perm, const uint32_t *keys,
-                  const int32_t *parents, uint32_t n, float4 *otri, float4 *nodes,
-                  uint32_t *arrive, const uint32_t *epoch, Control *ctl, cudaStream_t s);
+// K3: leaf gather + rearrange (K3a), in-block radix tree + refit (K3b), straddling nodes (K3c)
+// -> BVH nodes, parent links, sorted triangles.  Scratch: lbox (3 float2 per triangle),
+// items (emit_groups(n) * kOpenCap) and counts (emit_groups(n)), arrive (n words, zero or
+// older epochs), pend (2n float4); *epoch is this build's epoch (advanced by K1b).
+size_t emit_groups(uint32_t n);
+cudaError_t emit_init();  // once per device, before the first launch
+void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
+                 float4 *otri, float4 *nodes, int32_t *parents, float2 *lbox, OpenItem *items,
+                 uint32_t *counts, uint32_t *arrive, float4 *pend, const uint32_t *epoch,
+                 Control *ctl, cudaStream_t s);
 // Indexed mesh -> 48-byte soup (pad 0).  An index >= num_verts sets ERR_BAD_INDEX in
 // *err and gathers zeros instead of reading out of bounds.
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,

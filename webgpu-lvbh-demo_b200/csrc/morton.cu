@@ -72,8 +72,13 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const float4 *__restrict__ 
 // the digit histograms of all four sort passes are accumulated on the way.
 __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ tri, uint32_t n,
                                                      HostBounds hb, Control *__restrict__ ctl,
-                                                     uint32_t *__restrict__ keys) {
+                                                     uint32_t *__restrict__ keys,
+                                                     uint32_t *__restrict__ epoch) {
     __shared__ float4 stage[kWarps][96];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
+        const uint32_t e = *epoch + 1u;
+        *epoch = e == 0u ? 1u : e;
+    }
     __shared__ uint32_t hist[kSortPasses][kDigits];
     for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) (&hist[0][0])[i] = 0;
 
@@ -157,13 +162,13 @@ void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s) 
 }
 
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl, uint32_t *keys,
-                   cudaStream_t s) {
+                   uint32_t *epoch, cudaStream_t s) {
     const uint64_t chunks = (n + 31) / 32;
     uint64_t blocks = (chunks + kWarps - 1) / kWarps;
     const uint64_t cap = (uint64_t)sm_count() * 8;
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
-    k_morton<<<(unsigned)blocks, kThreads, 0, s>>>(tri, n, hb, ctl, keys);
+    k_morton<<<(unsigned)blocks, kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch);
 }
 
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,

@@ -33,6 +33,7 @@ constexpr int IPT = kSortItems;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1u;
+constexpr int kLookback = 8;  // predecessor tiles read per look-back step
 
 static_assert(T == kDigits, "one thread per digit in the per-digit phases");
 
@@ -54,7 +55,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s
     return warp_off + incl - x;
 }
 
-__global__ void __launch_bounds__(T) k_onesweep(const uint32_t *__restrict__ keys_in,
+__global__ void __launch_bounds__(T, 4) k_onesweep(const uint32_t *__restrict__ keys_in,
                                                 const uint32_t *__restrict__ vals_in,
                                                 uint32_t *__restrict__ keys_out,
                                                 uint32_t *__restrict__ vals_out, uint32_t n,
@@ -88,7 +89,7 @@ __global__ void __launch_bounds__(T) k_onesweep(const uint32_t *__restrict__ key
     const uint32_t digit_base = block_exclusive_scan(ctl->hist[pass][tid], s_warp);
 
     // Stable in-warp ranking, keys visited in input order (item-major, then lane).
-    uint32_t rank[IPT];
+    uint32_t rank[IPT / 2];  // two 16-bit ranks per word
     const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
@@ -101,7 +102,8 @@ __global__ void __launch_bounds__(T) k_onesweep(const uint32_t *__restrict__ key
         __syncwarp();
         if (valid && lane == 31 - __clz(peers)) s_whist[warp][d] = cnt + __popc(peers);
         __syncwarp();
-        rank[i] = cnt + __popc(peers & lt);
+        const uint32_t rk = cnt + __popc(peers & lt);
+        if (i & 1) rank[i / 2] |= rk << 16; else rank[i / 2] = rk;
     }
     __syncthreads();
 
@@ -114,7 +116,8 @@ __global__ void __launch_bounds__(T) k_onesweep(const uint32_t *__restrict__ key
         tile_count += c;
     }
 
-    // Decoupled look-back across tiles for digit tid.
+    // Decoupled look-back across tiles for digit tid: read kLookback predecessors at a time
+    // (independent loads), then add their counts newest first until a PREFIX is met.
     uint32_t *lb = lookback + (size_t)tile * kDigits + tid;
     uint32_t excl = 0;
     if (tile == 0) {
@@ -122,24 +125,33 @@ __global__ void __launch_bounds__(T) k_onesweep(const uint32_t *__restrict__ key
     } else {
         st_relaxed_gpu(lb, kFlagAgg | tile_count);
         long long t0 = 0;
-        bool timed = false;
-        for (int64_t kk = (int64_t)tile - 1; kk >= 0;) {
-            const uint32_t x = ld_relaxed_gpu(lookback + (size_t)kk * kDigits + tid);
-            const uint32_t flag = x & ~kCountMask;
-            if (flag == 0u) {
-                if (!timed) { t0 = clock64(); timed = true; }
-                else if (clock64() - t0 > kSpinLimitCycles ||
-                         (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT)) {
-                    // give up; once one wait has timed out every other one gives up at once
-                    atomicOr(&ctl->err, ERR_LOOKBACK_TIMEOUT);
-                    break;
-                }
-                __nanosleep(32);
-                continue;
+        bool timed = false, done = false;
+        int64_t kk = (int64_t)tile - 1;  // next predecessor to add
+        while (!done) {
+            uint32_t w[kLookback];
+#pragma unroll
+            for (int i = 0; i < kLookback; ++i)
+                w[i] = kk - i >= 0 ? ld_relaxed_gpu(lookback + (size_t)(kk - i) * kDigits + tid) : kFlagPrefix;
+            bool stalled = false;
+#pragma unroll
+            for (int i = 0; i < kLookback; ++i) {
+                if (done || stalled) continue;
+                const uint32_t flag = w[i] & ~kCountMask;
+                if (flag == 0u) { stalled = true; continue; }
+                excl += w[i] & kCountMask;
+                --kk;
+                if (flag == kFlagPrefix) done = true;
             }
-            excl += x & kCountMask;
-            if (flag == kFlagPrefix) break;
-            --kk;
+            if (kk < 0) done = true;
+            if (done || !stalled) continue;
+            if (!timed) { t0 = clock64(); timed = true; }
+            else if (clock64() - t0 > kSpinLimitCycles ||
+                     (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT)) {
+                // give up; once one wait has timed out every other one gives up at once
+                atomicOr(&ctl->err, ERR_LOOKBACK_TIMEOUT);
+                break;
+            }
+            __nanosleep(20);
         }
         st_relaxed_gpu(lb, kFlagPrefix | ((excl + tile_count) & kCountMask));
     }
@@ -155,7 +167,7 @@ __global__ void __launch_bounds__(T) k_onesweep(const uint32_t *__restrict__ key
         const uint32_t idx = wbase + i * 32 + lane;
         if (idx < n) {
             const uint32_t d = (k[i] >> shift) & (kDigits - 1);
-            const uint32_t pos = s_tile_start[d] + s_whist[warp][d] + rank[i];
+            const uint32_t pos = s_tile_start[d] + s_whist[warp][d] + ((rank[i / 2] >> (16 * (i & 1))) & 0xFFFFu);
             s_keys[pos] = k[i];
             s_vals[pos] = vals_in ? __ldcs(vals_in + idx) : idx;
         }

@@ -19,8 +19,8 @@ STATUS_NAMES = {OK: "LVBH_OK", EINVAL: "LVBH_EINVAL", ENOMEM: "LVBH_ENOMEM",
 # build flags
 INPUT_HOST, ASYNC, OUT_CALLER, PROFILE, NO_GRAPH = 0x1, 0x2, 0x4, 0x8, 0x10
 MAX_TRIS = 1 << 29
-NUM_STAGES = 6
-STAGE_NAMES = ("upload", "bounds", "morton", "sort", "tree", "refit")
+NUM_STAGES = 5
+STAGE_NAMES = ("upload", "bounds", "morton", "sort", "emit")
 
 
 class LvbhError(RuntimeError):
