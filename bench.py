@@ -38,14 +38,15 @@ for _p in (REPO, PKG):
 METRIC = "LBVH build Mprims/s"
 UNIT = "Mprims/s"
 
-# Algorithmic HBM bytes per triangle of each stage (fixed traffic model): bounds read 48;
-# Morton read 48 + key 4; sort 48 (3 LSD passes of 30-bit keys: histogram read 4, pass 1 read 4
-# write 8, passes 2-3 read 8 write 8); emit = tree (keys 4 + parents 8 + child links 8) +
-# refit and rearrange (perm 4 + gather 48 + write 48 + node words 56 + parent reads 8 + flag
-# atomics 8) = 20 + 172.
-MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "emit": 192}
-KERNELS = {"bounds": "k_bounds", "morton": "k_morton", "sort": "k_onesweep x4", "emit": "k_emit"}
-LAUNCHES_PER_BUILD = 7  # bounds, morton, 4 onesweep passes, emit
+# Algorithmic HBM bytes per triangle of each stage (fixed traffic model, 340 B in all): bounds
+# read 48; Morton read 48 + key 4; sort 48 (3 LSD passes of 30-bit keys: histogram read 4,
+# pass 1 read 4 write 8, passes 2-3 read 8 write 8); leaf gather perm 4 + gather 48 + write 48;
+# tree keys 4 + parents 8 + child links 8 + node words 56 + parent reads 8 + flag atomics 8.
+# The straddling-node pass completes part of the same tree and has no bytes of its own.
+MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "gather": 100, "tree": 92, "top": 0}
+KERNELS = {"bounds": ("k_bounds", 1), "morton": ("k_morton", 1), "sort": ("k_onesweep", 4),
+           "gather": ("k_leaf_gather", 1), "tree": ("k_tree_leaves", 1), "top": ("k_emit_top", 1)}
+LAUNCHES_PER_BUILD = 9  # bounds, morton, 4 onesweep passes, gather, tree, top
 MODEL_TOTAL = sum(MODEL_BYTES.values())  # 340 B per triangle
 
 
@@ -283,11 +284,14 @@ def run_ours(args, world, rank, local):
         for k, v in res.stage_ms.items():
             stages[k].append(v)
     stage_ms = {k: statistics.mean(v) for k, v in stages.items() if k != "upload"}
-    dom = max(MODEL_BYTES, key=lambda k: stage_ms[k])
-    dom_bytes = MODEL_BYTES[dom] * n
-    achieved = dom_bytes / (stage_ms[dom] * 1e-3) / 1e9
-    traffic = load_traffic(dom, n)
-    roofline = {"bound": "hbm", "kernel": KERNELS[dom],
+    # the dominant kernel: the longest single launch with bytes of its own
+    dom = max((k for k in MODEL_BYTES if MODEL_BYTES[k]), key=lambda k: stage_ms[k] / KERNELS[k][1])
+    kname, launches = KERNELS[dom]
+    launch_ms = stage_ms[dom] / launches
+    dom_bytes = MODEL_BYTES[dom] * n / launches
+    achieved = dom_bytes / (launch_ms * 1e-3) / 1e9
+    traffic = load_traffic(kname, n)
+    roofline = {"bound": "hbm", "kernel": kname, "launch_ms": launch_ms,
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes": dom_bytes,
@@ -334,13 +338,13 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
-def load_traffic(stage: str, n: int):
-    """dram read+write bytes per launch of the stage's kernel from the committed ncu summary
-    (profiles/traffic.json, scaled to n triangles), or None."""
+def load_traffic(kernel: str, n: int):
+    """dram read + write bytes per launch of `kernel` from the committed ncu capture summary
+    (profiles/traffic.json: bytes per triangle, scaled to n triangles), or None."""
     try:
         with open(os.path.join(REPO, "profiles", "traffic.json")) as f:
-            t = json.load(f)[stage]
-        return t["bytes_per_tri"] * n
+            t = json.load(f)["kernels"][kernel]
+        return t["dram_bytes_per_tri"] * n
     except Exception:
         return None
 

@@ -83,8 +83,10 @@ extern "C" {
 #define LVBH_STAGE_BOUNDS  1  /* scene box reduction (skipped when bounds are supplied) */
 #define LVBH_STAGE_MORTON  2  /* triangle centroid -> 30-bit Morton key + digit histograms */
 #define LVBH_STAGE_SORT    3  /* onesweep stable radix sort of (key, triangle index) */
-#define LVBH_STAGE_EMIT    4  /* radix tree + leaf gather + triangle rearrange + box refit */
-#define LVBH_NUM_STAGES    5
+#define LVBH_STAGE_GATHER  4  /* leaf gather: sorted triangle rearrange + leaf boxes */
+#define LVBH_STAGE_TREE    5  /* radix tree + box refit of every node inside a 256-leaf block */
+#define LVBH_STAGE_TOP     6  /* radix tree + box refit of the nodes that straddle blocks */
+#define LVBH_NUM_STAGES    7
 
 typedef struct lvbh_ctx lvbh_ctx;
 
@@ -145,6 +147,11 @@ LVBH_API int  lvbh_release(lvbh_ctx *ctx, lvbh_result *res);
 /* Per-stage device times (ms) of the last build made with LVBH_PROFILE, LVBH_NUM_STAGES
  * entries, after lvbh_sync(). */
 LVBH_API int  lvbh_stage_times(lvbh_ctx *ctx, float *ms_out);
+
+/* Copies `bytes` from device memory of the context's device to host memory and waits (for FFI
+ * callers that do not link the CUDA runtime themselves).  stream: cudaStream_t or NULL. */
+LVBH_API int  lvbh_copy_to_host(lvbh_ctx *ctx, void *dst_host, const void *src_device, size_t bytes,
+                                void *stream);
 
 /* Bytes of device scratch a build of `num_tris` triangles needs beyond its inputs/outputs. */
 LVBH_API size_t lvbh_scratch_bytes(uint32_t num_tris);

@@ -23,6 +23,7 @@ int main(void) {
     printf("create_null %d\n", lvbh_create(NULL, NULL));
     printf("stage_null %d\n", lvbh_stage_times(NULL, NULL));
     printf("trace_null %d\n", lvbh_trace(NULL, NULL, NULL, 0, NULL, 0, NULL, NULL, NULL, NULL));
+    printf("copy_null %d\n", lvbh_copy_to_host(NULL, NULL, NULL, 0, NULL));
     printf("last_error_null %s\n", lvbh_last_error(NULL));
     printf("scratch_1M %zu\n", lvbh_scratch_bytes(1u << 20));
     return 0;

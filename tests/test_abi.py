@@ -51,7 +51,7 @@ def test_c_header_layout_and_host_errors(tmp_path):
     assert int(kv["sizeof_config"]) == ctypes.sizeof(nat.Config)
     assert "sm_100a" in kv["version"]
     for k in ("build_null_ctx", "indexed_null_ctx", "sync_null", "release_null", "create_null",
-              "stage_null", "trace_null"):
+              "stage_null", "trace_null", "copy_null"):
         assert int(kv[k]) == nat.EINVAL, k
     assert kv["last_error_null"] == "no context"
     assert int(kv["scratch_1M"]) >= 12 * (1 << 20)

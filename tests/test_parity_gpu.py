@@ -166,7 +166,7 @@ def test_graph_replay_async_and_reuse(builder):
         builder.sync()
         assert_same({k: v.cpu().numpy() for k, v in outs.items()}, ref, "replay")
     res = builder.build_soup(dtri, None, graph=False, profile=True)
-    assert set(res.stage_ms) == {"upload", "bounds", "morton", "sort", "emit"}
+    assert set(res.stage_ms) == {"upload", "bounds", "morton", "sort", "gather", "tree", "top"}
     assert_same(res.to_numpy(), ref, "profiled")
     big = scenes.uniform_soup(300_000, seed=7)
     _, got = build_np(builder, big)

@@ -187,8 +187,7 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
     if (profile) cudaEventRecord(ctx->ev[4], s);
     launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
                 static_cast<float4 *>(out->nodes), out->parents, ctx->lbox, ctx->items, ctx->counts,
-                ctx->arrive, ctx->pend, ctx->epoch, ctx->ctl, s);
-    if (profile) cudaEventRecord(ctx->ev[5], s);
+                ctx->arrive, ctx->pend, ctx->epoch, ctx->ctl, s, profile ? ctx->ev + 5 : nullptr);
 }
 
 int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
@@ -472,6 +471,18 @@ int lvbh_stage_times(lvbh_ctx *ctx, float *ms_out) {
         if (e != cudaSuccess) { cudaGetLastError(); ms = 0.0f; }
         ms_out[i] = ms;
     }
+    return LVBH_OK;
+}
+
+int lvbh_copy_to_host(lvbh_ctx *ctx, void *dst_host, const void *src_device, size_t bytes,
+                      void *stream) {
+    if (!ctx) return LVBH_EINVAL;
+    if (bytes && (!dst_host || !src_device)) return fail(ctx, LVBH_EINVAL, "NULL copy pointer");
+    if (!bytes) return LVBH_OK;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    LVBH_CUDA(ctx, cudaMemcpyAsync(dst_host, src_device, bytes, cudaMemcpyDeviceToHost, s));
+    LVBH_CUDA(ctx, cudaStreamSynchronize(s));
     return LVBH_OK;
 }
 

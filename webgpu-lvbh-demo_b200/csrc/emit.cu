@@ -16,25 +16,22 @@
 // record follows from nearest-smaller-value queries on d alone: no per-node binary search,
 // no climbing, no atomics.
 //
-// Groups.  The work is cut into groups of consecutive "items" (disjoint, ordered leaf ranges
-// that are already complete subtrees) that one CTA holds in shared memory; the separators
-// between items are the d values at their ends.  Inside a group:
-//   1. nearest-smaller queries use, per 32 separators, a bitmask of those below each of the
-//      65 possible values (built with __ballot_sync): a query reads one or a few words;
-//   2. a split is local when both nearest smaller separators lie inside the group; its node
-//      range, Karras index and children follow at once;
-//   3. boxes are filled bottom-up in rounds separated by __syncthreads: a node is done in the
-//      first round in which both children are done; it writes its 64-byte record, its
-//      children's parent links and its merged box (into the shared-memory slot of its own
-//      index, where its parent will read it);
-//   4. nodes whose parent split is not local ("open") leave the group in leaf order as items
-//      of the next level.
-// Level 1 (k_emit_leaves) has one leaf per item - each thread gathers triangle perm[k]
-// (3 x 16-byte loads), writes it to the output soup at k and takes the leaf box (exact-zero
-// components nudged by 1e-8 as bvh-up-pass.js:209-210 does).  Levels >= 2 (k_emit_merge)
-// take the open items of kMergeGroups consecutive groups of the level below; the last level
-// holds everything left and completes the root.  A group leaves at most 2 x 64 open items
-// (they hang off the two boundary paths of a tree at most 64 deep), so buffers are fixed.
+// Passes.
+//   K3a (k_leaf_gather)  one thread per sorted leaf k: gathers triangle perm[k] (3 x 16-byte
+//                        loads), writes it to the output soup at k, and writes its box (exact-
+//                        zero components nudged by 1e-8 as bvh-up-pass.js:209-210 does) to a
+//                        24-byte scratch record.  Random-access bound.
+//   K3b (k_tree_leaves)  blocks of 256 sorted leaves, one thread per leaf / split, a persistent
+//                        grid that prefetches the next block.  Two sparse tables in shared
+//                        memory - minima of d, unions of leaf boxes - give every split its
+//                        nearest smaller separators by binary lifting and its children's boxes
+//                        by two O(1) range queries, so every node whose range stays inside the
+//                        block is completed at once (record and parent links staged in shared
+//                        memory and written coalesced).  A node or leaf whose parent split is
+//                        not inside the block leaves it as an "open item" (at most 2 x 64 per
+//                        block: they hang off the two boundary paths of a tree at most 64 deep).
+//   K3c (k_emit_top)     the nodes that straddle blocks (~3 % of them), built bottom-up from
+//                        the open items with arrival words (see below).
 #include "lvbh_device.cuh"
 #include "lvbh_internal.h"
 
@@ -394,17 +391,20 @@ cudaError_t emit_init() {
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
                  float4 *otri, float4 *nodes, int32_t *parents, float2 *lbox, OpenItem *items,
                  uint32_t *counts, uint32_t *arrive, float4 *pend, const uint32_t *epoch,
-                 Control *ctl, cudaStream_t s) {
+                 Control *ctl, cudaStream_t s, cudaEvent_t *ev) {
     if (n == 0) return;
     k_leaf_gather<<<(n + 255) / 256, 256, 0, s>>>(tri, perm, (int)n, otri, lbox, ctl);
+    if (ev) cudaEventRecord(ev[0], s);
     const int groups = (int)emit_groups(n);
     const int grid = min(groups, sm_count() * kTreeCtasPerSm);
     k_tree_leaves<<<grid, EB, leaves_smem_bytes(), s>>>(keys, lbox, (int)n, nodes, parents, items,
                                                          counts, ctl);
+    if (ev) cudaEventRecord(ev[1], s);
     if (groups > 1)
         k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(items, counts, groups, keys,
                                                                      (int)n, nodes, parents, arrive,
                                                                      pend, epoch, ctl);
+    if (ev) cudaEventRecord(ev[2], s);
 }
 
 }  // namespace lvbh

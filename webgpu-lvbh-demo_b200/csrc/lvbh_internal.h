@@ -67,10 +67,11 @@ void launch_onesweep(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t 
 // older epochs), pend (2n float4); *epoch is this build's epoch (advanced by K1b).
 size_t emit_groups(uint32_t n);
 cudaError_t emit_init();  // once per device, before the first launch
+// ev (may be nullptr): three events recorded after K3a, K3b and K3c.
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
                  float4 *otri, float4 *nodes, int32_t *parents, float2 *lbox, OpenItem *items,
                  uint32_t *counts, uint32_t *arrive, float4 *pend, const uint32_t *epoch,
-                 Control *ctl, cudaStream_t s);
+                 Control *ctl, cudaStream_t s, cudaEvent_t *ev);
 // Indexed mesh -> 48-byte soup (pad 0).  An index >= num_verts sets ERR_BAD_INDEX in
 // *err and gathers zeros instead of reading out of bounds.
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,

@@ -19,8 +19,8 @@ STATUS_NAMES = {OK: "LVBH_OK", EINVAL: "LVBH_EINVAL", ENOMEM: "LVBH_ENOMEM",
 # build flags
 INPUT_HOST, ASYNC, OUT_CALLER, PROFILE, NO_GRAPH = 0x1, 0x2, 0x4, 0x8, 0x10
 MAX_TRIS = 1 << 29
-NUM_STAGES = 5
-STAGE_NAMES = ("upload", "bounds", "morton", "sort", "emit")
+NUM_STAGES = 7
+STAGE_NAMES = ("upload", "bounds", "morton", "sort", "gather", "tree", "top")
 
 
 class LvbhError(RuntimeError):
@@ -70,6 +70,8 @@ def _load():
     L.lvbh_scratch_bytes.argtypes = [u32]
     L.lvbh_last_error.restype = ctypes.c_char_p
     L.lvbh_last_error.argtypes = [vp]
+    L.lvbh_copy_to_host.restype = i32
+    L.lvbh_copy_to_host.argtypes = [vp, vp, vp, ctypes.c_size_t, vp]
     L.lvbh_trace.restype = i32
     L.lvbh_trace.argtypes = [vp, vp, vp, u32, vp, u32, vp, vp, vp, vp]
     return L
