@@ -65,6 +65,7 @@ extern "C" {
 #define LVBH_ECUDA     4  /* a CUDA runtime call failed; lvbh_last_error() has the text */
 #define LVBH_EBUSY     5  /* serving: queue full / request not finished yet */
 #define LVBH_EDEVICE   6  /* a kernel reported an inconsistent structure (bounded climb exceeded) */
+#define LVBH_ERANGE    7  /* a size beyond a fixed capacity (lvbh_sort_pairs_noalloc) */
 
 /* ---- build flags ------------------------------------------------------------------- */
 #define LVBH_INPUT_HOST    0x1u  /* input pointers are host memory: copied to the device inside the call */
@@ -160,6 +161,26 @@ LVBH_API size_t lvbh_scratch_bytes(uint32_t num_tris);
 LVBH_API const char *lvbh_last_error(const lvbh_ctx *ctx);
 /* Library version string. */
 LVBH_API const char *lvbh_version(void);
+
+/* ---- allocation-free sort -------------------------------------------------------------
+ * No counterpart in the reference.  The build's stable radix sort of (key, index), for callers
+ * that cannot allocate device memory when they need it: a render or serving loop that must not
+ * stall (cudaMalloc / cudaFree synchronise the device), a process whose whole memory budget is
+ * already reserved by its own pool, or a plugin host that owns every device allocation.
+ *   keys_in   num_keys uint32 keys, device memory (not modified)
+ *   keys_out  num_keys sorted keys; perm_out num_keys input indices (ties keep input order)
+ *   stream    cudaStream_t or NULL; the call returns once the sort has finished
+ * All other memory (ping-pong keys and values, histograms, look-back words, error word) is one
+ * file-scope device array inside the library, sized for LVBH_NOALLOC_MAX_KEYS keys (about
+ * 9.5 MB, held by every GPU that loads the library until the process exits); larger inputs are
+ * rejected with LVBH_ERANGE before any GPU work.  The first call on each device looks up that
+ * array's device address (cudaGetSymbolAddress, with the device current); make it before any
+ * stream capture.  Calls share the array: two calls that overlap on the GPU (unordered
+ * streams, or threads) race.  Calls no cudaMalloc, cudaFree or allocating routine.
+ * Returns LVBH_OK, LVBH_ERANGE, LVBH_EINVAL (NULL pointer), LVBH_ETIMEOUT or LVBH_ECUDA. */
+#define LVBH_NOALLOC_MAX_KEYS ((uint32_t)1 << 20)
+LVBH_API int  lvbh_sort_pairs_noalloc(const uint32_t *keys_in, uint32_t num_keys,
+                                      uint32_t *keys_out, uint32_t *perm_out, void *stream);
 
 /* ---- validation consumer: closest-hit traversal ------------------------------------
  * Restates intersect_bvh / aabb_intersect / tri_intersect of scripts/pathtracer/pathtracer.js

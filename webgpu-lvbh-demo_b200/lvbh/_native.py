@@ -11,10 +11,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblvbh.so")
 
 # status codes (include/lvbh.h)
-OK, EINVAL, ENOMEM, ETIMEOUT, ECUDA, EBUSY, EDEVICE = 0, 1, 2, 3, 4, 5, 6
+OK, EINVAL, ENOMEM, ETIMEOUT, ECUDA, EBUSY, EDEVICE, ERANGE = 0, 1, 2, 3, 4, 5, 6, 7
 STATUS_NAMES = {OK: "LVBH_OK", EINVAL: "LVBH_EINVAL", ENOMEM: "LVBH_ENOMEM",
                 ETIMEOUT: "LVBH_ETIMEOUT", ECUDA: "LVBH_ECUDA", EBUSY: "LVBH_EBUSY",
-                EDEVICE: "LVBH_EDEVICE"}
+                EDEVICE: "LVBH_EDEVICE", ERANGE: "LVBH_ERANGE"}
+NOALLOC_MAX_KEYS = 1 << 20
 
 # build flags
 INPUT_HOST, ASYNC, OUT_CALLER, PROFILE, NO_GRAPH = 0x1, 0x2, 0x4, 0x8, 0x10
@@ -72,6 +73,8 @@ def _load():
     L.lvbh_last_error.argtypes = [vp]
     L.lvbh_copy_to_host.restype = i32
     L.lvbh_copy_to_host.argtypes = [vp, vp, vp, ctypes.c_size_t, vp]
+    L.lvbh_sort_pairs_noalloc.restype = i32
+    L.lvbh_sort_pairs_noalloc.argtypes = [vp, u32, vp, vp, vp]
     L.lvbh_trace.restype = i32
     L.lvbh_trace.argtypes = [vp, vp, vp, u32, vp, u32, vp, vp, vp, vp]
     return L
