@@ -338,6 +338,123 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, world, rank, local, clocks=None):
+    """The 4096-mesh batch: one lvbh_build_batched call vs the plain builder called once per
+    mesh (lvbh_build_soup through the C ABI, argument structs prepared outside the timed
+    region, no host wait between meshes).  Returns a dict for the JSON line."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import lvbh
+    from lvbh import _native, empty_outputs, scenes
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    count = args.batch_meshes
+    t_gen = time.perf_counter()
+    tri, offs = scenes.mesh_batch(count=count, seed=3)
+    t_gen = time.perf_counter() - t_gen
+    n = int(offs[-1])
+    sizes = np.diff(offs)
+    builder = lvbh.BVHBuilder(local, reserve_tris=int(sizes.max()))
+    stream = torch.cuda.Stream(dev)
+    dtri = torch.from_numpy(tri).to(dev)
+    outs = empty_outputs(n, dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def batched(profile=False, sync=False, graph=True, o=outs):
+        return builder.build_batched(dtri, offs, outputs=o, stream=stream, sync=sync,
+                                     profile=profile, graph=graph)
+
+    for _ in range(args.warmup):
+        batched(sync=True)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        batched()
+    ev1.record(stream)
+    builder.sync()
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+    stages = {k: [] for k in lvbh.STAGE_NAMES}
+    for _ in range(min(args.steps, 5)):
+        r = batched(profile=True, sync=True)
+        for k, v in r.stage_ms.items():
+            stages[k].append(v)
+    stage_ms = {k: statistics.mean(v) for k, v in stages.items() if k != "upload"}
+
+    # the plain builder once per mesh, into a second set of outputs
+    outs_b = empty_outputs(n, dev)
+    L, ctx = _native.lib, builder.ctx
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    calls = []
+    for i in range(count):
+        a, b = int(offs[i]), int(offs[i + 1])
+        r = _native.Result()
+        r.num_tris = r.num_nodes = b - a
+        if b > a:
+            r.nodes = outs_b["nodes"][a].data_ptr()
+            r.tris = outs_b["tris"][a].data_ptr()
+            r.parents = outs_b["parents"][2 * a].data_ptr()
+            r.leaf_index = outs_b["leaf_index"][a].data_ptr()
+            r.morton = outs_b["morton"][a].data_ptr()
+        calls.append((ctypes.c_void_p(dtri[a].data_ptr() if b > a else 0), b - a, r))
+
+    def per_mesh(graph):
+        flags = _native.OUT_CALLER | _native.ASYNC | (0 if graph else _native.NO_GRAPH)
+        for p, m, r in calls:
+            rc = L.lvbh_build_soup(ctx, p, m, None, flags, ctypes.byref(r), sp)
+            if rc:
+                _native.check(ctx, rc)
+        _native.check(ctx, L.lvbh_sync(ctx))
+
+    loop = {}
+    for graph in (False, True):
+        per_mesh(graph)  # warm-up
+        torch.cuda.synchronize(dev)
+        reps = 2
+        ev0.record(stream)
+        for _ in range(reps):
+            per_mesh(graph)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        loop["graph" if graph else "no_graph"] = ev0.elapsed_time(ev1) / reps
+    base_ms = max_over_ranks(min(loop.values()), world)
+    identical = all(torch.equal(outs[k], outs_b[k]) for k in outs)
+
+    # end to end: pinned host soup in, every mesh's root record out, each step
+    htri = torch.from_numpy(tri).pin_memory()
+    roots = torch.empty((count, 16), dtype=torch.int32).pin_memory()
+    root_idx = torch.from_numpy(offs[:-1][sizes > 0]).to(dev)
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        builder.build_batched(htri.numpy(), offs, outputs=outs, stream=stream, sync=True)
+        with torch.cuda.stream(stream):
+            roots[: root_idx.numel()].copy_(outs["nodes"].index_select(0, root_idx), non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e = max_over_ranks(statistics.mean(e2e_ms), world)
+    builder.close()
+    return {"workload": f"mesh_batch_{count}", "meshes": count, "num_tris": n,
+            "mesh_tris": {"min": int(sizes.min()), "max": int(sizes.max()), "mean": float(sizes.mean())},
+            "ms_per_batch": ms, "builds_per_s": world * count / (ms * 1e-3),
+            "mprims_per_s": world * n / (ms * 1e-3) / 1e6,
+            "per_mesh_loop_ms": loop, "per_mesh_builds_per_s": world * count / (base_ms * 1e-3),
+            "speedup_vs_per_mesh": base_ms / ms, "identical_trees": bool(identical),
+            "stage_ms": stage_ms, "launches_per_batch": 11,
+            "e2e": {"value": world * n / (e2e * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": e2e,
+                    "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 64 * int(root_idx.numel())},
+            "generate_s": round(t_gen, 1)}
+
+
 def load_traffic(kernel: str, n: int):
     """dram read + write bytes per launch of `kernel` from the committed ncu capture summary
     (profiles/traffic.json: bytes per triangle, scaled to n triangles), or None."""
@@ -357,6 +474,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="clustered16M")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-meshes", type=int, default=4096)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -364,6 +482,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "batch":
+            out = run_batched(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(out), flush=True)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -137,6 +137,29 @@ LVBH_API int  lvbh_build_indexed(lvbh_ctx *ctx, const float *xyz, uint32_t num_v
                         const uint32_t *idx3, uint32_t num_tris, const float *model_bounds,
                         uint32_t flags, lvbh_result *out, void *stream);
 
+/* Batched build: num_segs independent meshes laid end to end in one triangle soup, built in
+ * one stream-ordered launch sequence (replayed as a cached CUDA graph) instead of one
+ * build(TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS) per mesh (scripts/bvh/build-bvh.js:12-66 called
+ * num_segs times).
+ *   tri_array    12 floats per triangle for all meshes (host memory with LVBH_INPUT_HOST).
+ *   seg_offsets  HOST memory, num_segs + 1 entries: mesh s is triangles
+ *                [seg_offsets[s], seg_offsets[s+1]); seg_offsets[0] = 0, non-decreasing,
+ *                total = seg_offsets[num_segs] <= LVBH_MAX_TRIS.  Empty meshes are allowed.
+ *   seg_bounds   HOST memory, 6 floats per mesh used as that mesh's MODEL_BOUNDS, or NULL =
+ *                each mesh's own vertex box reduced on the device.
+ *   bounds_out   HOST memory, 6 floats per mesh receiving the bounds each mesh was quantised
+ *                with (written when the build completes: at lvbh_sync with LVBH_ASYNC), or NULL.
+ *   out          total-sized result.  Mesh s (n_s triangles from o_s = seg_offsets[s]) owns
+ *                node records and sorted triangles [o_s, o_s + n_s), parents entries
+ *                [2 o_s, 2 o_s + 2 n_s) and leaf_index / morton entries [o_s, o_s + n_s); every
+ *                index inside them is local to the mesh, so each slice is bit-identical to
+ *                lvbh_build_soup of that mesh alone and is a BVH_BUFFER / O_TRIANGLE_BUFFER of
+ *                its own.  out->bounds is zeroed.
+ * Flags, stream and synchronisation as for lvbh_build_soup. */
+LVBH_API int  lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *seg_offsets,
+                        uint32_t num_segs, const float *seg_bounds, float *bounds_out,
+                        uint32_t flags, lvbh_result *out, void *stream);
+
 /* Waits for the context's last build and returns its device-side status (LVBH_OK,
  * LVBH_EINVAL for non-finite vertices, LVBH_ETIMEOUT, LVBH_EDEVICE).  Fills out->bounds
  * of the result passed to that build when it is still reachable. */

@@ -58,6 +58,14 @@ struct GraphKey {
     bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
 
+struct BatchKey {
+    const void *tri = nullptr;
+    uint32_t total = 0, num_segs = 0, tiles = 0, blocks = 0;
+    int use_bounds = 0;
+    void *outs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool operator==(const BatchKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
+};
+
 }  // namespace
 
 struct lvbh_ctx {
@@ -84,11 +92,32 @@ struct lvbh_ctx {
     cudaStream_t cap_stream = nullptr;
     GraphKey gkey;
     cudaGraphExec_t gexec = nullptr;
+    // batched builds: segment table, per-segment bounds and histograms, look-back words and
+    // open items (device), and a pinned mirror of the table, host bounds and reduced bounds
+    uint32_t b_segs = 0, b_tiles = 0, b_blocks = 0;  // capacity
+    void *b_dev = nullptr;
+    SegRow *b_rows = nullptr;
+    uint32_t *b_tile_seg = nullptr, *b_blk_seg = nullptr;
+    uint32_t *b_zero = nullptr;  // seg_ord, seg_hist and look-back words, zeroed per build
+    size_t b_zero_bytes = 0;
+    uint32_t *b_ord = nullptr, *b_hist = nullptr, *b_lookback = nullptr;
+    float *b_bounds = nullptr;
+    OpenItem *b_items = nullptr;
+    uint32_t *b_counts = nullptr;
+    void *b_host = nullptr;
+    SegRow *bh_rows = nullptr;
+    float *bh_bounds = nullptr;
+    uint32_t *bh_ord = nullptr;
+    BatchKey bkey;
+    cudaGraphExec_t bgexec = nullptr;
     // last build, for lvbh_sync
     cudaStream_t last_stream = nullptr;
     lvbh_result *last_out = nullptr;
     HostBounds last_hb{};
     bool pending = false;
+    bool last_batch = false;
+    uint32_t last_segs = 0;
+    float *last_bounds_out = nullptr;
 };
 
 namespace {
@@ -124,9 +153,64 @@ int cuda_fail(lvbh_ctx *ctx, cudaError_t e, const char *what) {
 
 void free_arena(lvbh_ctx *ctx) {
     if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    if (ctx->bgexec) { cudaGraphExecDestroy(ctx->bgexec); ctx->bgexec = nullptr; }
     if (ctx->arena) cudaFree(ctx->arena);
     ctx->arena = nullptr;
     ctx->cap = 0;
+}
+
+void free_batch(lvbh_ctx *ctx) {
+    if (ctx->bgexec) { cudaGraphExecDestroy(ctx->bgexec); ctx->bgexec = nullptr; }
+    if (ctx->b_dev) cudaFree(ctx->b_dev);
+    if (ctx->b_host) cudaFreeHost(ctx->b_host);
+    ctx->b_dev = ctx->b_host = nullptr;
+    ctx->b_segs = ctx->b_tiles = ctx->b_blocks = 0;
+}
+
+// Batch scratch for up to `segs` segments, `tiles` sort tiles and `blocks` tree blocks.
+int ensure_batch(lvbh_ctx *ctx, uint32_t segs, uint32_t tiles, uint32_t blocks) {
+    if (ctx->b_dev && segs <= ctx->b_segs && tiles <= ctx->b_tiles && blocks <= ctx->b_blocks)
+        return LVBH_OK;
+    if (ctx->pending) cudaStreamSynchronize(ctx->last_stream);
+    segs = segs > ctx->b_segs ? segs : ctx->b_segs;
+    tiles = tiles > ctx->b_tiles ? tiles : ctx->b_tiles;
+    blocks = blocks > ctx->b_blocks ? blocks : ctx->b_blocks;
+    free_batch(ctx);
+    const size_t rows = align_up((segs + 1ull) * sizeof(SegRow));
+    const size_t ord = (size_t)segs * 6 * 4, hist = (size_t)segs * kSortPasses * kDigits * 4;
+    const size_t lb = (size_t)kSortPasses * tiles * kDigits * 4;
+    const size_t zero = align_up(ord + hist + lb);
+    const size_t bnd = align_up((size_t)segs * 6 * 4);
+    const size_t dev = rows + align_up(tiles * 4ull) + align_up(blocks * 4ull) + zero + bnd +
+                       align_up((size_t)blocks * kOpenCap * sizeof(OpenItem)) + align_up(blocks * 4ull);
+    void *p = nullptr;
+    LVBH_CUDA(ctx, cudaMalloc(&p, dev));
+    void *h = nullptr;
+    const size_t host = rows + bnd + align_up(ord);
+    cudaError_t e = cudaMallocHost(&h, host);
+    if (e != cudaSuccess) { cudaFree(p); return cuda_fail(ctx, e, "cudaMallocHost(batch)"); }
+    char *c = static_cast<char *>(p);
+    ctx->b_dev = p;
+    ctx->b_rows = reinterpret_cast<SegRow *>(c); c += rows;
+    ctx->b_tile_seg = reinterpret_cast<uint32_t *>(c); c += align_up(tiles * 4ull);
+    ctx->b_blk_seg = reinterpret_cast<uint32_t *>(c); c += align_up(blocks * 4ull);
+    ctx->b_zero = reinterpret_cast<uint32_t *>(c);
+    ctx->b_ord = ctx->b_zero;
+    ctx->b_hist = ctx->b_ord + (size_t)segs * 6;
+    ctx->b_lookback = ctx->b_hist + (size_t)segs * kSortPasses * kDigits;
+    c += zero;
+    ctx->b_bounds = reinterpret_cast<float *>(c); c += bnd;
+    ctx->b_items = reinterpret_cast<OpenItem *>(c); c += align_up((size_t)blocks * kOpenCap * sizeof(OpenItem));
+    ctx->b_counts = reinterpret_cast<uint32_t *>(c);
+    char *hc = static_cast<char *>(h);
+    ctx->b_host = h;
+    ctx->bh_rows = reinterpret_cast<SegRow *>(hc); hc += rows;
+    ctx->bh_bounds = reinterpret_cast<float *>(hc); hc += bnd;
+    ctx->bh_ord = reinterpret_cast<uint32_t *>(hc);
+    ctx->b_segs = segs;
+    ctx->b_tiles = tiles;
+    ctx->b_blocks = blocks;
+    return LVBH_OK;
 }
 
 int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
@@ -164,6 +248,7 @@ int ensure_stage(lvbh_ctx *ctx, size_t bytes) {
     ctx->stage = nullptr;
     ctx->stage_bytes = 0;
     if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    if (ctx->bgexec) { cudaGraphExecDestroy(ctx->bgexec); ctx->bgexec = nullptr; }
     LVBH_CUDA(ctx, cudaMalloc(&ctx->stage, bytes));
     ctx->stage_bytes = bytes;
     return LVBH_OK;
@@ -188,6 +273,65 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
     launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
                 static_cast<float4 *>(out->nodes), out->parents, ctx->lbox, ctx->items, ctx->counts,
                 ctx->arrive, ctx->pend, ctx->epoch, ctx->ctl, s, profile ? ctx->ev + 5 : nullptr);
+}
+
+// The batched build: every launch on `s`.  The segment table (and host bounds) are copied from
+// the pinned mirror, so a replayed graph picks up the table of the current call.
+void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool use_bounds,
+                   const lvbh_result *out, cudaStream_t s, bool profile) {
+    if (profile) cudaEventRecord(ctx->ev[1], s);
+    cudaMemcpyAsync(ctx->b_rows, ctx->bh_rows, (bp.num_segs + 1ull) * sizeof(SegRow),
+                    cudaMemcpyHostToDevice, s);
+    if (use_bounds)
+        cudaMemcpyAsync(ctx->b_bounds, ctx->bh_bounds, bp.num_segs * 6ull * sizeof(float),
+                        cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(reinterpret_cast<char *>(ctx->ctl) + offsetof(Control, err), 0,
+                    sizeof(Control) - offsetof(Control, err), s);
+    const uint32_t *zero_end = ctx->b_lookback + (size_t)kSortPasses * bp.tiles * kDigits;
+    cudaMemsetAsync(ctx->b_zero, 0, (zero_end - ctx->b_zero) * sizeof(uint32_t), s);
+    launch_seg_tables(ctx->b_rows, bp.num_segs, ctx->b_tile_seg, ctx->b_blk_seg, s);
+    if (!use_bounds) launch_bounds_batch(bp, tri, ctx->b_ord, s);
+    if (profile) cudaEventRecord(ctx->ev[2], s);
+    launch_morton_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, ctx->b_hist,
+                        ctx->ctl, out->morton, ctx->epoch, s);
+    if (profile) cudaEventRecord(ctx->ev[3], s);
+    launch_onesweep_batch(bp, out->morton, nullptr, ctx->keys_b, ctx->vals_b, 0, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    launch_onesweep_batch(bp, ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, 1, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    launch_onesweep_batch(bp, out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, 2, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    launch_onesweep_batch(bp, ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, 3, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    if (profile) cudaEventRecord(ctx->ev[4], s);
+    launch_emit_batch(bp, tri, out->leaf_index, out->morton, static_cast<float4 *>(out->tris),
+                      static_cast<float4 *>(out->nodes), out->parents, ctx->lbox, ctx->b_items,
+                      ctx->b_counts, ctx->arrive, ctx->pend, ctx->epoch, ctx->ctl, s,
+                      profile ? ctx->ev + 5 : nullptr);
+}
+
+int launch_batch_graph(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool use_bounds,
+                       const lvbh_result *out, cudaStream_t s) {
+    BatchKey key;
+    std::memset(static_cast<void *>(&key), 0, sizeof key);
+    key.tri = tri;
+    key.total = bp.total;
+    key.num_segs = bp.num_segs;
+    key.tiles = bp.tiles;
+    key.blocks = bp.blocks;
+    key.use_bounds = use_bounds;
+    key.outs[0] = out->nodes; key.outs[1] = out->tris; key.outs[2] = out->parents;
+    key.outs[3] = out->leaf_index; key.outs[4] = out->morton;
+    if (!ctx->bgexec || !(key == ctx->bkey)) {
+        if (ctx->bgexec) { cudaGraphExecDestroy(ctx->bgexec); ctx->bgexec = nullptr; }
+        if (!ctx->cap_stream) LVBH_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+        LVBH_CUDA(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_batch(ctx, tri, bp, use_bounds, out, ctx->cap_stream, false);
+        cudaGraph_t g = nullptr;
+        LVBH_CUDA(ctx, cudaStreamEndCapture(ctx->cap_stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&ctx->bgexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { ctx->bgexec = nullptr; return cuda_fail(ctx, e, "cudaGraphInstantiate(batch)"); }
+        ctx->bkey = key;
+    }
+    LVBH_CUDA(ctx, cudaGraphLaunch(ctx->bgexec, s));
+    return LVBH_OK;
 }
 
 int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
@@ -280,9 +424,18 @@ int build_common(lvbh_ctx *ctx, const float4 *tri_dev, uint32_t n, const float *
     ctx->last_stream = s;
     ctx->last_out = out;
     ctx->last_hb = hb;
+    ctx->last_batch = false;
     ctx->pending = true;
     if (flags & LVBH_ASYNC) return LVBH_OK;
     return lvbh_sync(ctx);
+}
+
+// Host inverse of the device's order-preserving float -> uint32 map (ord_lo).
+float ord_word_to_float(uint32_t o) {
+    const uint32_t u = (o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
 }
 
 int check_out(lvbh_ctx *ctx, uint32_t n, uint32_t flags, lvbh_result *out) {
@@ -335,6 +488,7 @@ void lvbh_destroy(lvbh_ctx *ctx) {
     DeviceGuard g(ctx->device);
     if (ctx->pending) cudaStreamSynchronize(ctx->last_stream);
     free_arena(ctx);
+    free_batch(ctx);
     if (ctx->stage) cudaFree(ctx->stage);
     for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
@@ -410,6 +564,88 @@ int lvbh_build_indexed(lvbh_ctx *ctx, const float *xyz, uint32_t num_verts, cons
                         out, s, profile_upload);
 }
 
+int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *seg_offsets,
+                       uint32_t num_segs, const float *seg_bounds, float *bounds_out,
+                       uint32_t flags, lvbh_result *out, void *stream) {
+    if (!ctx) return LVBH_EINVAL;
+    if (!out) return fail(ctx, LVBH_EINVAL, "out is NULL");
+    if (num_segs && !seg_offsets) return fail(ctx, LVBH_EINVAL, "seg_offsets is NULL");
+    if (num_segs > (1u << 24)) return fail(ctx, LVBH_EINVAL, "num_segs exceeds 2^24");
+    if (num_segs && seg_offsets[0] != 0) return fail(ctx, LVBH_EINVAL, "seg_offsets[0] must be 0");
+    uint64_t tiles = 0, blocks = 0;
+    for (uint32_t i = 0; i < num_segs; ++i) {
+        if (seg_offsets[i + 1] < seg_offsets[i]) return fail(ctx, LVBH_EINVAL, "seg_offsets must be non-decreasing");
+        const uint32_t n = seg_offsets[i + 1] - seg_offsets[i];
+        tiles += sort_tiles(n);
+        blocks += emit_groups(n);
+    }
+    const uint32_t total = num_segs ? seg_offsets[num_segs] : 0;
+    if (total > LVBH_MAX_TRIS) return fail(ctx, LVBH_EINVAL, "total triangles exceed LVBH_MAX_TRIS");
+    if (total && !tri_array) return fail(ctx, LVBH_EINVAL, "tri_array is NULL");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (int rc = check_out(ctx, total, flags, out)) return rc;
+    out->num_tris = out->num_nodes = total;
+    std::memset(out->bounds, 0, sizeof out->bounds);
+    if (total == 0) {
+        ctx->pending = false;
+        ctx->ev_valid = false;
+        if (bounds_out && seg_bounds) std::memcpy(bounds_out, seg_bounds, num_segs * 6ull * sizeof(float));
+        else if (bounds_out) std::memset(bounds_out, 0, num_segs * 6ull * sizeof(float));
+        return LVBH_OK;
+    }
+    if (int rc = ensure_arena(ctx, total)) return rc;
+    if (int rc = ensure_batch(ctx, num_segs, (uint32_t)tiles, (uint32_t)blocks)) return rc;
+    if (ctx->pending) lvbh_sync(ctx);  // the pinned mirror may still be read by the previous build
+    // segment table: first triangle, first sort tile, first tree block per segment
+    uint32_t tile = 0, blk = 0;
+    for (uint32_t i = 0; i <= num_segs; ++i) {
+        ctx->bh_rows[i] = SegRow{seg_offsets[i], tile, blk, 0u};
+        if (i < num_segs) {
+            const uint32_t n = seg_offsets[i + 1] - seg_offsets[i];
+            tile += sort_tiles(n);
+            blk += (uint32_t)emit_groups(n);
+        }
+    }
+    if (seg_bounds) std::memcpy(ctx->bh_bounds, seg_bounds, num_segs * 6ull * sizeof(float));
+    const BatchPlan bp{ctx->b_rows, ctx->b_tile_seg, ctx->b_blk_seg, num_segs, (uint32_t)tiles,
+                       (uint32_t)blocks, total};
+    LVBH_CUDA(ctx, cudaMemsetAsync(&ctx->ctl->aux_err, 0, sizeof(uint32_t), s));
+    const float4 *tri = reinterpret_cast<const float4 *>(tri_array);
+    const bool profile = (flags & LVBH_PROFILE) != 0;
+    if (profile) cudaEventRecord(ctx->ev[0], s);
+    if (flags & LVBH_INPUT_HOST) {
+        if (int rc = ensure_stage(ctx, 48ull * total)) return rc;
+        LVBH_CUDA(ctx, cudaMemcpyAsync(ctx->stage, tri_array, 48ull * total, cudaMemcpyHostToDevice, s));
+        tri = static_cast<const float4 *>(ctx->stage);
+    } else if (reinterpret_cast<uintptr_t>(tri_array) & 15u) {
+        return fail(ctx, LVBH_EINVAL, "device tri_array must be 16-byte aligned");
+    }
+    if (profile || (flags & LVBH_NO_GRAPH)) {
+        enqueue_batch(ctx, tri, bp, seg_bounds != nullptr, out, s, profile);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+    } else {
+        if (int rc = launch_batch_graph(ctx, tri, bp, seg_bounds != nullptr, out, s)) return rc;
+    }
+    ctx->ev_valid = profile;
+    LVBH_CUDA(ctx, cudaMemcpyAsync(ctx->host_ctl, ctx->ctl, offsetof(Control, pad1),
+                                   cudaMemcpyDeviceToHost, s));
+    if (bounds_out && !seg_bounds)
+        LVBH_CUDA(ctx, cudaMemcpyAsync(ctx->bh_ord, ctx->b_ord, num_segs * 6ull * 4,
+                                       cudaMemcpyDeviceToHost, s));
+    ctx->last_stream = s;
+    ctx->last_out = out;
+    ctx->last_hb = HostBounds{};
+    ctx->last_hb.use = seg_bounds != nullptr;
+    ctx->last_batch = true;
+    ctx->last_segs = num_segs;
+    ctx->last_bounds_out = bounds_out;
+    ctx->pending = true;
+    if (flags & LVBH_ASYNC) return LVBH_OK;
+    return lvbh_sync(ctx);
+}
+
 int lvbh_sync(lvbh_ctx *ctx) {
     if (!ctx) return LVBH_EINVAL;
     if (!ctx->pending) return LVBH_OK;
@@ -418,21 +654,26 @@ int lvbh_sync(lvbh_ctx *ctx) {
     cudaError_t e = cudaStreamSynchronize(ctx->last_stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamSynchronize");
     const uint32_t err = ctx->host_ctl[0] | ctx->host_ctl[1];
-    if (ctx->last_out) {
+    if (ctx->last_batch) {
+        if (ctx->last_bounds_out) {
+            if (ctx->last_hb.use) {
+                std::memcpy(ctx->last_bounds_out, ctx->bh_bounds, ctx->last_segs * 6ull * sizeof(float));
+            } else {
+                for (uint64_t i = 0; i < ctx->last_segs * 6ull; ++i) {
+                    const uint32_t o = ctx->bh_ord[i];
+                    const bool empty = ctx->bh_rows[i / 6 + 1].tri == ctx->bh_rows[i / 6].tri;
+                    ctx->last_bounds_out[i] = empty ? 0.0f : ord_word_to_float((i % 6) < 3 ? ~o : o);
+                }
+            }
+        }
+    } else if (ctx->last_out) {
         if (ctx->last_hb.use) {
             std::memcpy(ctx->last_out->bounds, ctx->last_hb.v, sizeof ctx->last_hb.v);
         } else {
             const uint32_t *b = ctx->host_ctl + offsetof(Control, bounds_ord) / 4;
             for (int a = 0; a < 3; ++a) {
-                uint32_t lo = ~b[a], hi = b[3 + a];
-                auto inv = [](uint32_t o) {
-                    uint32_t u = (o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o;
-                    float f;
-                    std::memcpy(&f, &u, 4);
-                    return f;
-                };
-                ctx->last_out->bounds[a] = inv(lo);
-                ctx->last_out->bounds[3 + a] = inv(hi);
+                ctx->last_out->bounds[a] = ord_word_to_float(~b[a]);
+                ctx->last_out->bounds[3 + a] = ord_word_to_float(b[3 + a]);
             }
         }
     }

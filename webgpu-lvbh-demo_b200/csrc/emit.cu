@@ -74,18 +74,50 @@ __device__ __forceinline__ int block_excl_sum(int v, int *s_warp, int *total) {
     return off + incl - v;
 }
 
+// Where a block of EB sorted leaves lives.  A batched build is a list of segments (meshes)
+// laid end to end; every block lies inside one segment and every index a kernel works with
+// is local to that segment (the plain build is the one-segment case).
+struct Span {
+    size_t start;  // the segment's first position in the batch
+    int n;         // the segment's triangle count
+    int b0;        // the block's first leaf within the segment
+};
+
+struct OneSeg {
+    int n;
+    __device__ __forceinline__ int blocks() const { return (n + EB - 1) / EB; }
+    __device__ __forceinline__ Span span(int blk) const { return Span{0, n, blk * EB}; }
+};
+
+struct ManySegs {
+    const SegRow *rows;       // num_segs + 1 rows
+    const uint32_t *blk_seg;  // segment of each block
+    int nblk;
+    __device__ __forceinline__ int blocks() const { return nblk; }
+    __device__ __forceinline__ Span span(int blk) const {
+        const uint32_t sg = __ldg(blk_seg + blk);
+        const uint32_t t0 = __ldg(&rows[sg].tri), t1 = __ldg(&rows[sg + 1].tri);
+        const int first = (int)__ldg(&rows[sg].blk);
+        return Span{t0, (int)(t1 - t0), (blk - first) * EB};
+    }
+};
+
 // K3a: leaf gather.  One thread per sorted position k: triangle perm[k] (3 x 16-byte loads)
 // to the output soup at k, its box (exact-zero components nudged by 1e-8 as
 // bvh-up-pass.js:209-210 does) to lbox[k] (min xyz, max xyz: 24 bytes).
-__global__ void __launch_bounds__(256) k_leaf_gather(const float4 *__restrict__ tri,
-                                                     const uint32_t *__restrict__ perm, int n,
+template <class Segs>
+__global__ void __launch_bounds__(256) k_leaf_gather(Segs segs, const float4 *__restrict__ tri,
+                                                     const uint32_t *__restrict__ perm,
                                                      float4 *__restrict__ otri,
                                                      float2 *__restrict__ lbox, Control *ctl) {
-    const int k = blockIdx.x * 256 + threadIdx.x;
-    if (k >= n) return;
+    const Span sp = segs.span(blockIdx.x);
+    const int kl = sp.b0 + threadIdx.x;
+    if (kl >= sp.n) return;
+    const size_t k = sp.start + kl;
     uint32_t ti = __ldg(perm + k);
-    if (ti >= (uint32_t)n) { atomicOr(&ctl->err, ERR_CLIMB); ti = 0; }
-    const float4 a = __ldg(tri + 3ull * ti), b = __ldg(tri + 3ull * ti + 1), c = __ldg(tri + 3ull * ti + 2);
+    if (ti >= (uint32_t)sp.n) { atomicOr(&ctl->err, ERR_CLIMB); ti = 0; }
+    const float4 *src = tri + 3ull * (sp.start + ti);
+    const float4 a = __ldg(src), b = __ldg(src + 1), c = __ldg(src + 2);
     st_stream(otri + 3ull * k, a);
     st_stream(otri + 3ull * k + 1, b);
     st_stream(otri + 3ull * k + 2, c);
@@ -134,21 +166,26 @@ __device__ __forceinline__ void range_box(const LeafTables &T, int a, int b, flo
 // table (nearest smaller separators on both sides), its Karras index and children from that
 // range, and its children's boxes by two range queries on the box table: all nodes of a block
 // complete at once.  The nodes that straddle blocks are left to K3c as open items.
-__global__ void __launch_bounds__(EB) k_tree_leaves(const uint32_t *__restrict__ keys,
-                                                    const float2 *__restrict__ lbox, int n,
-                                                    float4 *nodes, int32_t *parents,
+template <class Segs>
+__global__ void __launch_bounds__(EB) k_tree_leaves(Segs segs, const uint32_t *__restrict__ keys_all,
+                                                    const float2 *__restrict__ lbox_all,
+                                                    float4 *nodes_all, int32_t *parents_all,
                                                     OpenItem *out_items, uint32_t *out_counts,
                                                     Control *ctl) {
     extern __shared__ __align__(16) unsigned char smem[];
     LeafTables &T = *reinterpret_cast<LeafTables *>(smem);
     const int t = threadIdx.x;
-    const int nblk = (n + EB - 1) / EB;
+    const int nblk = segs.blocks();
 
-    // registers of the next block: this thread's key and leaf box, plus the two edge keys
+    // registers of the next block: its span, this thread's key and leaf box, the two edge keys
+    Span nsp{0, 0, 0};
     uint32_t nk = 0, nk_lo = 0, nk_hi = 0;
     float2 np0 = make_float2(0.f, 0.f), np1 = np0, np2 = np0;
     auto fetch = [&](int blk) {
-        const int b0 = blk * EB, k = b0 + t;
+        nsp = segs.span(blk);
+        const uint32_t *keys = keys_all + nsp.start;
+        const float2 *lbox = lbox_all + 3ull * nsp.start;
+        const int b0 = nsp.b0, n = nsp.n, k = b0 + t;
         if (k < n) {
             nk = __ldg(keys + k);
             np0 = __ldg(lbox + 3ull * k); np1 = __ldg(lbox + 3ull * k + 1); np2 = __ldg(lbox + 3ull * k + 2);
@@ -159,7 +196,10 @@ __global__ void __launch_bounds__(EB) k_tree_leaves(const uint32_t *__restrict__
     if ((int)blockIdx.x < nblk) fetch(blockIdx.x);
 
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
-        const int b0 = blk * EB;
+        const Span sp = nsp;
+        const int b0 = sp.b0, n = sp.n;
+        float4 *nodes = nodes_all + 4ull * sp.start;
+        int32_t *parents = parents_all + 2ull * sp.start;
         const int m = min(EB, n - b0);
         const int k = b0 + t;
         const bool active = t < m;
@@ -175,15 +215,18 @@ __global__ void __launch_bounds__(EB) k_tree_leaves(const uint32_t *__restrict__
         T.open[t] = 0;
         T.local[t] = 0;
         if (blk + (int)gridDim.x < nblk) fetch(blk + gridDim.x);
-        if (active && n == 1) {  // one leaf, one arrival at node 0: left slot only, f_1 = 1
-            nodes[0] = make_float4(box[0], box[1], box[2], __int_as_float(-1));
-            nodes[1] = make_float4(box[3], box[4], box[5], __int_as_float(1));
-            nodes[2] = make_float4(0.f, 0.f, 0.f, 0.f);
-            nodes[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-            parents[0] = 0;
-            parents[1] = 0;
+        if (n == 1) {  // one leaf, one arrival at node 0: left slot only, f_1 = 1
+            if (t == 0) {
+                nodes[0] = make_float4(box[0], box[1], box[2], __int_as_float(-1));
+                nodes[1] = make_float4(box[3], box[4], box[5], __int_as_float(1));
+                nodes[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+                nodes[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+                parents[0] = 0;
+                parents[1] = 0;
+                out_counts[blk] = 0;
+            }
+            continue;  // uniform across the block; the tables are untouched by other threads
         }
-        if (n == 1) return;
         if (k == 0) {  // the root has no parent; slot N-1 and record N-1 stay zero
             parents[0] = 0;
             parents[n - 1] = 0;
@@ -320,17 +363,26 @@ __global__ void __launch_bounds__(EB) k_tree_leaves(const uint32_t *__restrict__
 // record and both parent links.  Nothing waits, so the kernel cannot hang; climbs are bounded
 // and every index is range-checked.  The epoch makes the arrival words reusable without
 // clearing: a word left by an older build never equals the current epoch.
-__global__ void __launch_bounds__(256) k_emit_top(const OpenItem *__restrict__ items,
-                                                  const uint32_t *__restrict__ counts, int groups,
-                                                  const uint32_t *__restrict__ keys, int n,
-                                                  float4 *nodes, int32_t *parents,
-                                                  uint32_t *arrive, float4 *pend,
+template <class Segs>
+__global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__restrict__ items,
+                                                  const uint32_t *__restrict__ counts,
+                                                  const uint32_t *__restrict__ keys_all,
+                                                  float4 *nodes_all, int32_t *parents_all,
+                                                  uint32_t *arrive_all, float4 *pend_all,
                                                   const uint32_t *__restrict__ epoch_p,
                                                   Control *ctl) {
     const int gw = (blockIdx.x * 256 + threadIdx.x) / kTopLanes, lane = threadIdx.x % kTopLanes;
-    if (gw >= groups) return;
-    const uint32_t epoch = *epoch_p;
+    if (gw >= segs.blocks()) return;
     const int cnt = (int)min(counts[gw], (uint32_t)kOpenCap);
+    if (lane >= cnt) return;
+    const uint32_t epoch = *epoch_p;
+    const Span sp = segs.span(gw);
+    const int n = sp.n;
+    const uint32_t *keys = keys_all + sp.start;
+    float4 *nodes = nodes_all + 4ull * sp.start;
+    int32_t *parents = parents_all + 2ull * sp.start;
+    uint32_t *arrive = arrive_all + sp.start;
+    float4 *pend = pend_all + 2ull * sp.start;
     for (int q = lane; q < cnt; q += kTopLanes) {
         const OpenItem it = items[(size_t)gw * kOpenCap + q];
         int l = it.xl, r = it.xr, ref = __float_as_int(it.lo.w);
@@ -376,16 +428,42 @@ __global__ void __launch_bounds__(256) k_emit_top(const OpenItem *__restrict__ i
 
 inline size_t leaves_smem_bytes() { return sizeof(LeafTables); }
 
+template <class Segs>
+void launch_emit_impl(Segs segs, int groups, const float4 *tri, const uint32_t *perm,
+                      const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
+                      float2 *lbox, OpenItem *items, uint32_t *counts, uint32_t *arrive,
+                      float4 *pend, const uint32_t *epoch, Control *ctl, bool top,
+                      cudaStream_t s, cudaEvent_t *ev) {
+    k_leaf_gather<<<groups, 256, 0, s>>>(segs, tri, perm, otri, lbox, ctl);
+    if (ev) cudaEventRecord(ev[0], s);
+    const int grid = min(groups, sm_count() * kTreeCtasPerSm);
+    k_tree_leaves<<<grid, EB, leaves_smem_bytes(), s>>>(segs, keys, lbox, nodes, parents, items,
+                                                         counts, ctl);
+    if (ev) cudaEventRecord(ev[1], s);
+    if (top)
+        k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, counts, keys, nodes,
+                                                                     parents, arrive, pend, epoch,
+                                                                     ctl);
+    if (ev) cudaEventRecord(ev[2], s);
+}
+
+template <class K>
+cudaError_t prefer_shared(K kernel) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)leaves_smem_bytes());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared);
+}
+
 }  // namespace
 
 size_t emit_groups(uint32_t n) { return (n + EB - 1) / EB; }
 
 cudaError_t emit_init() {
-    cudaError_t e = cudaFuncSetAttribute(k_tree_leaves, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)leaves_smem_bytes());
+    cudaError_t e = prefer_shared(k_tree_leaves<OneSeg>);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_tree_leaves, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                (int)cudaSharedmemCarveoutMaxShared);
+    return prefer_shared(k_tree_leaves<ManySegs>);
 }
 
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
@@ -393,18 +471,20 @@ void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, 
                  uint32_t *counts, uint32_t *arrive, float4 *pend, const uint32_t *epoch,
                  Control *ctl, cudaStream_t s, cudaEvent_t *ev) {
     if (n == 0) return;
-    k_leaf_gather<<<(n + 255) / 256, 256, 0, s>>>(tri, perm, (int)n, otri, lbox, ctl);
-    if (ev) cudaEventRecord(ev[0], s);
     const int groups = (int)emit_groups(n);
-    const int grid = min(groups, sm_count() * kTreeCtasPerSm);
-    k_tree_leaves<<<grid, EB, leaves_smem_bytes(), s>>>(keys, lbox, (int)n, nodes, parents, items,
-                                                         counts, ctl);
-    if (ev) cudaEventRecord(ev[1], s);
-    if (groups > 1)
-        k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(items, counts, groups, keys,
-                                                                     (int)n, nodes, parents, arrive,
-                                                                     pend, epoch, ctl);
-    if (ev) cudaEventRecord(ev[2], s);
+    launch_emit_impl(OneSeg{(int)n}, groups, tri, perm, keys, otri, nodes, parents, lbox, items,
+                     counts, arrive, pend, epoch, ctl, groups > 1, s, ev);
+}
+
+void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
+                       const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
+                       float2 *lbox, OpenItem *items, uint32_t *counts, uint32_t *arrive,
+                       float4 *pend, const uint32_t *epoch, Control *ctl, cudaStream_t s,
+                       cudaEvent_t *ev) {
+    if (bp.blocks == 0) return;
+    launch_emit_impl(ManySegs{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks, tri, perm, keys,
+                     otri, nodes, parents, lbox, items, counts, arrive, pend, epoch, ctl, true, s,
+                     ev);
 }
 
 }  // namespace lvbh

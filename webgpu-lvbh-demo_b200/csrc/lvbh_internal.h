@@ -49,6 +49,21 @@ struct HostBounds {
     int use;  // 1 = quantise with v; 0 = with the device reduction in Control::bounds_ord
 };
 
+// Batched builds: segments (meshes) laid end to end in one soup.  Row s of the segment table
+// holds segment s's first triangle, first sort tile and first tree block; row num_segs holds
+// the totals.  Sort tiles (kSortTile keys) and tree blocks (kEmitBlock leaves) never cross a
+// segment boundary, so each tile or block works on one segment with segment-local indices.
+struct __align__(16) SegRow {
+    uint32_t tri, tile, blk, pad;
+};
+
+struct BatchPlan {
+    const SegRow *rows;        // num_segs + 1 rows (device)
+    const uint32_t *tile_seg;  // segment of each sort tile (device, `tiles` entries)
+    const uint32_t *blk_seg;   // segment of each tree block (device, `blocks` entries)
+    uint32_t num_segs, tiles, blocks, total;
+};
+
 int sm_count();
 
 // K1a: scene box over every vertex of the 48-byte triangle soup.
@@ -72,6 +87,27 @@ void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, 
                  float4 *otri, float4 *nodes, int32_t *parents, float2 *lbox, OpenItem *items,
                  uint32_t *counts, uint32_t *arrive, float4 *pend, const uint32_t *epoch,
                  Control *ctl, cudaStream_t s, cudaEvent_t *ev);
+// Batched forms of K1a, K1b, K2 and K3 over the segments of `bp`.  seg_ord holds 6 ordered
+// bound words per segment (zeroed before K1a; min at 0-2 as ~ord_lo, max at 3-5 as ord_lo),
+// seg_hist 4 x 256 digit counts per segment (zeroed before K1b); host_bounds, when not null,
+// holds 6 floats per segment that replace the device reduction.  K2's look-back words:
+// bp.tiles * 256 per pass, zeroed before the build.
+void launch_seg_tables(const SegRow *rows, uint32_t num_segs, uint32_t *tile_seg,
+                       uint32_t *blk_seg, cudaStream_t s);
+void launch_bounds_batch(const BatchPlan &bp, const float4 *tri, uint32_t *seg_ord, cudaStream_t s);
+void launch_morton_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,
+                         const uint32_t *seg_ord, uint32_t *seg_hist, Control *ctl,
+                         uint32_t *keys_out, uint32_t *epoch, cudaStream_t s);
+void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const uint32_t *vals_in,
+                           uint32_t *keys_out, uint32_t *vals_out, int pass,
+                           const uint32_t *seg_hist, Control *ctl, uint32_t *lookback,
+                           cudaStream_t s);
+// items / counts: bp.blocks * kOpenCap / bp.blocks entries.
+void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
+                       const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
+                       float2 *lbox, OpenItem *items, uint32_t *counts, uint32_t *arrive,
+                       float4 *pend, const uint32_t *epoch, Control *ctl, cudaStream_t s,
+                       cudaEvent_t *ev);
 // Indexed mesh -> 48-byte soup (pad 0).  An index >= num_verts sets ERR_BAD_INDEX in
 // *err and gathers zeros instead of reading out of bounds.
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,

@@ -132,6 +132,127 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
     }
 }
 
+// Batched K1a: one block per sort tile (at most kSortTile triangles of one segment); the
+// tile's vertex box goes into its segment's six ordered bound words.
+__global__ void __launch_bounds__(kThreads) k_bounds_batch(const float4 *__restrict__ tri,
+                                                           const SegRow *__restrict__ rows,
+                                                           const uint32_t *__restrict__ tile_seg,
+                                                           uint32_t *__restrict__ seg_ord) {
+    const uint32_t tile = blockIdx.x, sg = __ldg(tile_seg + tile);
+    const uint32_t t0 = __ldg(&rows[sg].tri), t1 = __ldg(&rows[sg + 1].tri);
+    const uint32_t first = t0 + (tile - __ldg(&rows[sg].tile)) * (uint32_t)kSortTile;
+    const uint32_t cnt = min((uint32_t)kSortTile, t1 - first);
+    const float4 *v = tri + 3ull * first;
+    const uint32_t nv = 3u * cnt;
+    float mn[3] = {INFINITY, INFINITY, INFINITY};
+    float mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = threadIdx.x; i < nv; i += kThreads) {
+        const float4 p = ld_stream(v + i);
+        mn[0] = fminf(mn[0], p.x); mx[0] = fmaxf(mx[0], p.x);
+        mn[1] = fminf(mn[1], p.y); mx[1] = fmaxf(mx[1], p.y);
+        mn[2] = fminf(mn[2], p.z); mx[2] = fmaxf(mx[2], p.z);
+    }
+    warp_minmax(mn, mx);
+    __shared__ float s[kWarps][6];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { s[warp][a] = mn[a]; s[warp][3 + a] = mx[a]; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int a = threadIdx.x;
+        float r = s[0][a];
+        for (int w = 1; w < kWarps; ++w) r = a < 3 ? fminf(r, s[w][a]) : fmaxf(r, s[w][a]);
+        uint32_t *o = seg_ord + 6ull * sg;
+        if (a < 3) atomicMax(o + a, ~ord_lo(r));
+        else atomicMax(o + a, ord_lo(r));
+    }
+}
+
+// Batched K1b: one block per sort tile; each warp takes chunks of 32 triangles of the tile
+// (the same transposed 16-byte loads as k_morton), quantises them with the segment's bounds
+// and adds the tile's digit counts to the segment's histograms.
+__global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restrict__ tri,
+                                                           const SegRow *__restrict__ rows,
+                                                           const uint32_t *__restrict__ tile_seg,
+                                                           const float *__restrict__ host_bounds,
+                                                           const uint32_t *__restrict__ seg_ord,
+                                                           uint32_t *__restrict__ seg_hist,
+                                                           Control *__restrict__ ctl,
+                                                           uint32_t *__restrict__ keys,
+                                                           uint32_t *__restrict__ epoch) {
+    __shared__ float4 stage[kWarps][96];
+    __shared__ uint32_t hist[kSortPasses][kDigits];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
+        const uint32_t e = *epoch + 1u;
+        *epoch = e == 0u ? 1u : e;
+    }
+    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) (&hist[0][0])[i] = 0;
+    const uint32_t tile = blockIdx.x, sg = __ldg(tile_seg + tile);
+    const uint32_t t0 = __ldg(&rows[sg].tri), t1 = __ldg(&rows[sg + 1].tri);
+    const uint32_t first = t0 + (tile - __ldg(&rows[sg].tile)) * (uint32_t)kSortTile;
+    const uint32_t cnt = min((uint32_t)kSortTile, t1 - first);
+    float umin[3], umax[3];
+    if (host_bounds) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { umin[a] = host_bounds[6ull * sg + a]; umax[a] = host_bounds[6ull * sg + 3 + a]; }
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            umin[a] = ord_lo_inv(~seg_ord[6ull * sg + a]);
+            umax[a] = ord_lo_inv(seg_ord[6ull * sg + 3 + a]);
+        }
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const float4 *src = tri + 3ull * first;
+    const uint32_t nv = 3u * cnt;
+    bool bad = false;
+    for (uint32_t c = warp; c < (cnt + 31) / 32; c += kWarps) {
+        const uint32_t base = 96u * c;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const uint32_t e = base + 32 * r + lane;
+            stage[warp][32 * r + lane] = e < nv ? ld_stream(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncwarp();
+        const float4 v0 = stage[warp][3 * lane], v1 = stage[warp][3 * lane + 1],
+                     v2 = stage[warp][3 * lane + 2];
+        __syncwarp();
+        const uint32_t t = 32u * c + lane;
+        if (t < cnt) {
+            bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
+            const uint32_t qx = quantise(fminf(v0.x, fminf(v1.x, v2.x)), fmaxf(v0.x, fmaxf(v1.x, v2.x)), umin[0], umax[0]);
+            const uint32_t qy = quantise(fminf(v0.y, fminf(v1.y, v2.y)), fmaxf(v0.y, fmaxf(v1.y, v2.y)), umin[1], umax[1]);
+            const uint32_t qz = quantise(fminf(v0.z, fminf(v1.z, v2.z)), fmaxf(v0.z, fmaxf(v1.z, v2.z)), umin[2], umax[2]);
+            const uint32_t key = morton3(qx, qy, qz);
+            keys[first + t] = key;
+#pragma unroll
+            for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (kDigitBits * p)) & (kDigits - 1)], 1u);
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
+    __syncthreads();
+    uint32_t *h = seg_hist + (size_t)sg * kSortPasses * kDigits;
+    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) {
+        const uint32_t c = (&hist[0][0])[i];
+        if (c) atomicAdd(h + i, c);
+    }
+}
+
+// Segment of every sort tile and tree block: one warp per segment fills its entries.
+__global__ void __launch_bounds__(256) k_seg_tables(const SegRow *__restrict__ rows, uint32_t num_segs,
+                                                    uint32_t *__restrict__ tile_seg,
+                                                    uint32_t *__restrict__ blk_seg) {
+    const uint32_t sg = (blockIdx.x * 256u + threadIdx.x) / 32u, lane = threadIdx.x & 31;
+    if (sg >= num_segs) return;
+    const SegRow a = rows[sg], b = rows[sg + 1];
+    for (uint32_t t = a.tile + lane; t < b.tile; t += 32) tile_seg[t] = sg;
+    for (uint32_t t = a.blk + lane; t < b.blk; t += 32) blk_seg[t] = sg;
+}
+
 __global__ void k_gather_indexed(const float *__restrict__ xyz, uint32_t num_verts,
                                  const uint32_t *__restrict__ idx3, uint32_t n,
                                  float4 *__restrict__ tri, uint32_t *__restrict__ err) {
@@ -175,6 +296,25 @@ void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t 
                            uint32_t n, float4 *tri, uint32_t *err, cudaStream_t s) {
     if (n == 0) return;
     k_gather_indexed<<<(n + 255) / 256, 256, 0, s>>>(xyz, num_verts, idx3, n, tri, err);
+}
+
+void launch_seg_tables(const SegRow *rows, uint32_t num_segs, uint32_t *tile_seg,
+                       uint32_t *blk_seg, cudaStream_t s) {
+    if (num_segs == 0) return;
+    k_seg_tables<<<(num_segs + 7) / 8, 256, 0, s>>>(rows, num_segs, tile_seg, blk_seg);
+}
+
+void launch_bounds_batch(const BatchPlan &bp, const float4 *tri, uint32_t *seg_ord, cudaStream_t s) {
+    if (bp.tiles == 0) return;
+    k_bounds_batch<<<bp.tiles, kThreads, 0, s>>>(tri, bp.rows, bp.tile_seg, seg_ord);
+}
+
+void launch_morton_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,
+                         const uint32_t *seg_ord, uint32_t *seg_hist, Control *ctl,
+                         uint32_t *keys_out, uint32_t *epoch, cudaStream_t s) {
+    if (bp.tiles == 0) return;
+    k_morton_batch<<<bp.tiles, kThreads, 0, s>>>(tri, bp.rows, bp.tile_seg, host_bounds, seg_ord,
+                                                 seg_hist, ctl, keys_out, epoch);
 }
 
 }  // namespace lvbh

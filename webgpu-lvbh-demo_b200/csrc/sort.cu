@@ -55,11 +55,43 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s
     return warp_off + incl - x;
 }
 
-__global__ void __launch_bounds__(T, 4) k_onesweep(const uint32_t *__restrict__ keys_in,
-                                                const uint32_t *__restrict__ vals_in,
-                                                uint32_t *__restrict__ keys_out,
-                                                uint32_t *__restrict__ vals_out, uint32_t n,
-                                                int pass, Control *__restrict__ ctl,
+// The keys a tile works on: its segment's first key in the batch and size, the tile's first
+// key within the segment, the segment's first tile (the look-back stops there) and the
+// segment's digit counts for this pass.  The plain sort is the one-segment case.
+struct TileSpan {
+    size_t start;
+    uint32_t n, base, first;
+    const uint32_t *hist;
+};
+
+struct OneSegSort {
+    uint32_t n;
+    const uint32_t *hist;  // this pass's counts
+    __device__ __forceinline__ TileSpan span(uint32_t tile) const {
+        return TileSpan{0, n, tile * (uint32_t)kSortTile, 0u, hist};
+    }
+};
+
+struct ManySegSort {
+    const SegRow *rows;
+    const uint32_t *tile_seg;
+    const uint32_t *seg_hist;  // [segment][pass][digit]
+    int pass;
+    __device__ __forceinline__ TileSpan span(uint32_t tile) const {
+        const uint32_t sg = __ldg(tile_seg + tile);
+        const uint32_t t0 = __ldg(&rows[sg].tri), t1 = __ldg(&rows[sg + 1].tri);
+        const uint32_t first = __ldg(&rows[sg].tile);
+        return TileSpan{t0, t1 - t0, (tile - first) * (uint32_t)kSortTile, first,
+                        seg_hist + ((size_t)sg * kSortPasses + pass) * kDigits};
+    }
+};
+
+template <class Segs>
+__global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__restrict__ keys_all,
+                                                const uint32_t *__restrict__ vals_all,
+                                                uint32_t *__restrict__ keys_out_all,
+                                                uint32_t *__restrict__ vals_out_all, int pass,
+                                                Control *__restrict__ ctl,
                                                 uint32_t *__restrict__ lookback) {
     __shared__ uint32_t s_keys[kSortTile];
     __shared__ uint32_t s_vals[kSortTile];
@@ -74,7 +106,12 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(const uint32_t *__restrict__ 
     for (int i = tid; i < W * kDigits; i += T) (&s_whist[0][0])[i] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
-    const uint32_t tile_base = tile * (uint32_t)kSortTile;
+    const TileSpan sp = segs.span(tile);
+    const uint32_t n = sp.n, tile_base = sp.base;
+    const uint32_t *keys_in = keys_all + sp.start;
+    const uint32_t *vals_in = vals_all ? vals_all + sp.start : nullptr;
+    uint32_t *keys_out = keys_out_all + sp.start;
+    uint32_t *vals_out = vals_out_all + sp.start;
     const int shift = pass * kDigitBits;
     const uint32_t wbase = tile_base + warp * (IPT * 32);
 
@@ -86,7 +123,7 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(const uint32_t *__restrict__ 
     }
 
     // Global start of this thread's digit: exclusive scan of the pass's digit counts.
-    const uint32_t digit_base = block_exclusive_scan(ctl->hist[pass][tid], s_warp);
+    const uint32_t digit_base = block_exclusive_scan(__ldg(sp.hist + tid), s_warp);
 
     // Stable in-warp ranking, keys visited in input order (item-major, then lane).
     uint32_t rank[IPT / 2];  // two 16-bit ranks per word
@@ -120,7 +157,7 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(const uint32_t *__restrict__ 
     // (independent loads), then add their counts newest first until a PREFIX is met.
     uint32_t *lb = lookback + (size_t)tile * kDigits + tid;
     uint32_t excl = 0;
-    if (tile == 0) {
+    if (tile == sp.first) {
         st_relaxed_gpu(lb, kFlagPrefix | tile_count);
     } else {
         st_relaxed_gpu(lb, kFlagAgg | tile_count);
@@ -131,7 +168,7 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(const uint32_t *__restrict__ 
             uint32_t w[kLookback];
 #pragma unroll
             for (int i = 0; i < kLookback; ++i)
-                w[i] = kk - i >= 0 ? ld_relaxed_gpu(lookback + (size_t)(kk - i) * kDigits + tid) : kFlagPrefix;
+                w[i] = kk - i >= (int64_t)sp.first ? ld_relaxed_gpu(lookback + (size_t)(kk - i) * kDigits + tid) : kFlagPrefix;
             bool stalled = false;
 #pragma unroll
             for (int i = 0; i < kLookback; ++i) {
@@ -142,7 +179,7 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(const uint32_t *__restrict__ 
                 --kk;
                 if (flag == kFlagPrefix) done = true;
             }
-            if (kk < 0) done = true;
+            if (kk < (int64_t)sp.first) done = true;
             if (done || !stalled) continue;
             if (!timed) { t0 = clock64(); timed = true; }
             else if (clock64() - t0 > kSpinLimitCycles ||
@@ -196,8 +233,18 @@ void launch_onesweep(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t 
                      cudaStream_t s) {
     if (n == 0) return;
     const uint32_t tiles = sort_tiles(n);
-    k_onesweep<<<tiles, T, 0, s>>>(keys_in, vals_in, keys_out, vals_out, n, pass, ctl,
-                                   lookback + (size_t)pass * tiles * kDigits);
+    k_onesweep<<<tiles, T, 0, s>>>(OneSegSort{n, &ctl->hist[pass][0]}, keys_in, vals_in, keys_out,
+                                   vals_out, pass, ctl, lookback + (size_t)pass * tiles * kDigits);
+}
+
+void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const uint32_t *vals_in,
+                           uint32_t *keys_out, uint32_t *vals_out, int pass,
+                           const uint32_t *seg_hist, Control *ctl, uint32_t *lookback,
+                           cudaStream_t s) {
+    if (bp.tiles == 0) return;
+    k_onesweep<<<bp.tiles, T, 0, s>>>(ManySegSort{bp.rows, bp.tile_seg, seg_hist, pass}, keys_in,
+                                      vals_in, keys_out, vals_out, pass, ctl,
+                                      lookback + (size_t)pass * bp.tiles * kDigits);
 }
 
 }  // namespace lvbh

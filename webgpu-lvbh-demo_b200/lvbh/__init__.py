@@ -28,7 +28,8 @@ from . import _native
 from ._native import (ASYNC, INPUT_HOST, NO_GRAPH, OUT_CALLER, PROFILE, STAGE_NAMES, LvbhError,
                       version)
 
-__all__ = ["initBVHBuild", "BVHBuilder", "BuildResult", "LvbhError", "version", "trace"]
+__all__ = ["initBVHBuild", "BVHBuilder", "BuildResult", "BatchResult", "LvbhError", "version",
+           "trace"]
 
 
 def _torch():
@@ -102,6 +103,22 @@ class BuildResult:
                 "leaf_index": self.leaf_index.cpu().numpy().view(np.uint32),
                 "morton": self.morton.cpu().numpy().view(np.uint32),
                 "bounds": self.bounds.copy()}
+
+
+@dataclass
+class BatchResult(BuildResult):
+    """Result of a batched build: the concatenated per-mesh buffers plus the mesh offsets
+    (int64, num_meshes + 1) and each mesh's quantisation box seg_bounds (float32, (M, 6))."""
+    offsets: Optional[np.ndarray] = None
+    seg_bounds: Optional[np.ndarray] = None
+
+    def mesh(self, i: int) -> BuildResult:
+        """Views of mesh i's slice - a standalone BVH of that mesh, identical to building it
+        alone with build_soup."""
+        a, b = int(self.offsets[i]), int(self.offsets[i + 1])
+        return BuildResult(nodes=self.nodes[a:b], tris=self.tris[a:b],
+                           parents=self.parents[2 * a:2 * b], leaf_index=self.leaf_index[a:b],
+                           morton=self.morton[a:b], bounds=self.seg_bounds[i].copy())
 
 
 def empty_outputs(n: int, device):
@@ -199,6 +216,54 @@ class BVHBuilder:
         return self._run(_native.lib.lvbh_build_indexed, (pv, nv, pi, n), n, bounds, flags,
                          outputs, stream, sync, profile, keep=(xyz, idx3))
 
+    def build_batched(self, tri, offsets, seg_bounds=None, outputs=None, stream=None, sync=True,
+                      profile=False, graph=True) -> BatchResult:
+        """Many meshes in one build.  tri: (sum N, 12) float32 host array or CUDA tensor with
+        the meshes end to end; offsets: num_meshes + 1 triangle offsets (offsets[0] = 0);
+        seg_bounds: (M, 6) float32 per-mesh MODEL_BOUNDS or None (each mesh's own box)."""
+        torch = _torch()
+        offs = np.ascontiguousarray(offsets, dtype=np.int64).ravel()
+        if offs.size < 1 or offs[0] != 0 or np.any(np.diff(offs) < 0) or offs[-1] > _native.MAX_TRIS:
+            raise ValueError("offsets must start at 0, be non-decreasing and end <= 2^29")
+        m = offs.size - 1
+        offs32 = offs.astype(np.uint32)
+        host = not isinstance(tri, torch.Tensor)
+        if host:
+            tri = np.ascontiguousarray(tri, dtype=np.float32).reshape(-1, 12)
+            ptr = tri.ctypes.data_as(ctypes.c_void_p)
+        else:
+            if tri.device.type != "cuda":
+                tri = tri.to(self.device)
+            tri = tri.contiguous().reshape(-1, 12)
+            if tri.dtype != torch.float32:
+                raise TypeError("device triangle soup must be float32")
+            ptr = ctypes.c_void_p(tri.data_ptr())
+        n = int(offs[-1])
+        if tri.shape[0] != n:
+            raise ValueError(f"soup holds {tri.shape[0]} triangles, offsets end at {n}")
+        if self._pending is not None:
+            self.sync()
+        outs = outputs if outputs is not None else empty_outputs(n, self.device)
+        r = _result_struct(outs, n)
+        sb = None if seg_bounds is None else np.ascontiguousarray(seg_bounds, dtype=np.float32).reshape(m, 6)
+        bout = np.zeros((m, 6), dtype=np.float32)
+        flags = OUT_CALLER | (INPUT_HOST if host else 0) | (0 if sync else ASYNC) \
+            | (PROFILE if profile else 0) | (0 if graph else NO_GRAPH)
+        rc = _native.lib.lvbh_build_batched(
+            self._ctx, ptr, offs32.ctypes.data_as(ctypes.c_void_p), m,
+            None if sb is None else sb.ctypes.data_as(ctypes.c_void_p),
+            bout.ctypes.data_as(ctypes.c_void_p), flags, ctypes.byref(r),
+            _stream_ptr(stream, self.device))
+        res = BatchResult(bounds=np.zeros(6, np.float32), offsets=offs, seg_bounds=bout, **outs)
+        if rc != _native.OK:
+            _native.check(self._ctx, rc)
+        if sync:
+            if profile:
+                res.stage_ms = self.stage_times()
+        else:
+            self._pending = (r, res, (tri, offs32, sb, bout), profile)
+        return res
+
     def _run(self, fn, head, n, bounds, flags, outputs, stream, sync, profile, keep):
         if self._pending is not None:
             self.sync()
@@ -226,7 +291,8 @@ class BVHBuilder:
         r, res, _, profile = self._pending
         self._pending = None
         _native.check(self._ctx, _native.lib.lvbh_sync(self._ctx))
-        res.bounds = np.array(r.bounds[:], dtype=np.float32)
+        if not isinstance(res, BatchResult):
+            res.bounds = np.array(r.bounds[:], dtype=np.float32)
         if profile:
             res.stage_ms = self.stage_times()
 

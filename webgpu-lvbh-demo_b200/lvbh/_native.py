@@ -61,6 +61,8 @@ def _load():
     L.lvbh_build_soup.argtypes = [vp, vp, u32, vp, u32, ctypes.POINTER(Result), vp]
     L.lvbh_build_indexed.restype = i32
     L.lvbh_build_indexed.argtypes = [vp, vp, u32, vp, u32, vp, u32, ctypes.POINTER(Result), vp]
+    L.lvbh_build_batched.restype = i32
+    L.lvbh_build_batched.argtypes = [vp, vp, vp, u32, vp, vp, u32, ctypes.POINTER(Result), vp]
     L.lvbh_sync.restype = i32
     L.lvbh_sync.argtypes = [vp]
     L.lvbh_release.restype = i32
