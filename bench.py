@@ -455,6 +455,128 @@ def run_batched(args, world, rank, local, clocks=None):
             "generate_s": round(t_gen, 1)}
 
 
+def percentiles(x):
+    import numpy as np
+    a = np.asarray(x, dtype=np.float64)
+    if a.size == 0:
+        return {"p50": None, "p99": None, "p999": None}
+    return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)),
+            "p999": float(np.percentile(a, 99.9))}
+
+
+def run_served(args, world, rank, local):
+    """Served builds: Poisson arrivals at each rate of the sweep, request sizes log-uniform in
+    [1024, 4194304] triangles of the clustered distribution, a 96 GB budget.  Each request's
+    triangles are a prefix of one of a few pooled, seeded clustered soups kept in device memory
+    (the payloads are resident before the run, as the server keeps vertex state resident).
+    Latency = submit -> the request's batch finished on the GPU (server clock).  Beside it the
+    plain per-request builder (lvbh_build_soup, one request at a time in arrival order) serves
+    the same trace."""
+    import numpy as np
+    import torch
+
+    import lvbh
+    from lvbh import scenes
+    from lvbh.server import Server
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    pool = [torch.from_numpy(scenes.clustered_soup(1 << 22, seed=100 + k)).to(dev)
+            for k in range(args.serve_pool)]
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    srv = Server(local, hbm_budget=96 << 30, slots=3, max_batch_tris=1 << 24, max_batch_reqs=4096)
+    plain = lvbh.BVHBuilder(local, reserve_tris=1 << 22)
+    pstream = torch.cuda.Stream(dev)
+    pouts = lvbh.empty_outputs(1 << 22, dev)
+    out = {"workload": "served_requests", "budget_gb": 96, "slots": 3, "rates": []}
+    # warm-up of both paths before the sweep: every kernel, every slot, the result memory
+    wsizes = scenes.request_sizes(args.warmup * 64, seed=99)
+    wt = [srv.submit(pool[i % len(pool)][: int(m)]) for i, m in enumerate(wsizes)]
+    for t in wt:
+        srv.wait(t)
+        srv.release(t)
+    for i, m in enumerate(wsizes[: args.warmup * 8]):
+        m = int(m)
+        plain.build_soup(pool[i % len(pool)][:m], None, stream=pstream, graph=False,
+                         outputs={k: v[: m * (2 if k == "parents" else 1)] for k, v in pouts.items()})
+    torch.cuda.synchronize(dev)
+    for rate in rates:
+        count = int(min(args.serve_max_requests, max(args.serve_min_requests, rate * args.serve_seconds)))
+        sizes = scenes.request_sizes(count, seed=4)
+        rng = np.random.default_rng(int(rate))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+        srcs = [pool[i % len(pool)][: int(sizes[i])] for i in range(count)]
+        # warm-up: a few requests through both paths
+        for i in range(min(8, count)):
+            t = srv.submit(srcs[i])
+            srv.wait(t)
+            srv.release(t)
+            plain.build_soup(srcs[i], None, outputs={k: v[: int(sizes[i]) * (2 if k == "parents" else 1)] for k, v in pouts.items()},
+                             stream=pstream, graph=False)
+        # one client thread: submits at the arrival times and, between arrivals, polls the
+        # oldest outstanding requests and releases the finished ones
+        import ctypes
+        from collections import deque
+        from lvbh import _native
+        L, h = _native.lib, srv._h
+        rinfo = _native.RequestInfo()
+        infos = []
+        outstanding = deque()
+
+        def reap(block=False):
+            while outstanding:
+                t = outstanding[0]
+                rc = (L.lvbh_wait(h, t, -1, None, ctypes.byref(rinfo)) if block
+                      else L.lvbh_poll(h, t, None, ctypes.byref(rinfo)))
+                if rc == _native.EBUSY:
+                    return
+                if rc != _native.OK:
+                    raise lvbh.LvbhError(rc, "served request failed")
+                infos.append((rinfo.latency_ms, rinfo.queued_ms, rinfo.batch_reqs))
+                L.lvbh_request_release(h, t)
+                outstanding.popleft()
+
+        s0 = srv.stats()
+        t0 = time.perf_counter()
+        for i in range(count):
+            while time.perf_counter() - t0 < arrivals[i]:
+                reap()
+            outstanding.append(srv.submit(srcs[i]))
+            srv._keep.clear()
+        while outstanding:
+            reap(block=True)
+        t_end = time.perf_counter()
+        s1 = srv.stats()
+        lat = [x[0] for x in infos]
+        span = max(t_end - t0, 1e-9)
+        served = {"rate": rate, "requests": count, "latency_ms": percentiles(lat),
+                  "queued_ms": percentiles([x[1] for x in infos]),
+                  "exec_ms": percentiles([x[0] - x[1] for x in infos]),
+                  "builds_per_s": count / span, "mprims_per_s": float(sizes.sum()) / span / 1e6,
+                  "batches": s1["batches"] - s0["batches"],
+                  "mean_batch_reqs": count / max(1, s1["batches"] - s0["batches"]),
+                  "max_batch_seen": s1["max_batch_seen"], "admission_waits": s1["admission_waits"] - s0["admission_waits"],
+                  "peak_result_gb": s1["peak_bytes"] / 2**30}
+        # the plain per-request builder on the same trace
+        plat = []
+        t0 = time.perf_counter()
+        for i in range(count):
+            while time.perf_counter() - t0 < arrivals[i]:
+                pass
+            m = int(sizes[i])
+            plain.build_soup(srcs[i], None, outputs={k: v[: m * (2 if k == "parents" else 1)] for k, v in pouts.items()},
+                             stream=pstream, graph=False)
+            plat.append((time.perf_counter() - t0 - arrivals[i]) * 1e3)
+        pspan = time.perf_counter() - t0
+        served["plain"] = {"latency_ms": percentiles(plat), "builds_per_s": count / pspan}
+        out["rates"].append(served)
+    st = srv.stats()
+    out["server_stats"] = {k: st[k] for k in ("batches", "completed", "failed", "max_batch_seen")}
+    srv.close()
+    plain.close()
+    return out
+
+
 def load_traffic(kernel: str, n: int):
     """dram read + write bytes per launch of `kernel` from the committed ncu capture summary
     (profiles/traffic.json: bytes per triangle, scaled to n triangles), or None."""
@@ -475,6 +597,11 @@ def main():
     ap.add_argument("--workload", default="clustered16M")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-meshes", type=int, default=4096)
+    ap.add_argument("--serve-rates", default="200,500,1000,2000,5000")
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-min-requests", type=int, default=1000)
+    ap.add_argument("--serve-max-requests", type=int, default=100_000)
+    ap.add_argument("--serve-pool", type=int, default=4)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -484,6 +611,10 @@ def main():
             run_reference(args, world, rank)
         elif args.workload == "batch":
             out = run_batched(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(out), flush=True)
+        elif args.workload == "served":
+            out = run_served(args, world, rank, local)
             if rank == 0:
                 print(json.dumps(out), flush=True)
         else:

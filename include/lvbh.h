@@ -146,7 +146,8 @@ LVBH_API int  lvbh_build_indexed(lvbh_ctx *ctx, const float *xyz, uint32_t num_v
  *                [seg_offsets[s], seg_offsets[s+1]); seg_offsets[0] = 0, non-decreasing,
  *                total = seg_offsets[num_segs] <= LVBH_MAX_TRIS.  Empty meshes are allowed.
  *   seg_bounds   HOST memory, 6 floats per mesh used as that mesh's MODEL_BOUNDS, or NULL =
- *                each mesh's own vertex box reduced on the device.
+ *                each mesh's own vertex box reduced on the device.  A mesh whose first value
+ *                is NaN is reduced on the device too (bounds given for some meshes only).
  *   bounds_out   HOST memory, 6 floats per mesh receiving the bounds each mesh was quantised
  *                with (written when the build completes: at lvbh_sync with LVBH_ASYNC), or NULL.
  *   out          total-sized result.  Mesh s (n_s triangles from o_s = seg_offsets[s]) owns
@@ -184,6 +185,73 @@ LVBH_API size_t lvbh_scratch_bytes(uint32_t num_tris);
 LVBH_API const char *lvbh_last_error(const lvbh_ctx *ctx);
 /* Library version string. */
 LVBH_API const char *lvbh_version(void);
+
+/* ---- build server: continuous batching under an HBM budget --------------------------
+ * No counterpart in the reference, whose build() is one awaited call per scene
+ * (scripts/bvh/build-bvh.js:12-66, scripts/main.js:88).  A server owns a scheduler thread,
+ * `slots` build contexts each on its own stream, and one device reservation of `hbm_budget`
+ * bytes that holds the contexts' scratch, each slot's staged input and every result until the
+ * client releases it.  Submitted requests queue; whenever a slot is free, the scheduler takes
+ * the queued requests in arrival order (up to max_batch_tris triangles and max_batch_reqs
+ * requests, and what the free result memory admits), copies their triangles into the slot's
+ * input, and runs one lvbh_build_batched over them.  Requests arriving while batches are on
+ * the GPU are coalesced into the next batch and their copies and kernels overlap the batches
+ * in flight.  Each result is bit-identical to lvbh_build_soup of the request alone. */
+typedef struct lvbh_server lvbh_server;
+
+typedef struct lvbh_server_config {
+    int      device;          /* CUDA device ordinal; -1 = the calling thread's current device */
+    uint32_t slots;           /* batches in flight at once (0 = 3) */
+    uint64_t hbm_budget;      /* device bytes for scratch, staged inputs and results (0 = 96 GB) */
+    uint32_t max_batch_tris;  /* largest batch and largest request (0 = 2^24) */
+    uint32_t max_batch_reqs;  /* most requests per batch (0 = 4096) */
+    uint32_t max_requests;    /* queued + in flight + unreleased (0 = 2^20); beyond: LVBH_EBUSY */
+    uint32_t pad;
+    uint64_t reserved[4];     /* must be zero */
+} lvbh_server_config;
+
+typedef struct lvbh_request_info {
+    int      status;      /* LVBH_OK, LVBH_EBUSY while not finished, else the build's error status */
+    uint32_t num_tris;
+    uint32_t batch_reqs;  /* requests in the batch that built it */
+    uint32_t batch_tris;  /* triangles in that batch */
+    double   queued_ms;   /* submit -> its batch was launched */
+    double   latency_ms;  /* submit -> its batch finished on the device */
+} lvbh_request_info;
+
+typedef struct lvbh_server_stats {
+    uint64_t submitted, completed, failed, batches, tris_built;
+    uint64_t budget_bytes;    /* the reservation */
+    uint64_t result_bytes;    /* part of it available to results */
+    uint64_t bytes_in_use;    /* results held now */
+    uint64_t peak_bytes;      /* most results held at once */
+    uint64_t admission_waits; /* times a queued batch waited for result memory */
+    uint32_t max_batch_seen;  /* most requests coalesced into one batch */
+    uint32_t pad;
+} lvbh_server_stats;
+
+LVBH_API int  lvbh_server_create(lvbh_server **srv, const lvbh_server_config *cfg);
+/* Finishes the queued and in-flight requests, then frees everything (results included). */
+LVBH_API void lvbh_server_destroy(lvbh_server *srv);
+/* Queues one build(TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS).  tri: 12 floats per triangle, device
+ * memory or (LVBH_INPUT_HOST) host memory - pinned host memory lets the copy overlap other
+ * batches; either must stay valid until the request has finished.  model_bounds: 6 host
+ * floats or NULL (reduce on the device), copied inside the call.  Returns LVBH_EINVAL for
+ * num_tris > max_batch_tris, LVBH_ENOMEM when the request could never fit the result memory,
+ * LVBH_EBUSY when max_requests are held. */
+LVBH_API int  lvbh_submit(lvbh_server *srv, const float *tri, uint32_t num_tris,
+                          const float *model_bounds, uint32_t flags, uint64_t *ticket);
+/* LVBH_EBUSY while the request is not finished; then its status, with *out (device pointers
+ * into the server's memory, valid until lvbh_request_release) and *info filled.  out and info
+ * may be NULL.  LVBH_EINVAL for an unknown ticket. */
+LVBH_API int  lvbh_poll(lvbh_server *srv, uint64_t ticket, lvbh_result *out, lvbh_request_info *info);
+/* As lvbh_poll, waiting up to timeout_ms (< 0: without limit) for the request to finish. */
+LVBH_API int  lvbh_wait(lvbh_server *srv, uint64_t ticket, int timeout_ms, lvbh_result *out,
+                        lvbh_request_info *info);
+/* Returns a finished request's result memory to the server (LVBH_EBUSY if not finished). */
+LVBH_API int  lvbh_request_release(lvbh_server *srv, uint64_t ticket);
+LVBH_API int  lvbh_server_stats_get(lvbh_server *srv, lvbh_server_stats *out);
+LVBH_API const char *lvbh_server_last_error(const lvbh_server *srv);
 
 /* ---- allocation-free sort -------------------------------------------------------------
  * No counterpart in the reference.  The build's stable radix sort of (key, index), for callers

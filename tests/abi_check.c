@@ -26,5 +26,22 @@ int main(void) {
     printf("copy_null %d\n", lvbh_copy_to_host(NULL, NULL, NULL, 0, NULL));
     printf("last_error_null %s\n", lvbh_last_error(NULL));
     printf("scratch_1M %zu\n", lvbh_scratch_bytes(1u << 20));
+    printf("batched_null_ctx %d\n", lvbh_build_batched(NULL, NULL, NULL, 0, NULL, NULL, 0, &r, NULL));
+    printf("sizeof_server_config %zu\n", sizeof(lvbh_server_config));
+    printf("sizeof_request_info %zu\n", sizeof(lvbh_request_info));
+    printf("off_latency %zu\n", offsetof(lvbh_request_info, latency_ms));
+    printf("sizeof_server_stats %zu\n", sizeof(lvbh_server_stats));
+    printf("off_max_batch_seen %zu\n", offsetof(lvbh_server_stats, max_batch_seen));
+    {
+        uint64_t t = 0;
+        printf("server_create_null %d\n", lvbh_server_create(NULL, NULL));
+        printf("submit_null %d\n", lvbh_submit(NULL, NULL, 0, NULL, 0, &t));
+        printf("poll_null %d\n", lvbh_poll(NULL, 1, NULL, NULL));
+        printf("wait_null %d\n", lvbh_wait(NULL, 1, 0, NULL, NULL));
+        printf("release_req_null %d\n", lvbh_request_release(NULL, 1));
+        printf("stats_null %d\n", lvbh_server_stats_get(NULL, NULL));
+        printf("server_error_null %s\n", lvbh_server_last_error(NULL));
+        lvbh_server_destroy(NULL);
+    }
     return 0;
 }

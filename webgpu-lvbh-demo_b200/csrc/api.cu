@@ -4,6 +4,7 @@
 // module's execute(): 69 queue submits and 20 host waits per build) with one stream-ordered
 // chain of 8 kernels and a memset, replayed as a cached CUDA graph when the same build shape
 // repeats, and a single host wait at the end (none with LVBH_ASYNC).
+#include <cmath>
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
@@ -290,7 +291,7 @@ void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool u
     const uint32_t *zero_end = ctx->b_lookback + (size_t)kSortPasses * bp.tiles * kDigits;
     cudaMemsetAsync(ctx->b_zero, 0, (zero_end - ctx->b_zero) * sizeof(uint32_t), s);
     launch_seg_tables(ctx->b_rows, bp.num_segs, ctx->b_tile_seg, ctx->b_blk_seg, s);
-    if (!use_bounds) launch_bounds_batch(bp, tri, ctx->b_ord, s);
+    launch_bounds_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, s);
     if (profile) cudaEventRecord(ctx->ev[2], s);
     launch_morton_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, ctx->b_hist,
                         ctx->ctl, out->morton, ctx->epoch, s);
@@ -455,6 +456,32 @@ int check_out(lvbh_ctx *ctx, uint32_t n, uint32_t flags, lvbh_result *out) {
 
 }  // namespace
 
+namespace lvbh {
+
+int ctx_reserve_batch(lvbh_ctx *ctx, uint32_t max_tris, uint32_t max_segs) {
+    if (!ctx) return LVBH_EINVAL;
+    DeviceGuard g(ctx->device);
+    if (int rc = ensure_arena(ctx, max_tris)) return rc;
+    return ensure_batch(ctx, max_segs, sort_tiles(max_tris) + max_segs,
+                        (uint32_t)emit_groups(max_tris) + max_segs);
+}
+
+size_t ctx_device_bytes(const lvbh_ctx *ctx) {
+    if (!ctx || !ctx->arena) return 0;
+    const uint32_t segs = ctx->b_segs, tiles = ctx->b_tiles, blocks = ctx->b_blocks;
+    size_t batch = 0;
+    if (ctx->b_dev) {
+        batch = align_up((segs + 1ull) * sizeof(SegRow)) + align_up(tiles * 4ull) + align_up(blocks * 4ull) +
+                align_up((size_t)segs * 6 * 4 + (size_t)segs * kSortPasses * kDigits * 4 +
+                         (size_t)kSortPasses * tiles * kDigits * 4) +
+                align_up((size_t)segs * 6 * 4) + align_up((size_t)blocks * kOpenCap * sizeof(OpenItem)) +
+                align_up(blocks * 4ull);
+    }
+    return arena_bytes(ctx->cap) + batch + ctx->stage_bytes;
+}
+
+}  // namespace lvbh
+
 extern "C" {
 
 const char *lvbh_version(void) { return "lvbh-b200 0.1 (sm_100a)"; }
@@ -590,8 +617,8 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
     if (total == 0) {
         ctx->pending = false;
         ctx->ev_valid = false;
-        if (bounds_out && seg_bounds) std::memcpy(bounds_out, seg_bounds, num_segs * 6ull * sizeof(float));
-        else if (bounds_out) std::memset(bounds_out, 0, num_segs * 6ull * sizeof(float));
+        for (uint64_t i = 0; bounds_out && i < num_segs * 6ull; ++i)
+            bounds_out[i] = (seg_bounds && !std::isnan(seg_bounds[i - i % 6])) ? seg_bounds[i] : 0.0f;
         return LVBH_OK;
     }
     if (int rc = ensure_arena(ctx, total)) return rc;
@@ -631,7 +658,7 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
     ctx->ev_valid = profile;
     LVBH_CUDA(ctx, cudaMemcpyAsync(ctx->host_ctl, ctx->ctl, offsetof(Control, pad1),
                                    cudaMemcpyDeviceToHost, s));
-    if (bounds_out && !seg_bounds)
+    if (bounds_out)
         LVBH_CUDA(ctx, cudaMemcpyAsync(ctx->bh_ord, ctx->b_ord, num_segs * 6ull * 4,
                                        cudaMemcpyDeviceToHost, s));
     ctx->last_stream = s;
@@ -656,12 +683,13 @@ int lvbh_sync(lvbh_ctx *ctx) {
     const uint32_t err = ctx->host_ctl[0] | ctx->host_ctl[1];
     if (ctx->last_batch) {
         if (ctx->last_bounds_out) {
-            if (ctx->last_hb.use) {
-                std::memcpy(ctx->last_bounds_out, ctx->bh_bounds, ctx->last_segs * 6ull * sizeof(float));
-            } else {
-                for (uint64_t i = 0; i < ctx->last_segs * 6ull; ++i) {
+            for (uint64_t i = 0; i < ctx->last_segs * 6ull; ++i) {
+                const uint64_t sg = i / 6;
+                if (ctx->last_hb.use && !std::isnan(ctx->bh_bounds[6 * sg])) {
+                    ctx->last_bounds_out[i] = ctx->bh_bounds[i];
+                } else {
                     const uint32_t o = ctx->bh_ord[i];
-                    const bool empty = ctx->bh_rows[i / 6 + 1].tri == ctx->bh_rows[i / 6].tri;
+                    const bool empty = ctx->bh_rows[sg + 1].tri == ctx->bh_rows[sg].tri;
                     ctx->last_bounds_out[i] = empty ? 0.0f : ord_word_to_float((i % 6) < 3 ? ~o : o);
                 }
             }

@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+struct lvbh_ctx;
+
 namespace lvbh {
 
 // Radix sort geometry: 8-bit digits, four passes cover every bit of a 32-bit key (Morton keys
@@ -66,6 +68,11 @@ struct BatchPlan {
 
 int sm_count();
 
+// Server support (api.cu): size a context's scratch for batched builds of up to max_tris
+// triangles in up to max_segs meshes, and report the device bytes the context holds.
+int ctx_reserve_batch(lvbh_ctx *ctx, uint32_t max_tris, uint32_t max_segs);
+size_t ctx_device_bytes(const lvbh_ctx *ctx);
+
 // K1a: scene box over every vertex of the 48-byte triangle soup.
 void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s);
 // K1b: triangle box centroid -> Morton key (input order) + the four digit histograms; flags
@@ -90,11 +97,12 @@ void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, 
 // Batched forms of K1a, K1b, K2 and K3 over the segments of `bp`.  seg_ord holds 6 ordered
 // bound words per segment (zeroed before K1a; min at 0-2 as ~ord_lo, max at 3-5 as ord_lo),
 // seg_hist 4 x 256 digit counts per segment (zeroed before K1b); host_bounds, when not null,
-// holds 6 floats per segment that replace the device reduction.  K2's look-back words:
-// bp.tiles * 256 per pass, zeroed before the build.
+// holds 6 floats per segment that replace the device reduction for every segment whose first
+// value is not NaN.  K2's look-back words: bp.tiles * 256 per pass, zeroed before the build.
 void launch_seg_tables(const SegRow *rows, uint32_t num_segs, uint32_t *tile_seg,
                        uint32_t *blk_seg, cudaStream_t s);
-void launch_bounds_batch(const BatchPlan &bp, const float4 *tri, uint32_t *seg_ord, cudaStream_t s);
+void launch_bounds_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,
+                         uint32_t *seg_ord, cudaStream_t s);
 void launch_morton_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,
                          const uint32_t *seg_ord, uint32_t *seg_hist, Control *ctl,
                          uint32_t *keys_out, uint32_t *epoch, cudaStream_t s);

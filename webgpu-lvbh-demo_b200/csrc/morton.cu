@@ -137,8 +137,10 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
 __global__ void __launch_bounds__(kThreads) k_bounds_batch(const float4 *__restrict__ tri,
                                                            const SegRow *__restrict__ rows,
                                                            const uint32_t *__restrict__ tile_seg,
+                                                           const float *__restrict__ host_bounds,
                                                            uint32_t *__restrict__ seg_ord) {
     const uint32_t tile = blockIdx.x, sg = __ldg(tile_seg + tile);
+    if (host_bounds && !isnan(__ldg(host_bounds + 6ull * sg))) return;  // bounds given
     const uint32_t t0 = __ldg(&rows[sg].tri), t1 = __ldg(&rows[sg + 1].tri);
     const uint32_t first = t0 + (tile - __ldg(&rows[sg].tile)) * (uint32_t)kSortTile;
     const uint32_t cnt = min((uint32_t)kSortTile, t1 - first);
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restr
     const uint32_t first = t0 + (tile - __ldg(&rows[sg].tile)) * (uint32_t)kSortTile;
     const uint32_t cnt = min((uint32_t)kSortTile, t1 - first);
     float umin[3], umax[3];
-    if (host_bounds) {
+    if (host_bounds && !isnan(host_bounds[6ull * sg])) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) { umin[a] = host_bounds[6ull * sg + a]; umax[a] = host_bounds[6ull * sg + 3 + a]; }
     } else {
@@ -304,9 +306,10 @@ void launch_seg_tables(const SegRow *rows, uint32_t num_segs, uint32_t *tile_seg
     k_seg_tables<<<(num_segs + 7) / 8, 256, 0, s>>>(rows, num_segs, tile_seg, blk_seg);
 }
 
-void launch_bounds_batch(const BatchPlan &bp, const float4 *tri, uint32_t *seg_ord, cudaStream_t s) {
+void launch_bounds_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,
+                         uint32_t *seg_ord, cudaStream_t s) {
     if (bp.tiles == 0) return;
-    k_bounds_batch<<<bp.tiles, kThreads, 0, s>>>(tri, bp.rows, bp.tile_seg, seg_ord);
+    k_bounds_batch<<<bp.tiles, kThreads, 0, s>>>(tri, bp.rows, bp.tile_seg, host_bounds, seg_ord);
 }
 
 void launch_morton_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,

@@ -45,6 +45,26 @@ class Result(ctypes.Structure):
                 ("owned", ctypes.c_uint32)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_uint32),
+                ("hbm_budget", ctypes.c_uint64), ("max_batch_tris", ctypes.c_uint32),
+                ("max_batch_reqs", ctypes.c_uint32), ("max_requests", ctypes.c_uint32),
+                ("pad", ctypes.c_uint32), ("reserved", ctypes.c_uint64 * 4)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("num_tris", ctypes.c_uint32),
+                ("batch_reqs", ctypes.c_uint32), ("batch_tris", ctypes.c_uint32),
+                ("queued_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in
+                ("submitted", "completed", "failed", "batches", "tris_built", "budget_bytes",
+                 "result_bytes", "bytes_in_use", "peak_bytes", "admission_waits")] + \
+               [("max_batch_seen", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {os.path.dirname(HERE)}` "
@@ -77,6 +97,22 @@ def _load():
     L.lvbh_copy_to_host.argtypes = [vp, vp, vp, ctypes.c_size_t, vp]
     L.lvbh_sort_pairs_noalloc.restype = i32
     L.lvbh_sort_pairs_noalloc.argtypes = [vp, u32, vp, vp, vp]
+    L.lvbh_server_create.restype = i32
+    L.lvbh_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ServerConfig)]
+    L.lvbh_server_destroy.restype = None
+    L.lvbh_server_destroy.argtypes = [vp]
+    L.lvbh_submit.restype = i32
+    L.lvbh_submit.argtypes = [vp, vp, u32, vp, u32, ctypes.POINTER(ctypes.c_uint64)]
+    L.lvbh_poll.restype = i32
+    L.lvbh_poll.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(Result), ctypes.POINTER(RequestInfo)]
+    L.lvbh_wait.restype = i32
+    L.lvbh_wait.argtypes = [vp, ctypes.c_uint64, i32, ctypes.POINTER(Result), ctypes.POINTER(RequestInfo)]
+    L.lvbh_request_release.restype = i32
+    L.lvbh_request_release.argtypes = [vp, ctypes.c_uint64]
+    L.lvbh_server_stats_get.restype = i32
+    L.lvbh_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    L.lvbh_server_last_error.restype = ctypes.c_char_p
+    L.lvbh_server_last_error.argtypes = [vp]
     L.lvbh_trace.restype = i32
     L.lvbh_trace.argtypes = [vp, vp, vp, u32, vp, u32, vp, vp, vp, vp]
     return L
