@@ -16,7 +16,14 @@ Prints one JSON line (rank 0).  Fields beyond the base contract:
   cpu_baseline  the CPU restatement of the reference build timed on this host's cores
   e2e           through the public C ABI from pinned host memory: H2D of the soup, the build,
                 D2H of the root node record, every step
+  batched       the 4096-mesh batch (log-uniform 64..262,144 triangles per mesh) built by one
+                lvbh_build_batched call vs the plain builder called once per mesh, identical trees
+  served        the build server under Poisson arrivals at 200..5000 requests/s (sizes
+                log-uniform in 1,024..4,194,304): p50/p99/p99.9 latency and builds/s beside the
+                plain per-request builder on the same arrival trace (1 GPU only)
 Under torchrun (N > 1) each rank builds its own replica (the build has no shardable exchange).
+
+    python bench.py --workload batch | served     the batched / served part alone
 """
 from __future__ import annotations
 
@@ -324,6 +331,14 @@ def run_ours(args, world, rank, local):
         cpu = cpu_baseline(tri)
 
     builder.close()
+    del dtri, outs, htri
+    torch.cuda.empty_cache()
+    batched = served = None
+    if not args.no_batched:
+        batched = run_batched(args, world, rank, local)
+        torch.cuda.empty_cache()
+    if not args.no_served and world == 1:
+        served = run_served(args, world, rank, local)
     if rank != 0:
         return
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -334,7 +349,7 @@ def run_ours(args, world, rank, local):
                        "l2": "input soup 805 MB > 126 MB L2; no flush", "graph": True},
             "gpu_launches": LAUNCHES_PER_BUILD * args.steps,
             "roofline": roofline, "stage_ms": stage_ms, "cpu_baseline": cpu, "e2e": e2e_line,
-            "clocks": clock_summary}
+            "clocks": clock_summary, "batched": batched, "served": served}
     print(json.dumps(line), flush=True)
 
 
@@ -597,6 +612,8 @@ def main():
     ap.add_argument("--workload", default="clustered16M")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-meshes", type=int, default=4096)
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--serve-rates", default="200,500,1000,2000,5000")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-min-requests", type=int, default=1000)

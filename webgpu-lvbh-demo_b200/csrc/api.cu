@@ -38,8 +38,9 @@ namespace {
 constexpr size_t kAlign = 256;
 inline size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
+// The control block and the sort's tile / chunk histograms.
 size_t control_bytes(uint32_t n) {
-    return align_up(sizeof(Control)) + (size_t)kSortPasses * sort_tiles(n) * kDigits * sizeof(uint32_t);
+    return align_up(sizeof(Control)) + sort_scratch_words(n) * sizeof(uint32_t);
 }
 
 // Scratch of a context sized for `cap` triangles: sort ping-pong keys and values, the tree
@@ -81,7 +82,7 @@ struct lvbh_ctx {
     uint32_t *counts = nullptr, *arrive = nullptr, *epoch = nullptr;
     float4 *pend = nullptr;
     Control *ctl = nullptr;
-    uint32_t *lookback = nullptr;
+    uint32_t *lookback = nullptr;  // the sort's tile and chunk histograms
     // staging for host input
     size_t stage_bytes = 0;
     void *stage = nullptr;
@@ -260,16 +261,17 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
                    const lvbh_result *out, cudaStream_t s, bool profile) {
     if (profile) cudaEventRecord(ctx->ev[1], s);
     cudaMemsetAsync(reinterpret_cast<char *>(ctx->ctl) + offsetof(Control, err), 0,
-                    control_bytes(n) - offsetof(Control, err), s);
+                    sizeof(Control) - offsetof(Control, err), s);
     if (!hb.use) launch_bounds(tri, n, ctx->ctl, s);
     if (profile) cudaEventRecord(ctx->ev[2], s);
-    launch_morton(tri, n, hb, ctx->ctl, out->morton, ctx->epoch, s);
+    // unsorted keys go to the leaf-box scratch (unused until K3a), so that the three passes
+    // ping-pong scratch -> result -> scratch -> result
+    uint32_t *keys_a = reinterpret_cast<uint32_t *>(ctx->lbox);
+    launch_morton(tri, n, hb, ctx->ctl, keys_a, ctx->epoch, s);
     if (profile) cudaEventRecord(ctx->ev[3], s);
-    // ping-pong so that the last pass lands in the result buffers
-    launch_onesweep(out->morton, nullptr, ctx->keys_b, ctx->vals_b, n, 0, ctx->ctl, ctx->lookback, s);
-    launch_onesweep(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 1, ctx->ctl, ctx->lookback, s);
-    launch_onesweep(out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, n, 2, ctx->ctl, ctx->lookback, s);
-    launch_onesweep(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 3, ctx->ctl, ctx->lookback, s);
+    launch_sort_pass(keys_a, nullptr, out->morton, out->leaf_index, n, 0, ctx->ctl, ctx->lookback, s);
+    launch_sort_pass(out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, n, 1, ctx->ctl, ctx->lookback, s);
+    launch_sort_pass(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 2, ctx->ctl, ctx->lookback, s);
     if (profile) cudaEventRecord(ctx->ev[4], s);
     launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
                 static_cast<float4 *>(out->nodes), out->parents, ctx->lbox, ctx->items, ctx->counts,
@@ -293,13 +295,13 @@ void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool u
     launch_seg_tables(ctx->b_rows, bp.num_segs, ctx->b_tile_seg, ctx->b_blk_seg, s);
     launch_bounds_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, s);
     if (profile) cudaEventRecord(ctx->ev[2], s);
+    uint32_t *keys_a = reinterpret_cast<uint32_t *>(ctx->lbox);  // as in enqueue_build
     launch_morton_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, ctx->b_hist,
-                        ctx->ctl, out->morton, ctx->epoch, s);
+                        ctx->ctl, keys_a, ctx->epoch, s);
     if (profile) cudaEventRecord(ctx->ev[3], s);
-    launch_onesweep_batch(bp, out->morton, nullptr, ctx->keys_b, ctx->vals_b, 0, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
-    launch_onesweep_batch(bp, ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, 1, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
-    launch_onesweep_batch(bp, out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, 2, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
-    launch_onesweep_batch(bp, ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, 3, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    launch_onesweep_batch(bp, keys_a, nullptr, out->morton, out->leaf_index, 0, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    launch_onesweep_batch(bp, out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, 1, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    launch_onesweep_batch(bp, ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, 2, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
     if (profile) cudaEventRecord(ctx->ev[4], s);
     launch_emit_batch(bp, tri, out->leaf_index, out->morton, static_cast<float4 *>(out->tris),
                       static_cast<float4 *>(out->nodes), out->parents, ctx->lbox, ctx->b_items,
@@ -501,7 +503,11 @@ int lvbh_create(lvbh_ctx **out, const lvbh_config *cfg) {
     for (auto &e : ctx->ev) {
         if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); lvbh_destroy(ctx); return LVBH_ECUDA; }
     }
-    if (emit_init() != cudaSuccess) { cudaGetLastError(); lvbh_destroy(ctx); return LVBH_ECUDA; }
+    if (emit_init() != cudaSuccess || sort_init() != cudaSuccess) {
+        cudaGetLastError();
+        lvbh_destroy(ctx);
+        return LVBH_ECUDA;
+    }
     if (cfg && cfg->reserve_tris) {
         if (cfg->reserve_tris > LVBH_MAX_TRIS) { lvbh_destroy(ctx); return LVBH_EINVAL; }
         if (int rc = ensure_arena(ctx, cfg->reserve_tris)) { lvbh_destroy(ctx); return rc; }

@@ -9,16 +9,22 @@ struct lvbh_ctx;
 
 namespace lvbh {
 
-// Radix sort geometry: 8-bit digits, four passes cover every bit of a 32-bit key (Morton keys
-// use 30 bits; keys of triangles outside host-supplied bounds may use all 32).
-constexpr int kDigitBits = 8;
+// Radix sort geometry of the build: Morton keys are below 2^30 (split_3's last mask tops out
+// at bit 27, shifted left by 2), so three passes of 10-bit digits cover every key bit.
+constexpr int kDigitBits = 10;
 constexpr int kDigits = 1 << kDigitBits;
-constexpr int kSortPasses = 4;
+constexpr int kSortPasses = 3;
+// Full 32-bit keys (the allocation-free sort of caller keys): four passes of 8-bit digits.
+constexpr int kDigitBits32 = 8;
+constexpr int kDigits32 = 1 << kDigitBits32;
+constexpr int kSortPasses32 = 4;
+constexpr int kHistWords = kSortPasses * kDigits;  // also holds the 4 x 256 counts of 32-bit keys
+static_assert(kSortPasses32 * kDigits32 <= kHistWords, "histogram space");
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;                       // keys per thread
 constexpr int kSortTile = kSortThreads * kSortItems; // keys per tile (4096)
 
-inline uint32_t sort_tiles(uint32_t n) { return (n + kSortTile - 1) / kSortTile; }
+__host__ __device__ inline uint32_t sort_tiles(uint32_t n) { return (n + kSortTile - 1) / kSortTile; }
 
 // Tree/refit pass: leaves per block of the in-block tree pass (one thread each); open nodes a
 // block can leave to the straddling pass (at most 2 x the tree depth 64).
@@ -39,11 +45,11 @@ struct __align__(16) OpenItem {
 struct Control {
     uint32_t aux_err;
     uint32_t err;
-    uint32_t tile_counter[kSortPasses];
+    uint32_t tile_counter[kSortPasses32];
     uint32_t pad0[2];
-    uint32_t bounds_ord[6];            // scene min (ord_hi) and max (ord_lo), see lvbh_device.cuh
+    uint32_t bounds_ord[6];   // scene min (ord_hi) and max (ord_lo), see lvbh_device.cuh
     uint32_t pad1[2];
-    uint32_t hist[kSortPasses][kDigits]; // global digit counts of the unsorted keys
+    uint32_t hist[kHistWords];  // global digit counts of the unsorted keys, pass-major
 };
 
 struct HostBounds {
@@ -79,10 +85,19 @@ void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s);
 // non-finite vertices in ctl->err and advances the build epoch *epoch used by K3c.
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl,
                    uint32_t *keys_out, uint32_t *epoch, cudaStream_t s);
-// K2: one onesweep pass over digit `pass`.  vals_in == nullptr generates the identity.
-void launch_onesweep(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
-                     uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *lookback,
-                     cudaStream_t s);
+// K2: one reduce-then-scan pass over 10-bit digit `pass` (0..2) of 30-bit keys (three
+// launches; the global digit counts come from ctl->hist).  vals_in == nullptr generates the
+// identity.  scratch: sort_scratch_words(n) words, no initialisation needed.
+size_t sort_scratch_words(uint32_t n);
+void launch_sort_pass(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
+                      uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *scratch,
+                      cudaStream_t s);
+// The same over 8-bit digit `pass` (0..3) of full 32-bit keys (counts in ctl->hist pass-major,
+// 256 per pass; look-back words kSortPasses32 * sort_tiles(n) * kDigits32).
+void launch_onesweep32(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
+                       uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *lookback,
+                       cudaStream_t s);
+cudaError_t sort_init();  // once per device, before the first launch
 // K3: leaf gather + rearrange (K3a), in-block radix tree + refit (K3b), straddling nodes (K3c)
 // -> BVH nodes, parent links, sorted triangles.  Scratch: lbox (3 float2 per triangle),
 // items (emit_groups(n) * kOpenCap) and counts (emit_groups(n)), arrive (n words, zero or

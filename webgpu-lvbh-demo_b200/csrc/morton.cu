@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
     __syncthreads();
     for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) {
         const uint32_t c = (&hist[0][0])[i];
-        if (c) atomicAdd(&ctl->hist[0][0] + i, c);
+        if (c) atomicAdd(ctl->hist + i, c);
     }
 }
 

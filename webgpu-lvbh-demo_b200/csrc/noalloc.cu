@@ -34,28 +34,28 @@ namespace {
 constexpr uint32_t kMaxKeys = LVBH_NOALLOC_MAX_KEYS;
 constexpr uint32_t kMaxTiles = (kMaxKeys + kSortTile - 1) / kSortTile;
 constexpr size_t kControlWords = (sizeof(Control) + 255) / 256 * 256 / 4;
-constexpr size_t kLookbackWords = (size_t)kSortPasses * kMaxTiles * kDigits;
+constexpr size_t kLookbackWords = (size_t)kSortPasses32 * kMaxTiles * kDigits32;
 constexpr size_t kScratchWords = kControlWords + kLookbackWords + 2ull * kMaxKeys;
 
 // Scratch of the allocation-free sort: [Control][look-back words][keys][values].
 static __device__ __align__(256) uint32_t g_scratch[kScratchWords];
 
-// Digit histograms of all four passes for keys that did not come from K1b.
+// Digit histograms of all four 8-bit passes of full 32-bit keys.
 __global__ void __launch_bounds__(256) k_digit_hist(const uint32_t *__restrict__ keys, uint32_t n,
                                                     Control *__restrict__ ctl) {
-    __shared__ uint32_t hist[kSortPasses][kDigits];
-    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += 256) (&hist[0][0])[i] = 0;
+    __shared__ uint32_t hist[kSortPasses32][kDigits32];
+    for (int i = threadIdx.x; i < kSortPasses32 * kDigits32; i += 256) (&hist[0][0])[i] = 0;
     __syncthreads();
     for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
         const uint32_t key = __ldg(keys + i);
 #pragma unroll
-        for (int p = 0; p < kSortPasses; ++p)
-            atomicAdd(&hist[p][(key >> (kDigitBits * p)) & (kDigits - 1)], 1u);
+        for (int p = 0; p < kSortPasses32; ++p)
+            atomicAdd(&hist[p][(key >> (kDigitBits32 * p)) & (kDigits32 - 1)], 1u);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += 256) {
+    for (int i = threadIdx.x; i < kSortPasses32 * kDigits32; i += 256) {
         const uint32_t c = (&hist[0][0])[i];
-        if (c) atomicAdd(&ctl->hist[0][0] + i, c);
+        if (c) atomicAdd(ctl->hist + i, c);
     }
 }
 
@@ -87,6 +87,10 @@ extern "C" int lvbh_sort_pairs_noalloc(const uint32_t *keys_in, uint32_t num_key
                 cudaGetLastError();
                 return LVBH_ECUDA;
             }
+            if (sort_init() != cudaSuccess) {
+                cudaGetLastError();
+                return LVBH_ECUDA;
+            }
             g_addr[dev] = p;
         }
         base = g_addr[dev];
@@ -98,15 +102,15 @@ extern "C" int lvbh_sort_pairs_noalloc(const uint32_t *keys_in, uint32_t num_key
     uint32_t *keys_b = lookback + kLookbackWords;
     uint32_t *vals_b = keys_b + kMaxKeys;
     // what must start at zero: the error words, tile counters, histograms and look-back words
-    const size_t zero_bytes = (kControlWords + (size_t)kSortPasses * sort_tiles(num_keys) * kDigits) * 4;
+    const size_t zero_bytes = (kControlWords + (size_t)kSortPasses32 * sort_tiles(num_keys) * kDigits32) * 4;
     if (cudaMemsetAsync(words, 0, zero_bytes, s) != cudaSuccess) { cudaGetLastError(); return LVBH_ECUDA; }
     int blocks = (int)((num_keys + 255) / 256);
     if (blocks > sm_count() * 4) blocks = sm_count() * 4;
     k_digit_hist<<<blocks, 256, 0, s>>>(keys_in, num_keys, ctl);
-    launch_onesweep(keys_in, nullptr, keys_b, vals_b, num_keys, 0, ctl, lookback, s);
-    launch_onesweep(keys_b, vals_b, keys_out, perm_out, num_keys, 1, ctl, lookback, s);
-    launch_onesweep(keys_out, perm_out, keys_b, vals_b, num_keys, 2, ctl, lookback, s);
-    launch_onesweep(keys_b, vals_b, keys_out, perm_out, num_keys, 3, ctl, lookback, s);
+    launch_onesweep32(keys_in, nullptr, keys_b, vals_b, num_keys, 0, ctl, lookback, s);
+    launch_onesweep32(keys_b, vals_b, keys_out, perm_out, num_keys, 1, ctl, lookback, s);
+    launch_onesweep32(keys_out, perm_out, keys_b, vals_b, num_keys, 2, ctl, lookback, s);
+    launch_onesweep32(keys_b, vals_b, keys_out, perm_out, num_keys, 3, ctl, lookback, s);
     if (cudaGetLastError() != cudaSuccess) return LVBH_ECUDA;
     uint32_t err = 0;
     if (cudaMemcpyAsync(&err, &ctl->err, sizeof err, cudaMemcpyDeviceToHost, s) != cudaSuccess ||

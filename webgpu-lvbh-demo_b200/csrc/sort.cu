@@ -3,12 +3,14 @@
 // Replaces the reference's 2-bit x 16-pass sort (scripts/bvh/kernels/radix-sort.js:162-499:
 // init_idx, init_off, two scan_up levels and scan_and_sort per pass, 64 submits and 16 host
 // waits).  Its result is the stable argsort of the keys - ties keep ascending input index -
-// and this pass keeps that contract with 8-bit digits, four passes over 32 bits:
+// and this pass keeps that contract.  The build's keys have 30 bits, sorted in three passes of
+// 10-bit digits; full 32-bit keys (the allocation-free entry point) take four 8-bit passes.
 //
 //   * the global digit counts of every pass come from K1b's histograms (one read of the keys);
 //   * a tile of 4096 keys (256 threads x 16) is ranked in shared memory: each warp walks its
-//     keys in input order, __match_any_sync groups equal digits, and the peers' lane order
-//     plus a per-warp running count gives each key its stable rank;
+//     keys in input order; the lanes holding the same digit (its peers) are found with one
+//     ballot per digit bit, and the peers' lane order plus a per-warp running count in a
+//     16-bit shared counter gives each key its stable rank;
 //   * the tile's digit counts are combined with earlier tiles by decoupled look-back: tiles
 //     are numbered by an atomic counter in launch order, each publishes its counts (flag
 //     AGGREGATE) and then its inclusive prefix (flag PREFIX) in one 32-bit word per digit, and
@@ -18,8 +20,18 @@
 //   * keys and values are staged in digit order in shared memory and written out so that
 //     consecutive threads write consecutive addresses of each digit's run.
 //
+// The plain build sorts one array of up to 2^29 keys, thousands of tiles long.  There a
+// look-back over 1024 digits would read 4 KB per predecessor tile and walk back about half a
+// wave of resident tiles, so its pass runs reduce-then-scan instead, with no waits at all:
+//   k_tile_hist   per tile of 4096 keys its digit counts, per chunk of 8 tiles their sum;
+//   k_chunk_scan  per chunk and digit the global output offset of the chunk's first key
+//                 (exclusive scan over chunks plus the digit's global start);
+//   k_scatter     ranks its tile as above, adds the counts of the earlier tiles of its chunk
+//                 (at most 7 rows of 4 KB, already final) to the chunk offset, and scatters.
+// The batched build's segments span at most 64 tiles, so it keeps the one-kernel look-back.
+//
 // HBM-bound: per key one 4-byte key read (+4-byte value read after the first pass) and two
-// 4-byte writes.
+// 4-byte writes (+ the 4-byte key read of k_tile_hist when reducing first).
 #include "lvbh_device.cuh"
 #include "lvbh_internal.h"
 
@@ -33,9 +45,7 @@ constexpr int IPT = kSortItems;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1u;
-constexpr int kLookback = 8;  // predecessor tiles read per look-back step
-
-static_assert(T == kDigits, "one thread per digit in the per-digit phases");
+constexpr int kLookback = 4;  // predecessor tiles read per look-back step and digit
 
 // Exclusive scan of one value per thread across the block; returns the thread's prefix.
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s_warp) {
@@ -86,33 +96,42 @@ struct ManySegSort {
     }
 };
 
-template <class Segs>
+template <int BITS>
+struct SortSmem {
+    static constexpr int D = 1 << BITS;
+    uint32_t keys[kSortTile];
+    uint32_t vals[kSortTile];
+    uint16_t whist[W][D];  // per-warp digit counts, then per-warp staging offsets
+    uint32_t out[D];       // output position of staged index 0 of each digit
+    uint32_t warp[W];
+    uint32_t tile;
+};
+
+template <int BITS, class Segs>
 __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__restrict__ keys_all,
                                                 const uint32_t *__restrict__ vals_all,
                                                 uint32_t *__restrict__ keys_out_all,
                                                 uint32_t *__restrict__ vals_out_all, int pass,
                                                 Control *__restrict__ ctl,
                                                 uint32_t *__restrict__ lookback) {
-    __shared__ uint32_t s_keys[kSortTile];
-    __shared__ uint32_t s_vals[kSortTile];
-    __shared__ uint32_t s_whist[W][kDigits];
-    __shared__ uint32_t s_tile_start[kDigits];
-    __shared__ uint32_t s_out[kDigits];
-    __shared__ uint32_t s_warp[W];
-    __shared__ uint32_t s_tile;
+    constexpr int D = 1 << BITS;
+    constexpr int P = D / T;  // digits per thread in the per-digit phases (contiguous)
+    static_assert(P >= 1 && P * T == D, "digits per thread");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SortSmem<BITS> &S = *reinterpret_cast<SortSmem<BITS> *>(smem_raw);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter[pass], 1u);
-    for (int i = tid; i < W * kDigits; i += T) (&s_whist[0][0])[i] = 0;
+    if (tid == 0) S.tile = atomicAdd(&ctl->tile_counter[pass], 1u);
+    for (int i = tid; i < W * D / 2; i += T) reinterpret_cast<uint32_t *>(&S.whist[0][0])[i] = 0;
     __syncthreads();
-    const uint32_t tile = s_tile;
+    const uint32_t tile = S.tile;
     const TileSpan sp = segs.span(tile);
     const uint32_t n = sp.n, tile_base = sp.base;
     const uint32_t *keys_in = keys_all + sp.start;
     const uint32_t *vals_in = vals_all ? vals_all + sp.start : nullptr;
     uint32_t *keys_out = keys_out_all + sp.start;
     uint32_t *vals_out = vals_out_all + sp.start;
-    const int shift = pass * kDigitBits;
+    const int shift = pass * BITS;
     const uint32_t wbase = tile_base + warp * (IPT * 32);
 
     uint32_t k[IPT];
@@ -122,9 +141,6 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
         k[i] = idx < n ? __ldcs(keys_in + idx) : 0u;
     }
 
-    // Global start of this thread's digit: exclusive scan of the pass's digit counts.
-    const uint32_t digit_base = block_exclusive_scan(__ldg(sp.hist + tid), s_warp);
-
     // Stable in-warp ranking, keys visited in input order (item-major, then lane).
     uint32_t rank[IPT / 2];  // two 16-bit ranks per word
     const uint32_t lt = lanemask_lt();
@@ -132,55 +148,111 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
     for (int i = 0; i < IPT; ++i) {
         const uint32_t idx = wbase + i * 32 + lane;
         const bool valid = idx < n;
-        const uint32_t d = valid ? (k[i] >> shift) & (kDigits - 1) : (uint32_t)kDigits + lane;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        const uint32_t d = (k[i] >> shift) & (D - 1);
+        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+        for (int b = 0; b < BITS; ++b) {
+            const uint32_t bit = (d >> b) & 1u;
+            const uint32_t vote = __ballot_sync(0xFFFFFFFFu, bit);
+            peers &= bit ? vote : ~vote;
+        }
         uint32_t cnt = 0;
-        if (valid) cnt = s_whist[warp][d];
+        if (valid) cnt = S.whist[warp][d];
         __syncwarp();
-        if (valid && lane == 31 - __clz(peers)) s_whist[warp][d] = cnt + __popc(peers);
+        if (valid && lane == 31 - __clz(peers)) S.whist[warp][d] = (uint16_t)(cnt + __popc(peers));
         __syncwarp();
         const uint32_t rk = cnt + __popc(peers & lt);
         if (i & 1) rank[i / 2] |= rk << 16; else rank[i / 2] = rk;
     }
     __syncthreads();
 
-    // Per digit (thread tid): warp-exclusive prefixes and the tile's count.
-    uint32_t tile_count = 0;
+    // Per digit (thread tid owns digits tid*P .. tid*P+P-1): warp-exclusive prefixes (in place)
+    // and the tile's counts.
+    uint32_t cnt[P];
 #pragma unroll
-    for (int w = 0; w < W; ++w) {
-        const uint32_t c = s_whist[w][tid];
-        s_whist[w][tid] = tile_count;
-        tile_count += c;
+    for (int j = 0; j < P; ++j) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const uint32_t x = S.whist[w][tid * P + j];
+            S.whist[w][tid * P + j] = (uint16_t)c;
+            c += x;
+        }
+        cnt[j] = c;
     }
 
-    // Decoupled look-back across tiles for digit tid: read kLookback predecessors at a time
-    // (independent loads), then add their counts newest first until a PREFIX is met.
-    uint32_t *lb = lookback + (size_t)tile * kDigits + tid;
-    uint32_t excl = 0;
-    if (tile == sp.first) {
-        st_relaxed_gpu(lb, kFlagPrefix | tile_count);
-    } else {
-        st_relaxed_gpu(lb, kFlagAgg | tile_count);
-        long long t0 = 0;
-        bool timed = false, done = false;
-        int64_t kk = (int64_t)tile - 1;  // next predecessor to add
-        while (!done) {
-            uint32_t w[kLookback];
+    // Publish the tile's counts at once (its inclusive prefix when it is the segment's first
+    // tile), so that later tiles can look back past it while it stages its keys.
+    uint32_t *lb = lookback + (size_t)tile * D + tid * P;
+    const bool first = tile == sp.first;
 #pragma unroll
-            for (int i = 0; i < kLookback; ++i)
-                w[i] = kk - i >= (int64_t)sp.first ? ld_relaxed_gpu(lookback + (size_t)(kk - i) * kDigits + tid) : kFlagPrefix;
+    for (int j = 0; j < P; ++j) st_relaxed_gpu(lb + j, (first ? kFlagPrefix : kFlagAgg) | cnt[j]);
+
+    // The tile's start of each digit in the staging buffer (exclusive scan of its counts).
+    uint32_t tst[P], tsum = 0;
+#pragma unroll
+    for (int j = 0; j < P; ++j) tsum += cnt[j];
+    uint32_t tstart = block_exclusive_scan(tsum, S.warp);
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        const int dg = tid * P + j;
+        tst[j] = tstart;
+#pragma unroll
+        for (int w = 0; w < W; ++w) S.whist[w][dg] = (uint16_t)(S.whist[w][dg] + tstart);
+        tstart += cnt[j];
+    }
+    __syncthreads();
+
+    // Stage keys and values in digit order.
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const uint32_t idx = wbase + i * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (k[i] >> shift) & (D - 1);
+            const uint32_t pos = S.whist[warp][d] + ((rank[i / 2] >> (16 * (i & 1))) & 0xFFFFu);
+            S.keys[pos] = k[i];
+            S.vals[pos] = vals_in ? __ldcs(vals_in + idx) : idx;
+        }
+    }
+
+    // Decoupled look-back across tiles, all P digits together: read kLookback predecessors
+    // per digit at a time (independent loads), add their counts newest first until a PREFIX.
+    uint32_t excl[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) excl[j] = 0;
+    if (!first) {
+        int kk[P];
+#pragma unroll
+        for (int j = 0; j < P; ++j) kk[j] = (int)tile - 1;  // next predecessor to add
+        uint32_t done = 0;
+        constexpr uint32_t kAll = (1u << P) - 1u;
+        long long t0 = 0;
+        bool timed = false;
+        while (done != kAll) {
+            uint32_t w[P][kLookback];
+#pragma unroll
+            for (int j = 0; j < P; ++j)
+#pragma unroll
+                for (int i = 0; i < kLookback; ++i)
+                    w[j][i] = (!(done >> j & 1u) && kk[j] - i >= (int)sp.first)
+                                  ? ld_relaxed_gpu(lookback + (size_t)(kk[j] - i) * D + tid * P + j)
+                                  : kFlagPrefix;
             bool stalled = false;
 #pragma unroll
-            for (int i = 0; i < kLookback; ++i) {
-                if (done || stalled) continue;
-                const uint32_t flag = w[i] & ~kCountMask;
-                if (flag == 0u) { stalled = true; continue; }
-                excl += w[i] & kCountMask;
-                --kk;
-                if (flag == kFlagPrefix) done = true;
+            for (int j = 0; j < P; ++j) {
+                bool stop = (done >> j & 1u) != 0;
+#pragma unroll
+                for (int i = 0; i < kLookback; ++i) {
+                    if (stop) continue;
+                    const uint32_t flag = w[j][i] & ~kCountMask;
+                    if (flag == 0u) { stop = true; stalled = true; continue; }
+                    excl[j] += w[j][i] & kCountMask;
+                    --kk[j];
+                    if (flag == kFlagPrefix) { stop = true; done |= 1u << j; }
+                }
+                if (kk[j] < (int)sp.first) done |= 1u << j;
             }
-            if (kk < (int64_t)sp.first) done = true;
-            if (done || !stalled) continue;
+            if (done == kAll || !stalled) continue;
             if (!timed) { t0 = clock64(); timed = true; }
             else if (clock64() - t0 > kSpinLimitCycles ||
                      (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT)) {
@@ -190,35 +262,30 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
             }
             __nanosleep(20);
         }
-        st_relaxed_gpu(lb, kFlagPrefix | ((excl + tile_count) & kCountMask));
+#pragma unroll
+        for (int j = 0; j < P; ++j) st_relaxed_gpu(lb + j, kFlagPrefix | ((excl[j] + cnt[j]) & kCountMask));
     }
 
-    const uint32_t start = block_exclusive_scan(tile_count, s_warp);
-    s_tile_start[tid] = start;
-    s_out[tid] = digit_base + excl - start;
-    __syncthreads();
-
-    // Stage keys and values in digit order.
+    // Global start of each digit: exclusive scan of the pass's counts.
+    uint32_t g[P], gsum = 0;
 #pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-        const uint32_t idx = wbase + i * 32 + lane;
-        if (idx < n) {
-            const uint32_t d = (k[i] >> shift) & (kDigits - 1);
-            const uint32_t pos = s_tile_start[d] + s_whist[warp][d] + ((rank[i / 2] >> (16 * (i & 1))) & 0xFFFFu);
-            s_keys[pos] = k[i];
-            s_vals[pos] = vals_in ? __ldcs(vals_in + idx) : idx;
-        }
+    for (int j = 0; j < P; ++j) { g[j] = __ldg(sp.hist + tid * P + j); gsum += g[j]; }
+    uint32_t gbase = block_exclusive_scan(gsum, S.warp);
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        S.out[tid * P + j] = gbase + excl[j] - tst[j];
+        gbase += g[j];
     }
     __syncthreads();
 
     const uint32_t tile_n = min((uint32_t)kSortTile, n - tile_base);
     bool oob = false;
     for (uint32_t j = tid; j < tile_n; j += T) {
-        const uint32_t key = s_keys[j];
-        const uint32_t o = s_out[(key >> shift) & (kDigits - 1)] + j;
+        const uint32_t key = S.keys[j];
+        const uint32_t o = S.out[(key >> shift) & (D - 1)] + j;
         if (o < n) {  // always true unless a look-back wait gave up
             keys_out[o] = key;
-            vals_out[o] = s_vals[j];
+            vals_out[o] = S.vals[j];
         } else {
             oob = true;
         }
@@ -226,15 +293,256 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
     if (oob) atomicOr(&ctl->err, ERR_LOOKBACK_TIMEOUT);
 }
 
+constexpr int kChunkTiles = 8;  // tiles per chunk of the reduce-then-scan pass
+
+inline uint32_t sort_chunks(uint32_t n) { return (sort_tiles(n) + kChunkTiles - 1) / kChunkTiles; }
+
+// Reduce: digit counts of every tile (tile_hist[tile][digit]) and of every chunk of kChunkTiles
+// tiles (chunk_sum[chunk][digit]).  One block per chunk; each thread owns P contiguous digits.
+template <int BITS>
+__global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ keys, uint32_t n, int pass,
+                                                 uint32_t *__restrict__ tile_hist,
+                                                 uint32_t *__restrict__ chunk_sum) {
+    constexpr int D = 1 << BITS, P = D / T;
+    __shared__ __align__(16) uint32_t h[D];
+    const int tid = threadIdx.x, shift = pass * BITS;
+    const uint32_t tiles = sort_tiles(n);
+    uint32_t acc[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) acc[j] = 0;
+    for (int tt = 0; tt < kChunkTiles; ++tt) {
+        const uint32_t tile = blockIdx.x * kChunkTiles + tt;
+        if (tile >= tiles) break;  // uniform across the block
+        for (int i = tid; i < D; i += T) h[i] = 0;
+        __syncthreads();
+        const uint32_t base = tile * (uint32_t)kSortTile;
+        uint32_t k[IPT];
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const uint32_t idx = base + i * T + tid;
+            k[i] = idx < n ? __ldcs(keys + idx) : 0xFFFFFFFFu;
+        }
+#pragma unroll
+        for (int i = 0; i < IPT; ++i)
+            if (base + i * T + tid < n) atomicAdd(&h[(k[i] >> shift) & (D - 1)], 1u);
+        __syncthreads();
+        uint32_t c[P];
+#pragma unroll
+        for (int j = 0; j < P; ++j) { c[j] = h[tid * P + j]; acc[j] += c[j]; }
+        uint32_t *row = tile_hist + (size_t)tile * D + tid * P;
+#pragma unroll
+        for (int j = 0; j < P; ++j) row[j] = c[j];
+        __syncthreads();
+    }
+    uint32_t *row = chunk_sum + (size_t)blockIdx.x * D + tid * P;
+#pragma unroll
+    for (int j = 0; j < P; ++j) row[j] = acc[j];
+}
+
+// Scan: chunk_off[c][d] = start of digit d in the pass's output (exclusive scan of the global
+// counts ghist over digits) + counts of digit d in chunks before c.  Block b covers digits
+// 32b .. 32b+31 (lane = digit); its 8 warps split the chunks.
+template <int BITS>
+__global__ void __launch_bounds__(T) k_chunk_scan(const uint32_t *__restrict__ chunk_sum, uint32_t chunks,
+                                                  const uint32_t *__restrict__ ghist,
+                                                  uint32_t *__restrict__ chunk_off) {
+    constexpr int D = 1 << BITS, P = D / T;
+    __shared__ uint32_t s_warp[W];
+    __shared__ uint32_t s_base[32];
+    __shared__ uint32_t s_part[W][32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // digit starts: exclusive scan of the global counts (thread tid holds digits tid*P..)
+    uint32_t g[P], gs = 0;
+#pragma unroll
+    for (int j = 0; j < P; ++j) { g[j] = __ldg(ghist + tid * P + j); gs += g[j]; }
+    uint32_t run = block_exclusive_scan(gs, s_warp);
+    const int d0 = blockIdx.x * 32;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        const int dg = tid * P + j;
+        if (dg >= d0 && dg < d0 + 32) s_base[dg - d0] = run;
+        run += g[j];
+    }
+    const uint32_t per = (chunks + W - 1) / W;
+    const uint32_t c0 = warp * per, c1 = min(chunks, c0 + per);
+    const int d = d0 + lane;
+    uint32_t sum = 0;
+    for (uint32_t c = c0; c < c1; ++c) sum += __ldg(chunk_sum + (size_t)c * D + d);
+    s_part[warp][lane] = sum;
+    __syncthreads();
+    uint32_t off = s_base[lane];
+    for (int w = 0; w < warp; ++w) off += s_part[w][lane];
+    for (uint32_t c = c0; c < c1; ++c) {
+        chunk_off[(size_t)c * D + d] = off;
+        off += __ldg(chunk_sum + (size_t)c * D + d);
+    }
+}
+
+// Scatter: the ranking and staging of k_onesweep; the prefix of each digit is the chunk's
+// offset plus the counts of the chunk's earlier tiles.  Tile = blockIdx.x, no waits.
+template <int BITS>
+__global__ void __launch_bounds__(T, 4) k_scatter(const uint32_t *__restrict__ keys_in,
+                                               const uint32_t *__restrict__ vals_in,
+                                               uint32_t *__restrict__ keys_out,
+                                               uint32_t *__restrict__ vals_out, uint32_t n,
+                                               int pass, const uint32_t *__restrict__ tile_hist,
+                                               const uint32_t *__restrict__ chunk_off,
+                                               Control *__restrict__ ctl) {
+    constexpr int D = 1 << BITS;
+    constexpr int P = D / T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SortSmem<BITS> &S = *reinterpret_cast<SortSmem<BITS> *>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < W * D / 2; i += T) reinterpret_cast<uint32_t *>(&S.whist[0][0])[i] = 0;
+    const uint32_t tile = blockIdx.x, tile_base = tile * (uint32_t)kSortTile;
+    const int shift = pass * BITS;
+    const uint32_t wbase = tile_base + warp * (IPT * 32);
+
+    uint32_t k[IPT];
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const uint32_t idx = wbase + i * 32 + lane;
+        k[i] = idx < n ? __ldcs(keys_in + idx) : 0u;
+    }
+    // the digit prefixes of this tile (final values: independent loads, in flight with the
+    // keys), parked in S.out until the tile's own starts are known
+    {
+        const uint32_t chunk = tile / kChunkTiles;
+        uint32_t pre[P];
+#pragma unroll
+        for (int j = 0; j < P; ++j) pre[j] = __ldg(chunk_off + (size_t)chunk * D + tid * P + j);
+        for (uint32_t t = chunk * kChunkTiles; t < tile; ++t) {
+#pragma unroll
+            for (int j = 0; j < P; ++j) pre[j] += __ldg(tile_hist + (size_t)t * D + tid * P + j);
+        }
+#pragma unroll
+        for (int j = 0; j < P; ++j) S.out[tid * P + j] = pre[j];
+    }
+    __syncthreads();
+
+    uint32_t rank[IPT / 2];
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const uint32_t idx = wbase + i * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t d = (k[i] >> shift) & (D - 1);
+        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+        for (int b = 0; b < BITS; ++b) {
+            const uint32_t bit = (d >> b) & 1u;
+            const uint32_t vote = __ballot_sync(0xFFFFFFFFu, bit);
+            peers &= bit ? vote : ~vote;
+        }
+        uint32_t cnt = 0;
+        if (valid) cnt = S.whist[warp][d];
+        __syncwarp();
+        if (valid && lane == 31 - __clz(peers)) S.whist[warp][d] = (uint16_t)(cnt + __popc(peers));
+        __syncwarp();
+        const uint32_t rk = cnt + __popc(peers & lt);
+        if (i & 1) rank[i / 2] |= rk << 16; else rank[i / 2] = rk;
+    }
+    __syncthreads();
+
+    uint32_t cnt[P], tsum = 0;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const uint32_t x = S.whist[w][tid * P + j];
+            S.whist[w][tid * P + j] = (uint16_t)c;
+            c += x;
+        }
+        cnt[j] = c;
+        tsum += c;
+    }
+    uint32_t tstart = block_exclusive_scan(tsum, S.warp);
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        const int dg = tid * P + j;
+#pragma unroll
+        for (int w = 0; w < W; ++w) S.whist[w][dg] = (uint16_t)(S.whist[w][dg] + tstart);
+        S.out[dg] -= tstart;
+        tstart += cnt[j];
+    }
+    __syncthreads();
+
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const uint32_t idx = wbase + i * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (k[i] >> shift) & (D - 1);
+            const uint32_t pos = S.whist[warp][d] + ((rank[i / 2] >> (16 * (i & 1))) & 0xFFFFu);
+            S.keys[pos] = k[i];
+            S.vals[pos] = vals_in ? __ldcs(vals_in + idx) : idx;
+        }
+    }
+    __syncthreads();
+
+    const uint32_t tile_n = min((uint32_t)kSortTile, n - tile_base);
+    bool oob = false;
+    for (uint32_t j = tid; j < tile_n; j += T) {
+        const uint32_t key = S.keys[j];
+        const uint32_t o = S.out[(key >> shift) & (D - 1)] + j;
+        if (o < n) {  // always true for consistent counts
+            keys_out[o] = key;
+            vals_out[o] = S.vals[j];
+        } else {
+            oob = true;
+        }
+    }
+    if (oob) atomicOr(&ctl->err, ERR_CLIMB);
+}
+
+template <int BITS, class Segs>
+void launch(Segs segs, uint32_t tiles, const uint32_t *keys_in, const uint32_t *vals_in,
+            uint32_t *keys_out, uint32_t *vals_out, int pass, Control *ctl, uint32_t *lookback,
+            cudaStream_t s) {
+    k_onesweep<BITS, Segs><<<tiles, T, sizeof(SortSmem<BITS>), s>>>(
+        segs, keys_in, vals_in, keys_out, vals_out, pass, ctl, lookback);
+}
+
+template <int BITS, class Segs>
+cudaError_t allow_smem() {
+    return cudaFuncSetAttribute(k_onesweep<BITS, Segs>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(SortSmem<BITS>));
+}
+
 }  // namespace
 
-void launch_onesweep(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
-                     uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *lookback,
-                     cudaStream_t s) {
+cudaError_t sort_init() {
+    cudaError_t e = allow_smem<kDigitBits, ManySegSort>();
+    if (e == cudaSuccess) e = allow_smem<kDigitBits32, OneSegSort>();
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_scatter<kDigitBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(SortSmem<kDigitBits>));
+    return e;
+}
+
+size_t sort_scratch_words(uint32_t n) { return ((size_t)sort_tiles(n) + 2ull * sort_chunks(n)) * kDigits; }
+
+void launch_sort_pass(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
+                      uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *scratch,
+                      cudaStream_t s) {
+    if (n == 0) return;
+    const uint32_t tiles = sort_tiles(n), chunks = sort_chunks(n);
+    uint32_t *tile_hist = scratch;
+    uint32_t *chunk_sum = tile_hist + (size_t)tiles * kDigits;
+    uint32_t *chunk_off = chunk_sum + (size_t)chunks * kDigits;
+    k_tile_hist<kDigitBits><<<chunks, T, 0, s>>>(keys_in, n, pass, tile_hist, chunk_sum);
+    k_chunk_scan<kDigitBits><<<kDigits / 32, T, 0, s>>>(chunk_sum, chunks, ctl->hist + pass * kDigits, chunk_off);
+    k_scatter<kDigitBits><<<tiles, T, sizeof(SortSmem<kDigitBits>), s>>>(
+        keys_in, vals_in, keys_out, vals_out, n, pass, tile_hist, chunk_off, ctl);
+}
+
+void launch_onesweep32(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
+                       uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *lookback,
+                       cudaStream_t s) {
     if (n == 0) return;
     const uint32_t tiles = sort_tiles(n);
-    k_onesweep<<<tiles, T, 0, s>>>(OneSegSort{n, &ctl->hist[pass][0]}, keys_in, vals_in, keys_out,
-                                   vals_out, pass, ctl, lookback + (size_t)pass * tiles * kDigits);
+    launch<kDigitBits32>(OneSegSort{n, ctl->hist + pass * kDigits32}, tiles, keys_in, vals_in,
+                         keys_out, vals_out, pass, ctl, lookback + (size_t)pass * tiles * kDigits32, s);
 }
 
 void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const uint32_t *vals_in,
@@ -242,9 +550,8 @@ void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const u
                            const uint32_t *seg_hist, Control *ctl, uint32_t *lookback,
                            cudaStream_t s) {
     if (bp.tiles == 0) return;
-    k_onesweep<<<bp.tiles, T, 0, s>>>(ManySegSort{bp.rows, bp.tile_seg, seg_hist, pass}, keys_in,
-                                      vals_in, keys_out, vals_out, pass, ctl,
-                                      lookback + (size_t)pass * bp.tiles * kDigits);
+    launch<kDigitBits>(ManySegSort{bp.rows, bp.tile_seg, seg_hist, pass}, bp.tiles, keys_in, vals_in,
+                       keys_out, vals_out, pass, ctl, lookback + (size_t)pass * bp.tiles * kDigits, s);
 }
 
 }  // namespace lvbh
