@@ -9,29 +9,31 @@
 // Tree.  With d[k] = delta(k, k+1) (common-prefix length of adjacent sorted keys, index
 // tie-break, -1 past either end), the Karras radix tree is the Cartesian tree of d: the node
 // whose split is s covers [L, R], where L-1 and R are the nearest positions left and right of
-// s with a smaller d.  That node is the LEFT child of split R when d[R] > d[L-1], else the
-// RIGHT child of split L-1 (the two values always differ), so its Karras index is R or L (0
-// for the root) - exactly the numbering compute_child_index produces.  Its children are the
-// nodes with Karras indices s and s+1 (leaves s, s+1 when L == s, R == s+1).  So every node's
-// record follows from nearest-smaller-value queries on d alone: no per-node binary search,
-// no climbing, no atomics.
+// s with a smaller d.  A node [L, R] is the LEFT child of split R when d[R] > d[L-1], else the
+// RIGHT child of split L-1 (adjacent d values always differ), so its Karras index is R or L
+// (0 for the root) - exactly the numbering compute_child_index produces - and its parent
+// follows from its own range alone.  The tree is therefore built bottom-up with the boxes:
+// every leaf climbs; at each split the first child to arrive parks, the second merges both
+// into the parent's record and climbs on.  No per-node binary search, N-1 box unions.
 //
 // Passes.
 //   K3a (k_leaf_gather)  one thread per sorted leaf k: gathers triangle perm[k] (3 x 16-byte
 //                        loads), writes it to the output soup at k, and writes its box (exact-
 //                        zero components nudged by 1e-8 as bvh-up-pass.js:209-210 does) to a
 //                        24-byte scratch record.  Random-access bound.
-//   K3b (k_tree_leaves)  blocks of 256 sorted leaves, one thread per leaf / split, a persistent
-//                        grid that prefetches the next block.  Two sparse tables in shared
-//                        memory - minima of d, unions of leaf boxes - give every split its
-//                        nearest smaller separators by binary lifting and its children's boxes
-//                        by two O(1) range queries, so every node whose range stays inside the
-//                        block is completed at once (record and parent links staged in shared
-//                        memory and written coalesced).  A node or leaf whose parent split is
-//                        not inside the block leaves it as an "open item" (at most 2 x 64 per
-//                        block: they hang off the two boundary paths of a tree at most 64 deep).
+//   K3b (k_tree_climb)   blocks of 256 sorted leaves in shared memory, a persistent grid that
+//                        prefetches the next block.  The climb runs in steps: the items still
+//                        climbing after a step are compacted into a queue, so warps stay full
+//                        while the number of items shrinks.  Parking and merging use an
+//                        arrival mask per split (shared-memory atomics) and parked items in
+//                        shared memory; records go straight to the node buffer, parent links
+//                        are staged and written coalesced.  An item whose parent split lies
+//                        outside the block, or whose sibling never arrives (the parent
+//                        straddles the block boundary), leaves as an "open item" (at most
+//                        2 x 64 per block: they hang off the two boundary paths of a tree at
+//                        most 64 deep).
 //   K3c (k_emit_top)     the nodes that straddle blocks (~3 % of them), built bottom-up from
-//                        the open items with arrival words (see below).
+//                        the open items with arrival words in global memory (see below).
 #include "lvbh_device.cuh"
 #include "lvbh_internal.h"
 
@@ -48,30 +50,6 @@ __device__ __forceinline__ int dd_global(const uint32_t *__restrict__ keys, int 
     if (x < 0 || x >= n - 1) return -1;
     const uint32_t a = __ldg(keys + x), b = __ldg(keys + x + 1);
     return a != b ? __clz(a ^ b) : 32 + __clz(x ^ (x + 1));
-}
-
-// Block-wide exclusive sum of one value per thread; returns the thread's offset, *total the sum.
-template <int kThreads>
-__device__ __forceinline__ int block_excl_sum(int v, int *s_warp, int *total) {
-    constexpr int W = kThreads / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    int off = 0, all = 0;
-#pragma unroll
-    for (int i = 0; i < W; ++i) {
-        off += i < warp ? s_warp[i] : 0;
-        all += s_warp[i];
-    }
-    __syncthreads();
-    *total = all;
-    return off + incl - v;
 }
 
 // Where a block of EB sorted leaves lives.  A batched build is a list of segments (meshes)
@@ -130,52 +108,37 @@ __global__ void __launch_bounds__(256) k_leaf_gather(Segs segs, const float4 *__
     lbox[3ull * k + 2] = make_float2(xy, xz);
 }
 
-// K3b shared memory: sparse tables over one block of EB leaves.
-//   md[l][x] = min of S[x .. x + 2^l - 1] (S[x] = d[b0 + x - 1], x in [0, EB])
-//   bx[l][c][x] = component c (min xyz, max xyz) of the union of leaf boxes x .. x + 2^l - 1
-// The records of the block are staged over bx once the range queries are done.
-struct LeafTables {
-    int8_t md[kLogEB + 1][EB + 4];
-    union {
-        float bx[kLogEB + 1][6][EB];
-        float4 rec[EB][4];  // records of the nodes completed here, by index - b0
-    };
-    int pint[EB];        // parent of internal node b0 + j (-1 = not set here)
-    int pleaf[EB];       // parent of leaf b0 + j (-1 = not set here)
-    uint32_t key[EB + 2];
-    uint8_t recv[EB];
-    uint8_t local[EB];   // split b0 + j stays inside the block
-    uint8_t open[EB];    // an open item starts at leaf b0 + j
-    int16_t pos[EB];     // its position among the block's open items
-    int warp[EB / 32];
+// K3b shared memory.  A climbing item is two float4: box min + link (node index, or
+// -(leaf + 1)), box max + its packed local range and end separators
+// (l | r << 8 | (d[l-1] + 1) << 16 | (d[r] + 1) << 24).
+struct ClimbSmem {
+    float4 pend[EB][2][2];  // [split][side][min/max] the child parked at each split
+    float4 q[2][EB][2];     // the items of the current and the next step
+    uint32_t key[EB + 2];   // keys of leaves b0-1 .. b0+EB
+    uint32_t mask[EB];      // arrivals at each split: bit 0 left child, bit 1 right child
+    int pint[EB];           // parent of internal node b0 + j (-1 = not set here)
+    int pleaf[EB];          // parent of leaf b0 + j (-1 = not set here)
+    int cnt[3];             // item counters, rotating over the steps
+    int open;               // open items emitted
 };
 
-// Union of leaf boxes [a, b] (0 <= a <= b < EB) from the box table.
-__device__ __forceinline__ void range_box(const LeafTables &T, int a, int b, float4 &lo, float4 &hi) {
-    const int l = 31 - __clz(b - a + 1);
-    const int c = b - (1 << l) + 1;
-    lo = make_float4(fminf(T.bx[l][0][a], T.bx[l][0][c]), fminf(T.bx[l][1][a], T.bx[l][1][c]),
-                     fminf(T.bx[l][2][a], T.bx[l][2][c]), 0.f);
-    hi = make_float4(fmaxf(T.bx[l][3][a], T.bx[l][3][c]), fmaxf(T.bx[l][4][a], T.bx[l][4][c]),
-                     fmaxf(T.bx[l][5][a], T.bx[l][5][c]), 0.f);
+__device__ __forceinline__ uint32_t pack_range(int l, int r, int dl, int dr) {
+    return (uint32_t)l | ((uint32_t)r << 8) | ((uint32_t)(dl + 1) << 16) | ((uint32_t)(dr + 1) << 24);
 }
 
-// K3b: the tree over blocks of EB sorted leaves; a persistent grid walks the blocks and
-// fetches the next block's keys and leaf boxes while it works on the current one.  Every
-// split whose node stays inside the block finds its node range by binary lifting on the d
-// table (nearest smaller separators on both sides), its Karras index and children from that
-// range, and its children's boxes by two range queries on the box table: all nodes of a block
-// complete at once.  The nodes that straddle blocks are left to K3c as open items.
+// K3b: the tree over blocks of EB sorted leaves (see the pass list above).
 template <class Segs>
-__global__ void __launch_bounds__(EB) k_tree_leaves(Segs segs, const uint32_t *__restrict__ keys_all,
+__global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
+                                                    const uint32_t *__restrict__ keys_all,
                                                     const float2 *__restrict__ lbox_all,
                                                     float4 *nodes_all, int32_t *parents_all,
                                                     OpenItem *out_items, uint32_t *out_counts,
                                                     Control *ctl) {
     extern __shared__ __align__(16) unsigned char smem[];
-    LeafTables &T = *reinterpret_cast<LeafTables *>(smem);
-    const int t = threadIdx.x;
+    ClimbSmem &S = *reinterpret_cast<ClimbSmem *>(smem);
+    const int t = threadIdx.x, lane = t & 31;
     const int nblk = segs.blocks();
+    const uint32_t lt = lanemask_lt();
 
     // registers of the next block: its span, this thread's key and leaf box, the two edge keys
     Span nsp{0, 0, 0};
@@ -203,29 +166,28 @@ __global__ void __launch_bounds__(EB) k_tree_leaves(Segs segs, const uint32_t *_
         const int m = min(EB, n - b0);
         const int k = b0 + t;
         const bool active = t < m;
-        T.key[t + 1] = active ? nk : 0u;
-        if (t == 0) T.key[0] = nk_lo;
-        if (t == EB - 1) T.key[EB + 1] = nk_hi;
-        const float box[6] = {np0.x, np0.y, np1.x, np1.y, np2.x, np2.y};
-#pragma unroll
-        for (int c = 0; c < 6; ++c) T.bx[0][c][t] = active ? box[c] : 0.f;
-        T.pint[t] = -1;
-        T.pleaf[t] = -1;
-        T.recv[t] = 0;
-        T.open[t] = 0;
-        T.local[t] = 0;
+        S.key[t + 1] = active ? nk : 0u;
+        if (t == 0) S.key[0] = nk_lo;
+        if (t == EB - 1) S.key[EB + 1] = nk_hi;
+        S.mask[t] = 0;
+        S.pint[t] = -1;
+        S.pleaf[t] = -1;
+        if (t < 3) S.cnt[t] = 0;
+        if (t == 0) S.open = 0;
+        const float4 leaf_lo = make_float4(np0.x, np0.y, np1.x, __int_as_float(-(k + 1)));
+        const float4 leaf_hi0 = make_float4(np1.y, np2.x, np2.y, 0.f);
         if (blk + (int)gridDim.x < nblk) fetch(blk + gridDim.x);
         if (n == 1) {  // one leaf, one arrival at node 0: left slot only, f_1 = 1
             if (t == 0) {
-                nodes[0] = make_float4(box[0], box[1], box[2], __int_as_float(-1));
-                nodes[1] = make_float4(box[3], box[4], box[5], __int_as_float(1));
+                nodes[0] = make_float4(leaf_lo.x, leaf_lo.y, leaf_lo.z, __int_as_float(-1));
+                nodes[1] = make_float4(leaf_hi0.x, leaf_hi0.y, leaf_hi0.z, __int_as_float(1));
                 nodes[2] = make_float4(0.f, 0.f, 0.f, 0.f);
                 nodes[3] = make_float4(0.f, 0.f, 0.f, 0.f);
                 parents[0] = 0;
                 parents[1] = 0;
                 out_counts[blk] = 0;
             }
-            continue;  // uniform across the block; the tables are untouched by other threads
+            continue;  // uniform across the block; no other thread reads what this one wrote
         }
         if (k == 0) {  // the root has no parent; slot N-1 and record N-1 stay zero
             parents[0] = 0;
@@ -235,122 +197,118 @@ __global__ void __launch_bounds__(EB) k_tree_leaves(Segs segs, const uint32_t *_
             last[0] = z; last[1] = z; last[2] = z; last[3] = z;
         }
         __syncthreads();
-        auto window_d = [&](int x) -> int {  // x in [b0-1, b0+EB-1]
-            if (x < 0 || x >= n - 1) return -1;
-            const uint32_t a = T.key[x - b0 + 1], b = T.key[x - b0 + 2];
-            return a != b ? __clz(a ^ b) : 32 + __clz(x ^ (x + 1));
+        auto dval = [&](int x) -> int {  // d of split b0 + x, x in [-1, EB - 1]
+            const int g = b0 + x;
+            if (g < 0 || g >= n - 1) return -1;
+            const uint32_t a = S.key[x + 1], b = S.key[x + 2];
+            return a != b ? __clz(a ^ b) : 32 + __clz(g ^ (g + 1));
         };
-        T.md[0][t] = (int8_t)window_d(b0 - 1 + t);
-        if (t == 0) T.md[0][EB] = (int8_t)window_d(b0 + EB - 1);
-        __syncthreads();
-        // sparse tables
-#pragma unroll 1
-        for (int l = 1; l <= kLogEB; ++l) {
-            const int h = 1 << (l - 1);
-            if (t + (1 << l) - 1 <= EB) T.md[l][t] = min(T.md[l - 1][t], T.md[l - 1][t + h]);
-            if (t + (1 << l) - 1 < m) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) T.bx[l][c][t] = fminf(T.bx[l - 1][c][t], T.bx[l - 1][c][t + h]);
-#pragma unroll
-                for (int c = 3; c < 6; ++c) T.bx[l][c][t] = fmaxf(T.bx[l - 1][c][t], T.bx[l - 1][c][t + h]);
-            }
-            __syncthreads();
-        }
-
-        // split j = t (between leaves b0 + j and b0 + j + 1), its separator S[q], q = j + 1
-        const int j = t, q = t + 1;
-        int il = -1, ir = -1;
-        if (j < m - 1) {
-            const int v = T.md[0][q];
-            int pos = q;
-#pragma unroll
-            for (int l = kLogEB; l >= 0; --l)
-                if (pos - (1 << l) >= 0 && T.md[l][pos - (1 << l)] >= v) pos -= 1 << l;
-            const int a = pos - 1;  // nearest smaller on the left, or -1
-            pos = q;
-#pragma unroll
-            for (int l = kLogEB; l >= 0; --l)
-                if (pos + (1 << l) <= m && T.md[l][pos + 1] >= v) pos += 1 << l;
-            const int b = pos + 1;  // nearest smaller on the right, or past the window
-            if (a >= 0 && b <= m) {
-                il = a;
-                ir = b - 1;
-                T.local[j] = 1;
-            }
-        }
-        __syncthreads();
-
-        auto S = [&](int x) -> int { return T.md[0][x]; };
-        auto split_local = [&](int ps) -> bool { return ps >= 0 && ps < m - 1 && T.local[ps]; };
-        int P = 0;
-        bool node_open = false;
-        float4 w0, w1, w2, w3;
-        if (il >= 0) {
-            const bool root = (b0 + il == 0) && (b0 + ir == n - 1);
-            const bool left_child = S(ir + 1) > S(il);
-            P = root ? 0 : (left_child ? b0 + ir : b0 + il);
-            const int lref = (il == j) ? -(b0 + j + 1) : b0 + j;
-            const int rref = (ir == j + 1) ? -(b0 + j + 2) : b0 + j + 1;
-            float4 l0, l1, r0, r1;
-            range_box(T, il, j, l0, l1);
-            range_box(T, j + 1, ir, r0, r1);
-            w0 = make_float4(l0.x, l0.y, l0.z, __int_as_float(lref));
-            w1 = make_float4(l1.x, l1.y, l1.z, __int_as_float(2));
-            w2 = make_float4(r0.x, r0.y, r0.z, __int_as_float(rref));
-            w3 = make_float4(r1.x, r1.y, r1.z, __int_as_float(0));
-            T.recv[P - b0] = 1;
-            if (lref >= 0) T.pint[lref - b0] = P; else T.pleaf[-(lref + 1) - b0] = P;
-            if (rref >= 0) T.pint[rref - b0] = P; else T.pleaf[-(rref + 1) - b0] = P;
-            node_open = !root && !split_local(left_child ? ir : il - 1);
-            if (node_open) T.open[il] = 1;
-        }
-        bool leaf_open = false;
-        if (active) {  // a leaf whose parent split is not local leaves the block as it is
-            const int ps = S(t + 1) > S(t) ? t : t - 1;
-            leaf_open = !split_local(ps);
-            if (leaf_open) T.open[t] = 1;
-        }
-        __syncthreads();
-
-        // open items in leaf order: the item starting at leaf t takes position pos[t]
-        int total;
-        const int f = T.open[t];
-        T.pos[t] = (int16_t)block_excl_sum<EB>(f, T.warp, &total);
-        __syncthreads();
         OpenItem *out = out_items + (size_t)blk * kOpenCap;
-        auto emit_open = [&](int a, int b, int ref) {
-            const int at = T.pos[a];
-            if (at >= kOpenCap) { atomicOr(&ctl->err, ERR_CLIMB); return; }
-            float4 lo, hi;
-            range_box(T, a, b, lo, hi);
+        auto emit = [&](float4 lo, float4 hi) {  // an item leaves the block for K3c
+            const uint32_t pk = __float_as_uint(hi.w);
             OpenItem it;
-            it.lo = make_float4(lo.x, lo.y, lo.z, __int_as_float(ref));
-            it.hi = make_float4(hi.x, hi.y, hi.z, __int_as_float(S(b + 1)));
-            it.xl = b0 + a;
-            it.xr = b0 + b;
+            it.lo = lo;
+            it.hi = make_float4(hi.x, hi.y, hi.z, __int_as_float((int)(pk >> 24) - 1));
+            it.xl = b0 + (int)(pk & 255u);
+            it.xr = b0 + (int)((pk >> 8) & 255u);
             it.pad0 = it.pad1 = 0;
-            out[at] = it;
+            const int at = atomicAdd(&S.open, 1);
+            if (at < kOpenCap) out[at] = it;
+            else atomicOr(&ctl->err, ERR_CLIMB);
         };
-        if (leaf_open) emit_open(t, t, -(k + 1));
-        if (node_open) emit_open(il, ir, P);
-        if (t == 0) out_counts[blk] = (uint32_t)min(total, kOpenCap);
-        if (t == 0 && total > kOpenCap) atomicOr(&ctl->err, ERR_CLIMB);
-        __syncthreads();  // the box table is done with: stage the records over it
-        if (il >= 0) {
-            float4 *rc = T.rec[P - b0];
-            rc[0] = w0; rc[1] = w1; rc[2] = w2; rc[3] = w3;
+        // One step of an item: leave the block, park at its parent split, or merge with the
+        // parked sibling into the parent (returned in nlo/nhi, true unless it is the root).
+        auto climb = [&](float4 lo, float4 hi, float4 &nlo, float4 &nhi) -> bool {
+            const uint32_t pk = __float_as_uint(hi.w);
+            const int l = (int)(pk & 255u), r = (int)((pk >> 8) & 255u);
+            const int dl = (int)((pk >> 16) & 255u) - 1, dr = (int)(pk >> 24) - 1;
+            const bool is_left = dr > dl;
+            const int s = is_left ? r : l - 1;
+            if (s < 0 || s > m - 2) {
+                emit(lo, hi);
+                return false;
+            }
+            const int side = is_left ? 0 : 1;
+            S.pend[s][side][0] = lo;
+            S.pend[s][side][1] = hi;
+            __threadfence_block();
+            if (atomicOr(&S.mask[s], 1u << side) == 0u) return false;  // first arrival parks
+            __threadfence_block();
+            const float4 slo = S.pend[s][side ^ 1][0], shi = S.pend[s][side ^ 1][1];
+            const float4 Llo = is_left ? lo : slo, Lhi = is_left ? hi : shi;
+            const float4 Rlo = is_left ? slo : lo, Rhi = is_left ? shi : hi;
+            const uint32_t lpk = __float_as_uint(Lhi.w), rpk = __float_as_uint(Rhi.w);
+            const int L = (int)(lpk & 255u), R = (int)((rpk >> 8) & 255u);
+            const int ndl = (int)((lpk >> 16) & 255u) - 1, ndr = (int)(rpk >> 24) - 1;
+            const bool root = (b0 + L == 0) && (b0 + R == n - 1);
+            const int P = root ? 0 : (ndr > ndl ? b0 + R : b0 + L);
+            float4 *rc = nodes + 4ull * P;
+            rc[0] = Llo;
+            rc[1] = make_float4(Lhi.x, Lhi.y, Lhi.z, __int_as_float(2));
+            rc[2] = Rlo;
+            rc[3] = make_float4(Rhi.x, Rhi.y, Rhi.z, __int_as_float(0));
+            const int lref = __float_as_int(Llo.w), rref = __float_as_int(Rlo.w);
+            if (lref >= 0) S.pint[lref - b0] = P; else S.pleaf[-(lref + 1) - b0] = P;
+            if (rref >= 0) S.pint[rref - b0] = P; else S.pleaf[-(rref + 1) - b0] = P;
+            if (root) return false;
+            nlo = make_float4(fminf(Llo.x, Rlo.x), fminf(Llo.y, Rlo.y), fminf(Llo.z, Rlo.z), __int_as_float(P));
+            nhi = make_float4(fmaxf(Lhi.x, Rhi.x), fmaxf(Lhi.y, Rhi.y), fmaxf(Lhi.z, Rhi.z),
+                              __uint_as_float(pack_range(L, R, ndl, ndr)));
+            return true;
+        };
+        // the items that climb on go to queue oq, counted in S.cnt[oc] (warp-aggregated)
+        auto append = [&](bool cont, float4 nlo, float4 nhi, int oq, int oc) {
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, cont);
+            int base = 0;
+            if (lane == 0 && bal) base = atomicAdd(&S.cnt[oc], __popc(bal));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (cont) {
+                const int at = base + __popc(bal & lt);
+                S.q[oq][at][0] = nlo;
+                S.q[oq][at][1] = nhi;
+            }
+        };
+
+        // step 0: the leaves
+        float4 nlo = make_float4(0.f, 0.f, 0.f, 0.f), nhi = nlo;
+        bool cont = false;
+        if (active)
+            cont = climb(leaf_lo, make_float4(leaf_hi0.x, leaf_hi0.y, leaf_hi0.z,
+                                              __uint_as_float(pack_range(t, t, dval(t - 1), dval(t)))),
+                         nlo, nhi);
+        append(cont, nlo, nhi, 0, 0);
+        // later steps: the merged parents, compacted
+        int cur = 0, c = 0;
+        for (int guard = 0; guard < 2 * EB; ++guard) {
+            __syncthreads();
+            const int count = S.cnt[c];
+            if (count == 0) break;
+            const int nc = c == 2 ? 0 : c + 1, rc = nc == 2 ? 0 : nc + 1;
+            cont = false;
+            if (t < count) cont = climb(S.q[cur][t][0], S.q[cur][t][1], nlo, nhi);
+            append(cont, nlo, nhi, cur ^ 1, nc);
+            if (t == 0) S.cnt[rc] = 0;
+            cur ^= 1;
+            c = nc;
+        }
+        // a child parked at a split whose sibling never came: the parent straddles the block
+        if (t < m - 1) {
+            const uint32_t mk = S.mask[t];
+            if (mk == 1u || mk == 2u) {
+                const int side = mk == 1u ? 0 : 1;
+                emit(S.pend[t][side][0], S.pend[t][side][1]);
+            }
         }
         __syncthreads();
-        // records and parent links, coalesced
         if (active) {
-            if (T.recv[t]) {
-                float4 *dst = nodes + 4ull * k;
-                dst[0] = T.rec[t][0]; dst[1] = T.rec[t][1]; dst[2] = T.rec[t][2]; dst[3] = T.rec[t][3];
-            }
-            if (T.pint[t] >= 0) parents[k] = T.pint[t];
-            if (T.pleaf[t] >= 0) parents[n + k] = T.pleaf[t];
+            if (S.pint[t] >= 0) parents[k] = S.pint[t];
+            if (S.pleaf[t] >= 0) parents[n + k] = S.pleaf[t];
         }
-        __syncthreads();  // before the next block overwrites the tables
+        if (t == 0) {
+            out_counts[blk] = (uint32_t)min(S.open, kOpenCap);
+            if (S.open > kOpenCap) atomicOr(&ctl->err, ERR_CLIMB);
+        }
+        __syncthreads();  // before the next block overwrites shared memory
     }
 }
 
@@ -426,7 +384,7 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
     }
 }
 
-inline size_t leaves_smem_bytes() { return sizeof(LeafTables); }
+inline size_t leaves_smem_bytes() { return sizeof(ClimbSmem); }
 
 template <class Segs>
 void launch_emit_impl(Segs segs, int groups, const float4 *tri, const uint32_t *perm,
@@ -437,7 +395,7 @@ void launch_emit_impl(Segs segs, int groups, const float4 *tri, const uint32_t *
     k_leaf_gather<<<groups, 256, 0, s>>>(segs, tri, perm, otri, lbox, ctl);
     if (ev) cudaEventRecord(ev[0], s);
     const int grid = min(groups, sm_count() * kTreeCtasPerSm);
-    k_tree_leaves<<<grid, EB, leaves_smem_bytes(), s>>>(segs, keys, lbox, nodes, parents, items,
+    k_tree_climb<<<grid, EB, leaves_smem_bytes(), s>>>(segs, keys, lbox, nodes, parents, items,
                                                          counts, ctl);
     if (ev) cudaEventRecord(ev[1], s);
     if (top)
@@ -461,9 +419,9 @@ cudaError_t prefer_shared(K kernel) {
 size_t emit_groups(uint32_t n) { return (n + EB - 1) / EB; }
 
 cudaError_t emit_init() {
-    cudaError_t e = prefer_shared(k_tree_leaves<OneSeg>);
+    cudaError_t e = prefer_shared(k_tree_climb<OneSeg>);
     if (e != cudaSuccess) return e;
-    return prefer_shared(k_tree_leaves<ManySegs>);
+    return prefer_shared(k_tree_climb<ManySegs>);
 }
 
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
