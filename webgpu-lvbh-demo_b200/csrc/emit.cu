@@ -45,6 +45,7 @@ constexpr int EB = kEmitBlock;                 // level 1: leaves (threads) per 
 constexpr int kLogEB = 8;                      // EB == 1 << kLogEB
 constexpr int kTreeCtasPerSm = 3;             // resident K3b CTAs per SM (persistent grid)
 constexpr int kTopLanes = 8;                   // K3c threads per block of K3b
+constexpr int kFreeClimb = 64;                 // K3b items left when compaction stops
 
 __device__ __forceinline__ int dd_global(const uint32_t *__restrict__ keys, int n, int x) {
     if (x < 0 || x >= n - 1) return -1;
@@ -231,9 +232,9 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             const int side = is_left ? 0 : 1;
             S.pend[s][side][0] = lo;
             S.pend[s][side][1] = hi;
-            __threadfence_block();
+            fence_acq_rel_cta();
             if (atomicOr(&S.mask[s], 1u << side) == 0u) return false;  // first arrival parks
-            __threadfence_block();
+            fence_acq_rel_cta();
             const float4 slo = S.pend[s][side ^ 1][0], shi = S.pend[s][side ^ 1][1];
             const float4 Llo = is_left ? lo : slo, Lhi = is_left ? hi : shi;
             const float4 Rlo = is_left ? slo : lo, Rhi = is_left ? shi : hi;
@@ -277,12 +278,24 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
                                               __uint_as_float(pack_range(t, t, dval(t - 1), dval(t)))),
                          nlo, nhi);
         append(cont, nlo, nhi, 0, 0);
-        // later steps: the merged parents, compacted
+        // later steps: the merged parents, compacted.  Once at most kFreeClimb items are left,
+        // each takes one thread of the first warps and climbs on its own, item in registers,
+        // without block barriers (the park / merge handshake works across warps).
         int cur = 0, c = 0;
         for (int guard = 0; guard < 2 * EB; ++guard) {
             __syncthreads();
             const int count = S.cnt[c];
-            if (count == 0) break;
+            if (count <= kFreeClimb) {
+                if (t < count) {
+                    float4 lo = S.q[cur][t][0], hi = S.q[cur][t][1];
+                    for (int g2 = 0; g2 < 2 * EB; ++g2) {
+                        if (!climb(lo, hi, nlo, nhi)) break;
+                        lo = nlo;
+                        hi = nhi;
+                    }
+                }
+                break;
+            }
             const int nc = c == 2 ? 0 : c + 1, rc = nc == 2 ? 0 : nc + 1;
             cont = false;
             if (t < count) cont = climb(S.q[cur][t][0], S.q[cur][t][1], nlo, nhi);
@@ -291,6 +304,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             cur ^= 1;
             c = nc;
         }
+        __syncthreads();
         // a child parked at a split whose sibling never came: the parent straddles the block
         if (t < m - 1) {
             const uint32_t mk = S.mask[t];
@@ -357,9 +371,9 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
             const float4 h1 = make_float4(xx, xy, xz, __int_as_float(is_left ? l : r));
             pend[2ull * own] = h0;
             pend[2ull * own + 1] = h1;
-            __threadfence();
+            fence_acq_rel_gpu();
             if (atomicExch(arrive + s, epoch) != epoch) { done = true; break; }  // first arrival
-            __threadfence();
+            fence_acq_rel_gpu();
             const float4 g0 = __ldcg(pend + 2ull * sib), g1 = __ldcg(pend + 2ull * sib + 1);
             const int sib_ref = __float_as_int(g0.w), sib_far = __float_as_int(g1.w);
             const int L = is_left ? l : sib_far, R = is_left ? sib_far : r;

@@ -66,6 +66,11 @@ __device__ __forceinline__ bool finite3(float4 v) {
     return isfinite(v.x) && isfinite(v.y) && isfinite(v.z);
 }
 
+// Acquire-release fences: order this thread's earlier memory operations before its later
+// ones for the given scope (the park / merge handshakes need no sequential consistency).
+__device__ __forceinline__ void fence_acq_rel_cta() { asm volatile("fence.acq_rel.cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 // Relaxed gpu-scope load / store of a 32-bit word another CTA publishes.
 __device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t *p) {
     uint32_t v;
