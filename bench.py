@@ -47,13 +47,15 @@ UNIT = "Mprims/s"
 
 # Algorithmic HBM bytes per triangle of each stage (fixed traffic model, 340 B in all): bounds
 # read 48; Morton read 48 + key 4; sort 48 (3 LSD passes of 30-bit keys: histogram read 4,
-# pass 1 read 4 write 8, passes 2-3 read 8 write 8); leaf gather perm 4 + gather 48 + write 48;
-# tree keys 4 + parents 8 + child links 8 + node words 56 + parent reads 8 + flag atomics 8.
-# The straddling-node pass completes part of the same tree and has no bytes of its own.
-MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "gather": 100, "tree": 92, "top": 0}
-KERNELS = {"bounds": ("k_bounds", 1), "morton": ("k_morton", 1), "sort": ("k_onesweep", 4),
-           "gather": ("k_leaf_gather", 1), "tree": ("k_tree_leaves", 1), "top": ("k_emit_top", 1)}
-LAUNCHES_PER_BUILD = 9  # bounds, morton, 4 onesweep passes, gather, tree, top
+# pass 1 read 4 write 8, passes 2-3 read 8 write 8); leaf gather perm 4 + gather 48 + write 48
+# and tree keys 4 + parents 8 + child links 8 + node words 56 + parent reads 8 + flag atomics 8,
+# both done by the one tree-pass kernel (the gather stage is fused into it).  The
+# straddling-node pass completes part of the same tree and has no bytes of its own.
+MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "gather": 0, "tree": 192, "top": 0}
+KERNELS = {"bounds": ("k_bounds", 1), "morton": ("k_morton", 1), "sort": ("k_scatter", 3),
+           "gather": (None, 0), "tree": ("k_tree_climb", 1), "top": ("k_emit_top", 1)}
+# bounds, morton, 3 sort passes x (tile histograms, chunk scan, scatter), tree, top
+LAUNCHES_PER_BUILD = 13
 MODEL_TOTAL = sum(MODEL_BYTES.values())  # 340 B per triangle
 
 

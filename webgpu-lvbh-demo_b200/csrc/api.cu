@@ -47,7 +47,7 @@ size_t control_bytes(uint32_t n) {
 // pass's open-node buffers, the control block and the look-back words.
 size_t arena_bytes(uint32_t cap) {
     const size_t groups = emit_groups(cap);
-    return 3 * align_up((size_t)cap * 4) + align_up((size_t)cap * 24) + align_up((size_t)cap * 32) +
+    return 4 * align_up((size_t)cap * 4) + align_up((size_t)cap * 32) +
            align_up(groups * kOpenCap * sizeof(OpenItem)) + align_up(groups * sizeof(uint32_t)) +
            align_up(sizeof(uint32_t)) + control_bytes(cap);
 }
@@ -77,7 +77,7 @@ struct lvbh_ctx {
     uint32_t cap = 0;
     void *arena = nullptr;
     uint32_t *keys_b = nullptr, *vals_b = nullptr;
-    float2 *lbox = nullptr;
+    uint32_t *keys_a = nullptr;  // unsorted Morton keys (input of the first sort pass)
     OpenItem *items = nullptr;
     uint32_t *counts = nullptr, *arrive = nullptr, *epoch = nullptr;
     float4 *pend = nullptr;
@@ -229,7 +229,7 @@ int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
     ctx->keys_b = reinterpret_cast<uint32_t *>(c); c += kb;
     ctx->vals_b = reinterpret_cast<uint32_t *>(c); c += kb;
     ctx->arrive = reinterpret_cast<uint32_t *>(c); c += kb;
-    ctx->lbox = reinterpret_cast<float2 *>(c); c += align_up((size_t)cap * 24);
+    ctx->keys_a = reinterpret_cast<uint32_t *>(c); c += kb;
     ctx->pend = reinterpret_cast<float4 *>(c); c += align_up((size_t)cap * 32);
     ctx->items = reinterpret_cast<OpenItem *>(c); c += align_up(groups * kOpenCap * sizeof(OpenItem));
     ctx->counts = reinterpret_cast<uint32_t *>(c); c += align_up(groups * sizeof(uint32_t));
@@ -264,9 +264,9 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
                     sizeof(Control) - offsetof(Control, err), s);
     if (!hb.use) launch_bounds(tri, n, ctx->ctl, s);
     if (profile) cudaEventRecord(ctx->ev[2], s);
-    // unsorted keys go to the leaf-box scratch (unused until K3a), so that the three passes
-    // ping-pong scratch -> result -> scratch -> result
-    uint32_t *keys_a = reinterpret_cast<uint32_t *>(ctx->lbox);
+    // unsorted keys go to keys_a, so that the three passes ping-pong keys_a -> result ->
+    // scratch -> result
+    uint32_t *keys_a = ctx->keys_a;
     launch_morton(tri, n, hb, ctx->ctl, keys_a, ctx->epoch, s);
     if (profile) cudaEventRecord(ctx->ev[3], s);
     launch_sort_pass(keys_a, nullptr, out->morton, out->leaf_index, n, 0, ctx->ctl, ctx->lookback, s);
@@ -274,7 +274,7 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
     launch_sort_pass(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 2, ctx->ctl, ctx->lookback, s);
     if (profile) cudaEventRecord(ctx->ev[4], s);
     launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
-                static_cast<float4 *>(out->nodes), out->parents, ctx->lbox, ctx->items, ctx->counts,
+                static_cast<float4 *>(out->nodes), out->parents, ctx->items, ctx->counts,
                 ctx->arrive, ctx->pend, ctx->epoch, ctx->ctl, s, profile ? ctx->ev + 5 : nullptr);
 }
 
@@ -295,7 +295,7 @@ void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool u
     launch_seg_tables(ctx->b_rows, bp.num_segs, ctx->b_tile_seg, ctx->b_blk_seg, s);
     launch_bounds_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, s);
     if (profile) cudaEventRecord(ctx->ev[2], s);
-    uint32_t *keys_a = reinterpret_cast<uint32_t *>(ctx->lbox);  // as in enqueue_build
+    uint32_t *keys_a = ctx->keys_a;
     launch_morton_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, ctx->b_hist,
                         ctx->ctl, keys_a, ctx->epoch, s);
     if (profile) cudaEventRecord(ctx->ev[3], s);
@@ -304,7 +304,7 @@ void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool u
     launch_onesweep_batch(bp, ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, 2, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
     if (profile) cudaEventRecord(ctx->ev[4], s);
     launch_emit_batch(bp, tri, out->leaf_index, out->morton, static_cast<float4 *>(out->tris),
-                      static_cast<float4 *>(out->nodes), out->parents, ctx->lbox, ctx->b_items,
+                      static_cast<float4 *>(out->nodes), out->parents, ctx->b_items,
                       ctx->b_counts, ctx->arrive, ctx->pend, ctx->epoch, ctx->ctl, s,
                       profile ? ctx->ev + 5 : nullptr);
 }

@@ -81,38 +81,11 @@ struct ManySegs {
     }
 };
 
-// K3a: leaf gather.  One thread per sorted position k: triangle perm[k] (3 x 16-byte loads)
-// to the output soup at k, its box (exact-zero components nudged by 1e-8 as
-// bvh-up-pass.js:209-210 does) to lbox[k] (min xyz, max xyz: 24 bytes).
-template <class Segs>
-__global__ void __launch_bounds__(256) k_leaf_gather(Segs segs, const float4 *__restrict__ tri,
-                                                     const uint32_t *__restrict__ perm,
-                                                     float4 *__restrict__ otri,
-                                                     float2 *__restrict__ lbox, Control *ctl) {
-    const Span sp = segs.span(blockIdx.x);
-    const int kl = sp.b0 + threadIdx.x;
-    if (kl >= sp.n) return;
-    const size_t k = sp.start + kl;
-    uint32_t ti = __ldg(perm + k);
-    if (ti >= (uint32_t)sp.n) { atomicOr(&ctl->err, ERR_CLIMB); ti = 0; }
-    const float4 *src = tri + 3ull * (sp.start + ti);
-    const float4 a = __ldg(src), b = __ldg(src + 1), c = __ldg(src + 2);
-    st_stream(otri + 3ull * k, a);
-    st_stream(otri + 3ull * k + 1, b);
-    st_stream(otri + 3ull * k + 2, c);
-    float nx = fminf(a.x, fminf(b.x, c.x)), ny = fminf(a.y, fminf(b.y, c.y)), nz = fminf(a.z, fminf(b.z, c.z));
-    float xx = fmaxf(a.x, fmaxf(b.x, c.x)), xy = fmaxf(a.y, fmaxf(b.y, c.y)), xz = fmaxf(a.z, fmaxf(b.z, c.z));
-    nx = nx == 0.0f ? -1e-8f : nx; ny = ny == 0.0f ? -1e-8f : ny; nz = nz == 0.0f ? -1e-8f : nz;
-    xx = xx == 0.0f ? 1e-8f : xx;  xy = xy == 0.0f ? 1e-8f : xy;  xz = xz == 0.0f ? 1e-8f : xz;
-    lbox[3ull * k] = make_float2(nx, ny);
-    lbox[3ull * k + 1] = make_float2(nz, xx);
-    lbox[3ull * k + 2] = make_float2(xy, xz);
-}
-
 // K3b shared memory.  A climbing item is two float4: box min + link (node index, or
 // -(leaf + 1)), box max + its packed local range and end separators
 // (l | r << 8 | (d[l-1] + 1) << 16 | (d[r] + 1) << 24).
 struct ClimbSmem {
+    float4 tri[2][EB][3];   // the gathered triangles of this block and the next (cp.async)
     float4 pend[EB][2][2];  // [split][side][min/max] the child parked at each split
     float4 q[2][EB][2];     // the items of the current and the next step
     uint32_t key[EB + 2];   // keys of leaves b0-1 .. b0+EB
@@ -127,11 +100,16 @@ __device__ __forceinline__ uint32_t pack_range(int l, int r, int dl, int dr) {
     return (uint32_t)l | ((uint32_t)r << 8) | ((uint32_t)(dl + 1) << 16) | ((uint32_t)(dr + 1) << 24);
 }
 
-// K3b: the tree over blocks of EB sorted leaves (see the pass list above).
+// K3b: leaf gather, rearrange and the tree over blocks of EB sorted leaves (see the pass list
+// above).  Leaf t of a block gathers triangle perm[b0 + t]: its index is loaded two blocks
+// ahead, its three 16-byte rows are copied into shared memory one block ahead (cp.async, no
+// registers held meanwhile), then written to the output soup and reduced to the leaf box.
 template <class Segs>
 __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
                                                     const uint32_t *__restrict__ keys_all,
-                                                    const float2 *__restrict__ lbox_all,
+                                                    const float4 *__restrict__ tri_all,
+                                                    const uint32_t *__restrict__ perm_all,
+                                                    float4 *__restrict__ otri_all,
                                                     float4 *nodes_all, int32_t *parents_all,
                                                     OpenItem *out_items, uint32_t *out_counts,
                                                     Control *ctl) {
@@ -141,25 +119,41 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
     const int nblk = segs.blocks();
     const uint32_t lt = lanemask_lt();
 
-    // registers of the next block: its span, this thread's key and leaf box, the two edge keys
+    // two blocks ahead: this thread's permutation entry
+    uint32_t pa = 0;
+    auto fetch_perm = [&](int blk) {
+        const Span sp = segs.span(blk);
+        if (sp.b0 + t < sp.n) pa = __ldg(perm_all + sp.start + sp.b0 + t);
+    };
+    // one block ahead: its span, this thread's key and triangle (into S.tri[buf]), edge keys
     Span nsp{0, 0, 0};
     uint32_t nk = 0, nk_lo = 0, nk_hi = 0;
-    float2 np0 = make_float2(0.f, 0.f), np1 = np0, np2 = np0;
-    auto fetch = [&](int blk) {
+    bool bad_perm = false;
+    auto fetch_leaf = [&](int blk, int buf) {
         nsp = segs.span(blk);
         const uint32_t *keys = keys_all + nsp.start;
-        const float2 *lbox = lbox_all + 3ull * nsp.start;
         const int b0 = nsp.b0, n = nsp.n, k = b0 + t;
         if (k < n) {
             nk = __ldg(keys + k);
-            np0 = __ldg(lbox + 3ull * k); np1 = __ldg(lbox + 3ull * k + 1); np2 = __ldg(lbox + 3ull * k + 2);
+            uint32_t ti = pa;
+            if (ti >= (uint32_t)n) { bad_perm = true; ti = 0; }
+            const float4 *src = tri_all + 3ull * (nsp.start + ti);
+            cp_async16(&S.tri[buf][t][0], src);
+            cp_async16(&S.tri[buf][t][1], src + 1);
+            cp_async16(&S.tri[buf][t][2], src + 2);
         }
+        cp_async_commit();
         if (t == 0) nk_lo = b0 > 0 ? __ldg(keys + b0 - 1) : 0u;
         if (t == EB - 1) nk_hi = (b0 + EB < n) ? __ldg(keys + b0 + EB) : 0u;
     };
-    if ((int)blockIdx.x < nblk) fetch(blockIdx.x);
+    int buf = 0;
+    if ((int)blockIdx.x < nblk) {
+        fetch_perm(blockIdx.x);
+        fetch_leaf(blockIdx.x, 0);
+        if ((int)(blockIdx.x + gridDim.x) < nblk) fetch_perm(blockIdx.x + gridDim.x);
+    }
 
-    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x, buf ^= 1) {
         const Span sp = nsp;
         const int b0 = sp.b0, n = sp.n;
         float4 *nodes = nodes_all + 4ull * sp.start;
@@ -175,9 +169,28 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
         S.pleaf[t] = -1;
         if (t < 3) S.cnt[t] = 0;
         if (t == 0) S.open = 0;
-        const float4 leaf_lo = make_float4(np0.x, np0.y, np1.x, __int_as_float(-(k + 1)));
-        const float4 leaf_hi0 = make_float4(np1.y, np2.x, np2.y, 0.f);
-        if (blk + (int)gridDim.x < nblk) fetch(blk + gridDim.x);
+        // this leaf's triangle: to the output soup, and its box (exact-zero components nudged
+        // by 1e-8 as bvh-up-pass.js:209-210 does)
+        cp_async_wait_all();
+        float4 leaf_lo = make_float4(0.f, 0.f, 0.f, __int_as_float(-(k + 1)));
+        float4 leaf_hi0 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (active) {
+            const float4 a = S.tri[buf][t][0], b = S.tri[buf][t][1], c = S.tri[buf][t][2];
+            float4 *dst = otri_all + 3ull * (sp.start + k);
+            st_stream(dst, a);
+            st_stream(dst + 1, b);
+            st_stream(dst + 2, c);
+            float nx = fminf(a.x, fminf(b.x, c.x)), ny = fminf(a.y, fminf(b.y, c.y)), nz = fminf(a.z, fminf(b.z, c.z));
+            float xx = fmaxf(a.x, fmaxf(b.x, c.x)), xy = fmaxf(a.y, fmaxf(b.y, c.y)), xz = fmaxf(a.z, fmaxf(b.z, c.z));
+            nx = nx == 0.0f ? -1e-8f : nx; ny = ny == 0.0f ? -1e-8f : ny; nz = nz == 0.0f ? -1e-8f : nz;
+            xx = xx == 0.0f ? 1e-8f : xx;  xy = xy == 0.0f ? 1e-8f : xy;  xz = xz == 0.0f ? 1e-8f : xz;
+            leaf_lo = make_float4(nx, ny, nz, __int_as_float(-(k + 1)));
+            leaf_hi0 = make_float4(xx, xy, xz, 0.f);
+        }
+        if (blk + (int)gridDim.x < nblk) {
+            fetch_leaf(blk + gridDim.x, buf ^ 1);
+            if (blk + 2 * (int)gridDim.x < nblk) fetch_perm(blk + 2 * gridDim.x);
+        }
         if (n == 1) {  // one leaf, one arrival at node 0: left slot only, f_1 = 1
             if (t == 0) {
                 nodes[0] = make_float4(leaf_lo.x, leaf_lo.y, leaf_lo.z, __int_as_float(-1));
@@ -324,6 +337,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
         }
         __syncthreads();  // before the next block overwrites shared memory
     }
+    if (bad_perm) atomicOr(&ctl->err, ERR_CLIMB);
 }
 
 // K3c: the nodes that straddle blocks.  kTopLanes threads per block of K3b; each climbs one of
@@ -403,14 +417,13 @@ inline size_t leaves_smem_bytes() { return sizeof(ClimbSmem); }
 template <class Segs>
 void launch_emit_impl(Segs segs, int groups, const float4 *tri, const uint32_t *perm,
                       const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
-                      float2 *lbox, OpenItem *items, uint32_t *counts, uint32_t *arrive,
-                      float4 *pend, const uint32_t *epoch, Control *ctl, bool top,
-                      cudaStream_t s, cudaEvent_t *ev) {
-    k_leaf_gather<<<groups, 256, 0, s>>>(segs, tri, perm, otri, lbox, ctl);
-    if (ev) cudaEventRecord(ev[0], s);
+                      OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
+                      const uint32_t *epoch, Control *ctl, bool top, cudaStream_t s,
+                      cudaEvent_t *ev) {
+    if (ev) cudaEventRecord(ev[0], s);  // the leaf gather runs inside the tree pass
     const int grid = min(groups, sm_count() * kTreeCtasPerSm);
-    k_tree_climb<<<grid, EB, leaves_smem_bytes(), s>>>(segs, keys, lbox, nodes, parents, items,
-                                                         counts, ctl);
+    k_tree_climb<<<grid, EB, leaves_smem_bytes(), s>>>(segs, keys, tri, perm, otri, nodes, parents,
+                                                        items, counts, ctl);
     if (ev) cudaEventRecord(ev[1], s);
     if (top)
         k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, counts, keys, nodes,
@@ -439,24 +452,23 @@ cudaError_t emit_init() {
 }
 
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
-                 float4 *otri, float4 *nodes, int32_t *parents, float2 *lbox, OpenItem *items,
+                 float4 *otri, float4 *nodes, int32_t *parents, OpenItem *items,
                  uint32_t *counts, uint32_t *arrive, float4 *pend, const uint32_t *epoch,
                  Control *ctl, cudaStream_t s, cudaEvent_t *ev) {
     if (n == 0) return;
     const int groups = (int)emit_groups(n);
-    launch_emit_impl(OneSeg{(int)n}, groups, tri, perm, keys, otri, nodes, parents, lbox, items,
-                     counts, arrive, pend, epoch, ctl, groups > 1, s, ev);
+    launch_emit_impl(OneSeg{(int)n}, groups, tri, perm, keys, otri, nodes, parents, items, counts,
+                     arrive, pend, epoch, ctl, groups > 1, s, ev);
 }
 
 void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
                        const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
-                       float2 *lbox, OpenItem *items, uint32_t *counts, uint32_t *arrive,
+                       OpenItem *items, uint32_t *counts, uint32_t *arrive,
                        float4 *pend, const uint32_t *epoch, Control *ctl, cudaStream_t s,
                        cudaEvent_t *ev) {
     if (bp.blocks == 0) return;
     launch_emit_impl(ManySegs{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks, tri, perm, keys,
-                     otri, nodes, parents, lbox, items, counts, arrive, pend, epoch, ctl, true, s,
-                     ev);
+                     otri, nodes, parents, items, counts, arrive, pend, epoch, ctl, true, s, ev);
 }
 
 }  // namespace lvbh

@@ -98,15 +98,15 @@ void launch_onesweep32(const uint32_t *keys_in, const uint32_t *vals_in, uint32_
                        uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *lookback,
                        cudaStream_t s);
 cudaError_t sort_init();  // once per device, before the first launch
-// K3: leaf gather + rearrange (K3a), in-block radix tree + refit (K3b), straddling nodes (K3c)
-// -> BVH nodes, parent links, sorted triangles.  Scratch: lbox (3 float2 per triangle),
-// items (emit_groups(n) * kOpenCap) and counts (emit_groups(n)), arrive (n words, zero or
-// older epochs), pend (2n float4); *epoch is this build's epoch (advanced by K1b).
+// K3: leaf gather + rearrange + in-block radix tree and refit (K3b), straddling nodes (K3c)
+// -> BVH nodes, parent links, sorted triangles.  Scratch: items (emit_groups(n) * kOpenCap)
+// and counts (emit_groups(n)), arrive (n words, zero or older epochs), pend (2n float4);
+// *epoch is this build's epoch (advanced by K1b).
 size_t emit_groups(uint32_t n);
 cudaError_t emit_init();  // once per device, before the first launch
-// ev (may be nullptr): three events recorded after K3a, K3b and K3c.
+// ev (may be nullptr): three events, recorded before K3b, after K3b and after K3c.
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
-                 float4 *otri, float4 *nodes, int32_t *parents, float2 *lbox, OpenItem *items,
+                 float4 *otri, float4 *nodes, int32_t *parents, OpenItem *items,
                  uint32_t *counts, uint32_t *arrive, float4 *pend, const uint32_t *epoch,
                  Control *ctl, cudaStream_t s, cudaEvent_t *ev);
 // Batched forms of K1a, K1b, K2 and K3 over the segments of `bp`.  seg_ord holds 6 ordered
@@ -128,9 +128,8 @@ void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const u
 // items / counts: bp.blocks * kOpenCap / bp.blocks entries.
 void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
                        const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
-                       float2 *lbox, OpenItem *items, uint32_t *counts, uint32_t *arrive,
-                       float4 *pend, const uint32_t *epoch, Control *ctl, cudaStream_t s,
-                       cudaEvent_t *ev);
+                       OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
+                       const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev);
 // Indexed mesh -> 48-byte soup (pad 0).  An index >= num_verts sets ERR_BAD_INDEX in
 // *err and gathers zeros instead of reading out of bounds.
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,
