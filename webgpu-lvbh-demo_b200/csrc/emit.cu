@@ -43,7 +43,7 @@ namespace {
 
 constexpr int EB = kEmitBlock;                 // level 1: leaves (threads) per CTA
 constexpr int kLogEB = 8;                      // EB == 1 << kLogEB
-constexpr int kTreeCtasPerSm = 3;             // resident K3b CTAs per SM (persistent grid)
+constexpr int kTreeCtasPerSm = 4;             // resident K3b CTAs per SM (persistent grid)
 constexpr int kTopLanes = 8;                   // K3c threads per block of K3b
 constexpr int kFreeClimb = 64;                 // K3b items left when compaction stops
 
@@ -87,7 +87,8 @@ struct ManySegs {
 struct ClimbSmem {
     float4 tri[2][EB][3];   // the gathered triangles of this block and the next (cp.async)
     float4 pend[EB][2][2];  // [split][side][min/max] the child parked at each split
-    float4 q[2][EB][2];     // the items of the current and the next step
+    float4 q[2][EB / 2][2]; // the items of the current and the next step (a step after the
+                            // first has at most EB / 2: every merge takes two items)
     uint32_t key[EB + 2];   // keys of leaves b0-1 .. b0+EB
     uint32_t mask[EB];      // arrivals at each split: bit 0 left child, bit 1 right child
     int pint[EB];           // parent of internal node b0 + j (-1 = not set here)
