@@ -43,6 +43,7 @@ namespace {
 
 constexpr int EB = kEmitBlock;                 // level 1: leaves (threads) per CTA
 constexpr int kLogEB = 8;                      // EB == 1 << kLogEB
+static_assert(EB == 1 << kLogEB && 2 * kLogEB + 14 <= 32, "packed item ranges");
 constexpr int kTreeCtasPerSm = 4;             // resident K3b CTAs per SM (persistent grid)
 constexpr int kTopLanes = 8;                   // K3c threads per block of K3b
 constexpr int kFreeClimb = 64;                 // K3b items left when compaction stops
@@ -83,7 +84,7 @@ struct ManySegs {
 
 // K3b shared memory.  A climbing item is two float4: box min + link (node index, or
 // -(leaf + 1)), box max + its packed local range and end separators
-// (l | r << 8 | (d[l-1] + 1) << 16 | (d[r] + 1) << 24).
+// (l | r << kLogEB | (d[l-1] + 1) << 2 kLogEB | (d[r] + 1) << 2 kLogEB + 7; d + 1 <= 64).
 struct ClimbSmem {
     float4 tri[2][EB][3];   // the gathered triangles of this block and the next (cp.async)
     float4 pend[EB][2][2];  // [split][side][min/max] the child parked at each split
@@ -98,8 +99,13 @@ struct ClimbSmem {
 };
 
 __device__ __forceinline__ uint32_t pack_range(int l, int r, int dl, int dr) {
-    return (uint32_t)l | ((uint32_t)r << 8) | ((uint32_t)(dl + 1) << 16) | ((uint32_t)(dr + 1) << 24);
+    return (uint32_t)l | ((uint32_t)r << kLogEB) | ((uint32_t)(dl + 1) << (2 * kLogEB)) |
+           ((uint32_t)(dr + 1) << (2 * kLogEB + 7));
 }
+__device__ __forceinline__ int range_l(uint32_t p) { return (int)(p & (EB - 1)); }
+__device__ __forceinline__ int range_r(uint32_t p) { return (int)((p >> kLogEB) & (EB - 1)); }
+__device__ __forceinline__ int range_dl(uint32_t p) { return (int)((p >> (2 * kLogEB)) & 127u) - 1; }
+__device__ __forceinline__ int range_dr(uint32_t p) { return (int)(p >> (2 * kLogEB + 7)) - 1; }
 
 // K3b: leaf gather, rearrange and the tree over blocks of EB sorted leaves (see the pass list
 // above).  Leaf t of a block gathers triangle perm[b0 + t]: its index is loaded two blocks
@@ -223,9 +229,9 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             const uint32_t pk = __float_as_uint(hi.w);
             OpenItem it;
             it.lo = lo;
-            it.hi = make_float4(hi.x, hi.y, hi.z, __int_as_float((int)(pk >> 24) - 1));
-            it.xl = b0 + (int)(pk & 255u);
-            it.xr = b0 + (int)((pk >> 8) & 255u);
+            it.hi = make_float4(hi.x, hi.y, hi.z, __int_as_float(range_dr(pk)));
+            it.xl = b0 + range_l(pk);
+            it.xr = b0 + range_r(pk);
             it.pad0 = it.pad1 = 0;
             const int at = atomicAdd(&S.open, 1);
             if (at < kOpenCap) out[at] = it;
@@ -235,8 +241,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
         // parked sibling into the parent (returned in nlo/nhi, true unless it is the root).
         auto climb = [&](float4 lo, float4 hi, float4 &nlo, float4 &nhi) -> bool {
             const uint32_t pk = __float_as_uint(hi.w);
-            const int l = (int)(pk & 255u), r = (int)((pk >> 8) & 255u);
-            const int dl = (int)((pk >> 16) & 255u) - 1, dr = (int)(pk >> 24) - 1;
+            const int l = range_l(pk), r = range_r(pk), dl = range_dl(pk), dr = range_dr(pk);
             const bool is_left = dr > dl;
             const int s = is_left ? r : l - 1;
             if (s < 0 || s > m - 2) {
@@ -253,8 +258,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             const float4 Llo = is_left ? lo : slo, Lhi = is_left ? hi : shi;
             const float4 Rlo = is_left ? slo : lo, Rhi = is_left ? shi : hi;
             const uint32_t lpk = __float_as_uint(Lhi.w), rpk = __float_as_uint(Rhi.w);
-            const int L = (int)(lpk & 255u), R = (int)((rpk >> 8) & 255u);
-            const int ndl = (int)((lpk >> 16) & 255u) - 1, ndr = (int)(rpk >> 24) - 1;
+            const int L = range_l(lpk), R = range_r(rpk), ndl = range_dl(lpk), ndr = range_dr(rpk);
             const bool root = (b0 + L == 0) && (b0 + R == n - 1);
             const int P = root ? 0 : (ndr > ndl ? b0 + R : b0 + L);
             float4 *rc = nodes + 4ull * P;
