@@ -87,9 +87,11 @@ struct ManySegs {
 // (l | r << kLogEB | (d[l-1] + 1) << 2 kLogEB | (d[r] + 1) << 2 kLogEB + 7; d + 1 <= 64).
 struct ClimbSmem {
     float4 tri[2][EB][3];   // the gathered triangles of this block and the next (cp.async)
-    float4 pend[EB][2][2];  // [split][side][min/max] the child parked at each split
-    float4 q[2][EB / 2][2]; // the items of the current and the next step (a step after the
-                            // first has at most EB / 2: every merge takes two items)
+    float4 pend[2][2][EB];  // [side][min/max][split] the child parked at each split
+    float4 q[2][2][EB / 2]; // [queue][min/max][item] the items of the current and the next
+                            // step (a step after the first has at most EB / 2: every merge
+                            // takes two items).  Split / item index innermost keeps the
+                            // 16-byte accesses of random splits off each other's banks.
     uint32_t key[EB + 2];   // keys of leaves b0-1 .. b0+EB
     uint32_t mask[EB];      // arrivals at each split: bit 0 left child, bit 1 right child
     int pint[EB];           // parent of internal node b0 + j (-1 = not set here)
@@ -249,12 +251,12 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
                 return false;
             }
             const int side = is_left ? 0 : 1;
-            S.pend[s][side][0] = lo;
-            S.pend[s][side][1] = hi;
+            S.pend[side][0][s] = lo;
+            S.pend[side][1][s] = hi;
             fence_acq_rel_cta();
             if (atomicOr(&S.mask[s], 1u << side) == 0u) return false;  // first arrival parks
             fence_acq_rel_cta();
-            const float4 slo = S.pend[s][side ^ 1][0], shi = S.pend[s][side ^ 1][1];
+            const float4 slo = S.pend[side ^ 1][0][s], shi = S.pend[side ^ 1][1][s];
             const float4 Llo = is_left ? lo : slo, Lhi = is_left ? hi : shi;
             const float4 Rlo = is_left ? slo : lo, Rhi = is_left ? shi : hi;
             const uint32_t lpk = __float_as_uint(Lhi.w), rpk = __float_as_uint(Rhi.w);
@@ -283,8 +285,8 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             base = __shfl_sync(0xFFFFFFFFu, base, 0);
             if (cont) {
                 const int at = base + __popc(bal & lt);
-                S.q[oq][at][0] = nlo;
-                S.q[oq][at][1] = nhi;
+                S.q[oq][0][at] = nlo;
+                S.q[oq][1][at] = nhi;
             }
         };
 
@@ -305,7 +307,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             const int count = S.cnt[c];
             if (count <= kFreeClimb) {
                 if (t < count) {
-                    float4 lo = S.q[cur][t][0], hi = S.q[cur][t][1];
+                    float4 lo = S.q[cur][0][t], hi = S.q[cur][1][t];
                     for (int g2 = 0; g2 < 2 * EB; ++g2) {
                         if (!climb(lo, hi, nlo, nhi)) break;
                         lo = nlo;
@@ -316,7 +318,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             }
             const int nc = c == 2 ? 0 : c + 1, rc = nc == 2 ? 0 : nc + 1;
             cont = false;
-            if (t < count) cont = climb(S.q[cur][t][0], S.q[cur][t][1], nlo, nhi);
+            if (t < count) cont = climb(S.q[cur][0][t], S.q[cur][1][t], nlo, nhi);
             append(cont, nlo, nhi, cur ^ 1, nc);
             if (t == 0) S.cnt[rc] = 0;
             cur ^= 1;
@@ -328,7 +330,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             const uint32_t mk = S.mask[t];
             if (mk == 1u || mk == 2u) {
                 const int side = mk == 1u ? 0 : 1;
-                emit(S.pend[t][side][0], S.pend[t][side][1]);
+                emit(S.pend[side][0][t], S.pend[side][1][t]);
             }
         }
         __syncthreads();
