@@ -47,7 +47,7 @@ size_t control_bytes(uint32_t n) {
 // pass's open-node buffers, the control block and the look-back words.
 size_t arena_bytes(uint32_t cap) {
     const size_t groups = emit_groups(cap);
-    return 4 * align_up((size_t)cap * 4) + align_up((size_t)cap * 32) +
+    return 4 * align_up((size_t)cap * 4) + align_up((size_t)cap * 32) + align_up((size_t)cap) +
            align_up(groups * kOpenCap * sizeof(OpenItem)) + align_up(groups * sizeof(uint32_t)) +
            align_up(sizeof(uint32_t)) + control_bytes(cap);
 }
@@ -81,6 +81,7 @@ struct lvbh_ctx {
     OpenItem *items = nullptr;
     uint32_t *counts = nullptr, *arrive = nullptr, *epoch = nullptr;
     float4 *pend = nullptr;
+    uint8_t *pend_d = nullptr;
     Control *ctl = nullptr;
     uint32_t *lookback = nullptr;  // the sort's tile and chunk histograms
     // staging for host input
@@ -231,6 +232,7 @@ int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
     ctx->arrive = reinterpret_cast<uint32_t *>(c); c += kb;
     ctx->keys_a = reinterpret_cast<uint32_t *>(c); c += kb;
     ctx->pend = reinterpret_cast<float4 *>(c); c += align_up((size_t)cap * 32);
+    ctx->pend_d = reinterpret_cast<uint8_t *>(c); c += align_up((size_t)cap);
     ctx->items = reinterpret_cast<OpenItem *>(c); c += align_up(groups * kOpenCap * sizeof(OpenItem));
     ctx->counts = reinterpret_cast<uint32_t *>(c); c += align_up(groups * sizeof(uint32_t));
     ctx->epoch = reinterpret_cast<uint32_t *>(c); c += align_up(sizeof(uint32_t));
@@ -275,7 +277,8 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
     if (profile) cudaEventRecord(ctx->ev[4], s);
     launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
                 static_cast<float4 *>(out->nodes), out->parents, ctx->items, ctx->counts,
-                ctx->arrive, ctx->pend, ctx->epoch, ctx->ctl, s, profile ? ctx->ev + 5 : nullptr);
+                ctx->arrive, ctx->pend, ctx->pend_d, ctx->epoch, ctx->ctl, s,
+                profile ? ctx->ev + 5 : nullptr);
 }
 
 // The batched build: every launch on `s`.  The segment table (and host bounds) are copied from
@@ -305,7 +308,7 @@ void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool u
     if (profile) cudaEventRecord(ctx->ev[4], s);
     launch_emit_batch(bp, tri, out->leaf_index, out->morton, static_cast<float4 *>(out->tris),
                       static_cast<float4 *>(out->nodes), out->parents, ctx->b_items,
-                      ctx->b_counts, ctx->arrive, ctx->pend, ctx->epoch, ctx->ctl, s,
+                      ctx->b_counts, ctx->arrive, ctx->pend, ctx->pend_d, ctx->epoch, ctx->ctl, s,
                       profile ? ctx->ev + 5 : nullptr);
 }
 

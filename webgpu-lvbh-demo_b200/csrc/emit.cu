@@ -48,12 +48,6 @@ constexpr int kTreeCtasPerSm = 4;             // resident K3b CTAs per SM (persi
 constexpr int kTopLanes = 8;                   // K3c threads per block of K3b
 constexpr int kFreeClimb = 64;                 // K3b items left when compaction stops
 
-__device__ __forceinline__ int dd_global(const uint32_t *__restrict__ keys, int n, int x) {
-    if (x < 0 || x >= n - 1) return -1;
-    const uint32_t a = __ldg(keys + x), b = __ldg(keys + x + 1);
-    return a != b ? __clz(a ^ b) : 32 + __clz(x ^ (x + 1));
-}
-
 // Where a block of EB sorted leaves lives.  A batched build is a list of segments (meshes)
 // laid end to end; every block lies inside one segment and every index a kernel works with
 // is local to that segment (the plain build is the one-segment case).
@@ -234,7 +228,8 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             it.hi = make_float4(hi.x, hi.y, hi.z, __int_as_float(range_dr(pk)));
             it.xl = b0 + range_l(pk);
             it.xr = b0 + range_r(pk);
-            it.pad0 = it.pad1 = 0;
+            it.pad0 = range_dl(pk);
+            it.pad1 = 0;
             const int at = atomicAdd(&S.open, 1);
             if (at < kOpenCap) out[at] = it;
             else atomicOr(&ctl->err, ERR_CLIMB);
@@ -348,20 +343,23 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
 }
 
 // K3c: the nodes that straddle blocks.  kTopLanes threads per block of K3b; each climbs one of
-// the block's open items (a block leaves about 8) through the remaining splits.  At a split the first arriving child parks
-// its box, link and far range end in pend[] at its own index (r when it is a left child, l
-// when a right child - no two pending children ever share one), fences, and exchanges the
-// build's epoch into the split's arrival word; the second, seeing the epoch already there,
-// reads its sibling back, merges, finds the parent's range and Karras index and writes the
-// record and both parent links.  Nothing waits, so the kernel cannot hang; climbs are bounded
-// and every index is range-checked.  The epoch makes the arrival words reusable without
-// clearing: a word left by an older build never equals the current epoch.
+// the block's open items (a block leaves about 8) through the remaining splits.  At a split the
+// first arriving child parks its box, link and far range end in pend[] and its far end's
+// separator in pend_d[], both at its own index (r when it is a left child, l when a right child -
+// no two pending children ever share one), fences, and exchanges the build's epoch into the
+// split's arrival word; the second, seeing the epoch already there, reads its sibling back,
+// merges, and has the parent's range, both end separators and so its Karras index without
+// touching the keys.  A completed record and its two parent links are stored after the next
+// split's exchange, so the fence before that exchange waits for the two parked rows only.
+// Nothing waits, so the kernel cannot hang; climbs are bounded and every index is
+// range-checked.  The epoch makes the arrival words reusable without clearing: a word left by
+// an older build never equals the current epoch.
 template <class Segs>
 __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__restrict__ items,
                                                   const uint32_t *__restrict__ counts,
-                                                  const uint32_t *__restrict__ keys_all,
                                                   float4 *nodes_all, int32_t *parents_all,
                                                   uint32_t *arrive_all, float4 *pend_all,
+                                                  uint8_t *pend_d_all,
                                                   const uint32_t *__restrict__ epoch_p,
                                                   Control *ctl) {
     const int gw = (blockIdx.x * 256 + threadIdx.x) / kTopLanes, lane = threadIdx.x % kTopLanes;
@@ -371,16 +369,28 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
     const uint32_t epoch = *epoch_p;
     const Span sp = segs.span(gw);
     const int n = sp.n;
-    const uint32_t *keys = keys_all + sp.start;
     float4 *nodes = nodes_all + 4ull * sp.start;
     int32_t *parents = parents_all + 2ull * sp.start;
     uint32_t *arrive = arrive_all + sp.start;
     float4 *pend = pend_all + 2ull * sp.start;
+    uint8_t *pend_d = pend_d_all + sp.start;
     for (int q = lane; q < cnt; q += kTopLanes) {
         const OpenItem it = items[(size_t)gw * kOpenCap + q];
         int l = it.xl, r = it.xr, ref = __float_as_int(it.lo.w);
         float nx = it.lo.x, ny = it.lo.y, nz = it.lo.z, xx = it.hi.x, xy = it.hi.y, xz = it.hi.z;
-        int dl = dd_global(keys, n, l - 1), dr = __float_as_int(it.hi.w);
+        int dl = it.pad0, dr = __float_as_int(it.hi.w);
+        // the record completed at the previous split, stored after the next exchange
+        bool have = false;
+        float4 w0, w1, w2, w3;
+        int wP = 0, wl = 0, wr = 0;
+        auto flush = [&]() {
+            if (!have) return;
+            float4 *rc = nodes + 4ull * wP;
+            rc[0] = w0; rc[1] = w1; rc[2] = w2; rc[3] = w3;
+            parents[wl >= 0 ? wl : n - (wl + 1)] = wP;
+            parents[wr >= 0 ? wr : n - (wr + 1)] = wP;
+            have = false;
+        };
         bool done = false;
         for (int level = 0; level < 160; ++level) {
             if (l == 0 && r == n - 1) { done = true; break; }  // root complete
@@ -392,10 +402,14 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
             const float4 h1 = make_float4(xx, xy, xz, __int_as_float(is_left ? l : r));
             pend[2ull * own] = h0;
             pend[2ull * own + 1] = h1;
+            pend_d[own] = (uint8_t)((is_left ? dl : dr) + 1);
             fence_acq_rel_gpu();
-            if (atomicExch(arrive + s, epoch) != epoch) { done = true; break; }  // first arrival
+            const bool first = atomicExch(arrive + s, epoch) != epoch;
+            flush();
+            if (first) { done = true; break; }  // the sibling completes the parent
             fence_acq_rel_gpu();
             const float4 g0 = __ldcg(pend + 2ull * sib), g1 = __ldcg(pend + 2ull * sib + 1);
+            const int gd = (int)__ldcg(pend_d + sib) - 1;
             const int sib_ref = __float_as_int(g0.w), sib_far = __float_as_int(g1.w);
             const int L = is_left ? l : sib_far, R = is_left ? sib_far : r;
             if (L < 0 || R >= n || L > l || R < r || sib_ref < -n || sib_ref >= n - 1) break;
@@ -403,18 +417,19 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
             const float4 hi0 = is_left ? g0 : h0, hi1 = is_left ? g1 : h1;
             nx = fminf(nx, g0.x); ny = fminf(ny, g0.y); nz = fminf(nz, g0.z);
             xx = fmaxf(xx, g1.x); xy = fmaxf(xy, g1.y); xz = fmaxf(xz, g1.z);
-            const int ndl = dd_global(keys, n, L - 1), ndr = dd_global(keys, n, R);
+            const int ndl = is_left ? dl : gd, ndr = is_left ? gd : dr;
             const int P = (L == 0 && R == n - 1) ? 0 : (ndr > ndl ? R : L);
-            float4 *rc = nodes + 4ull * P;
-            rc[0] = lo0;
-            rc[1] = make_float4(lo1.x, lo1.y, lo1.z, __int_as_float(2));
-            rc[2] = hi0;
-            rc[3] = make_float4(hi1.x, hi1.y, hi1.z, __int_as_float(0));
-            const int lref = __float_as_int(lo0.w), rref = __float_as_int(hi0.w);
-            parents[lref >= 0 ? lref : n - (lref + 1)] = P;
-            parents[rref >= 0 ? rref : n - (rref + 1)] = P;
+            w0 = lo0;
+            w1 = make_float4(lo1.x, lo1.y, lo1.z, __int_as_float(2));
+            w2 = hi0;
+            w3 = make_float4(hi1.x, hi1.y, hi1.z, __int_as_float(0));
+            wP = P;
+            wl = __float_as_int(lo0.w);
+            wr = __float_as_int(hi0.w);
+            have = true;
             l = L; r = R; ref = P; dl = ndl; dr = ndr;
         }
+        flush();
         if (!done) atomicOr(&ctl->err, ERR_CLIMB);
     }
 }
@@ -425,17 +440,17 @@ template <class Segs>
 void launch_emit_impl(Segs segs, int groups, const float4 *tri, const uint32_t *perm,
                       const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
                       OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
-                      const uint32_t *epoch, Control *ctl, bool top, cudaStream_t s,
-                      cudaEvent_t *ev) {
+                      uint8_t *pend_d, const uint32_t *epoch, Control *ctl, bool top,
+                      cudaStream_t s, cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], s);  // the leaf gather runs inside the tree pass
     const int grid = min(groups, sm_count() * kTreeCtasPerSm);
     k_tree_climb<<<grid, EB, leaves_smem_bytes(), s>>>(segs, keys, tri, perm, otri, nodes, parents,
                                                         items, counts, ctl);
     if (ev) cudaEventRecord(ev[1], s);
     if (top)
-        k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, counts, keys, nodes,
-                                                                     parents, arrive, pend, epoch,
-                                                                     ctl);
+        k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, counts, nodes,
+                                                                     parents, arrive, pend, pend_d,
+                                                                     epoch, ctl);
     if (ev) cudaEventRecord(ev[2], s);
 }
 
@@ -460,22 +475,23 @@ cudaError_t emit_init() {
 
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
                  float4 *otri, float4 *nodes, int32_t *parents, OpenItem *items,
-                 uint32_t *counts, uint32_t *arrive, float4 *pend, const uint32_t *epoch,
-                 Control *ctl, cudaStream_t s, cudaEvent_t *ev) {
+                 uint32_t *counts, uint32_t *arrive, float4 *pend, uint8_t *pend_d,
+                 const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev) {
     if (n == 0) return;
     const int groups = (int)emit_groups(n);
     launch_emit_impl(OneSeg{(int)n}, groups, tri, perm, keys, otri, nodes, parents, items, counts,
-                     arrive, pend, epoch, ctl, groups > 1, s, ev);
+                     arrive, pend, pend_d, epoch, ctl, groups > 1, s, ev);
 }
 
 void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
                        const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
-                       OpenItem *items, uint32_t *counts, uint32_t *arrive,
-                       float4 *pend, const uint32_t *epoch, Control *ctl, cudaStream_t s,
+                       OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
+                       uint8_t *pend_d, const uint32_t *epoch, Control *ctl, cudaStream_t s,
                        cudaEvent_t *ev) {
     if (bp.blocks == 0) return;
     launch_emit_impl(ManySegs{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks, tri, perm, keys,
-                     otri, nodes, parents, items, counts, arrive, pend, epoch, ctl, true, s, ev);
+                     otri, nodes, parents, items, counts, arrive, pend, pend_d, epoch, ctl, true, s,
+                     ev);
 }
 
 }  // namespace lvbh

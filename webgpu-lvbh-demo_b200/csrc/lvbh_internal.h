@@ -32,11 +32,12 @@ constexpr int kEmitBlock = 256;
 constexpr int kOpenCap = 128;
 
 // A complete subtree handed from one level of the tree pass to the next: box min + link,
-// box max + the separator d after it, and its leaf range.
+// box max + the separator d after it (d[xr]), its leaf range and the separator before it
+// (d[xl - 1]).
 struct __align__(16) OpenItem {
     float4 lo;
     float4 hi;
-    int xl, xr, pad0, pad1;
+    int xl, xr, pad0, pad1;  // pad0: d[xl - 1]
 };
 
 // Per-build control block in device memory.  Everything from `err` on is zeroed by one memset
@@ -100,15 +101,15 @@ void launch_onesweep32(const uint32_t *keys_in, const uint32_t *vals_in, uint32_
 cudaError_t sort_init();  // once per device, before the first launch
 // K3: leaf gather + rearrange + in-block radix tree and refit (K3b), straddling nodes (K3c)
 // -> BVH nodes, parent links, sorted triangles.  Scratch: items (emit_groups(n) * kOpenCap)
-// and counts (emit_groups(n)), arrive (n words, zero or older epochs), pend (2n float4);
-// *epoch is this build's epoch (advanced by K1b).
+// and counts (emit_groups(n)), arrive (n words, zero or older epochs), pend (2n float4),
+// pend_d (n bytes); *epoch is this build's epoch (advanced by K1b).
 size_t emit_groups(uint32_t n);
 cudaError_t emit_init();  // once per device, before the first launch
 // ev (may be nullptr): three events, recorded before K3b, after K3b and after K3c.
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
                  float4 *otri, float4 *nodes, int32_t *parents, OpenItem *items,
-                 uint32_t *counts, uint32_t *arrive, float4 *pend, const uint32_t *epoch,
-                 Control *ctl, cudaStream_t s, cudaEvent_t *ev);
+                 uint32_t *counts, uint32_t *arrive, float4 *pend, uint8_t *pend_d,
+                 const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev);
 // Batched forms of K1a, K1b, K2 and K3 over the segments of `bp`.  seg_ord holds 6 ordered
 // bound words per segment (zeroed before K1a; min at 0-2 as ~ord_lo, max at 3-5 as ord_lo),
 // seg_hist 4 x 256 digit counts per segment (zeroed before K1b); host_bounds, when not null,
@@ -129,7 +130,8 @@ void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const u
 void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
                        const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
                        OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
-                       const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev);
+                       uint8_t *pend_d, const uint32_t *epoch, Control *ctl, cudaStream_t s,
+                       cudaEvent_t *ev);
 // Indexed mesh -> 48-byte soup (pad 0).  An index >= num_verts sets ERR_BAD_INDEX in
 // *err and gathers zeros instead of reading out of bounds.
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,
