@@ -88,8 +88,8 @@ struct ClimbSmem {
                             // 16-byte accesses of random splits off each other's banks.
     uint32_t key[EB + 2];   // keys of leaves b0-1 .. b0+EB
     uint32_t mask[EB];      // arrivals at each split: bit 0 left child, bit 1 right child
-    int pint[EB];           // parent of internal node b0 + j (-1 = not set here)
-    int pleaf[EB];          // parent of leaf b0 + j (-1 = not set here)
+    int par[2 * EB];        // parent of internal node b0 + j at j, of leaf b0 + j at EB + j
+                            // (-1 = not set here)
     int cnt[3];             // item counters, rotating over the steps
     int open;               // open items emitted
 };
@@ -168,8 +168,8 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
         if (t == 0) S.key[0] = nk_lo;
         if (t == EB - 1) S.key[EB + 1] = nk_hi;
         S.mask[t] = 0;
-        S.pint[t] = -1;
-        S.pleaf[t] = -1;
+        S.par[t] = -1;
+        S.par[EB + t] = -1;
         if (t < 3) S.cnt[t] = 0;
         if (t == 0) S.open = 0;
         // this leaf's triangle: to the output soup, and its box (exact-zero components nudged
@@ -248,27 +248,25 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             const int side = is_left ? 0 : 1;
             S.pend[side][0][s] = lo;
             S.pend[side][1][s] = hi;
-            fence_acq_rel_cta();
-            if (atomicOr(&S.mask[s], 1u << side) == 0u) return false;  // first arrival parks
-            fence_acq_rel_cta();
+            if (atom_or_acq_rel_cta(&S.mask[s], 1u << side) == 0u) return false;  // first parks
             const float4 slo = S.pend[side ^ 1][0][s], shi = S.pend[side ^ 1][1][s];
-            const float4 Llo = is_left ? lo : slo, Lhi = is_left ? hi : shi;
-            const float4 Rlo = is_left ? slo : lo, Rhi = is_left ? shi : hi;
-            const uint32_t lpk = __float_as_uint(Lhi.w), rpk = __float_as_uint(Rhi.w);
-            const int L = range_l(lpk), R = range_r(rpk), ndl = range_dl(lpk), ndr = range_dr(rpk);
+            const uint32_t spk = __float_as_uint(shi.w);
+            const int L = is_left ? l : range_l(spk), R = is_left ? range_r(spk) : r;
+            const int ndl = is_left ? dl : range_dl(spk), ndr = is_left ? range_dr(spk) : dr;
             const bool root = (b0 + L == 0) && (b0 + R == n - 1);
             const int P = root ? 0 : (ndr > ndl ? b0 + R : b0 + L);
+            // the record: this child in slot `side`, the sibling in the other (f_1 = 2, f_2 = 0)
             float4 *rc = nodes + 4ull * P;
-            rc[0] = Llo;
-            rc[1] = make_float4(Lhi.x, Lhi.y, Lhi.z, __int_as_float(2));
-            rc[2] = Rlo;
-            rc[3] = make_float4(Rhi.x, Rhi.y, Rhi.z, __int_as_float(0));
-            const int lref = __float_as_int(Llo.w), rref = __float_as_int(Rlo.w);
-            if (lref >= 0) S.pint[lref - b0] = P; else S.pleaf[-(lref + 1) - b0] = P;
-            if (rref >= 0) S.pint[rref - b0] = P; else S.pleaf[-(rref + 1) - b0] = P;
+            rc[2 * side] = lo;
+            rc[2 * side + 1] = make_float4(hi.x, hi.y, hi.z, __int_as_float(2 - 2 * side));
+            rc[2 - 2 * side] = slo;
+            rc[3 - 2 * side] = make_float4(shi.x, shi.y, shi.z, __int_as_float(2 * side));
+            const int mref = __float_as_int(lo.w), sref = __float_as_int(slo.w);
+            S.par[mref >= 0 ? mref - b0 : EB - 1 - b0 - mref] = P;
+            S.par[sref >= 0 ? sref - b0 : EB - 1 - b0 - sref] = P;
             if (root) return false;
-            nlo = make_float4(fminf(Llo.x, Rlo.x), fminf(Llo.y, Rlo.y), fminf(Llo.z, Rlo.z), __int_as_float(P));
-            nhi = make_float4(fmaxf(Lhi.x, Rhi.x), fmaxf(Lhi.y, Rhi.y), fmaxf(Lhi.z, Rhi.z),
+            nlo = make_float4(fminf(lo.x, slo.x), fminf(lo.y, slo.y), fminf(lo.z, slo.z), __int_as_float(P));
+            nhi = make_float4(fmaxf(hi.x, shi.x), fmaxf(hi.y, shi.y), fmaxf(hi.z, shi.z),
                               __uint_as_float(pack_range(L, R, ndl, ndr)));
             return true;
         };
@@ -330,8 +328,8 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
         }
         __syncthreads();
         if (active) {
-            if (S.pint[t] >= 0) parents[k] = S.pint[t];
-            if (S.pleaf[t] >= 0) parents[n + k] = S.pleaf[t];
+            if (S.par[t] >= 0) parents[k] = S.par[t];
+            if (S.par[EB + t] >= 0) parents[n + k] = S.par[EB + t];
         }
         if (t == 0) {
             out_counts[blk] = (uint32_t)min(S.open, kOpenCap);

@@ -71,6 +71,16 @@ __device__ __forceinline__ bool finite3(float4 v) {
 __device__ __forceinline__ void fence_acq_rel_cta() { asm volatile("fence.acq_rel.cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
+// Shared-memory atomic OR with acquire-release semantics at CTA scope: the caller's earlier
+// writes are visible to a thread that later sees its bit, and what the caller reads after it
+// includes the writes of threads whose bits it saw.
+__device__ __forceinline__ uint32_t atom_or_acq_rel_cta(uint32_t *p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.cta.shared.or.b32 %0, [%1], %2;"
+                 : "=r"(old) : "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v) : "memory");
+    return old;
+}
+
 // Relaxed gpu-scope load / store of a 32-bit word another CTA publishes.
 __device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t *p) {
     uint32_t v;
