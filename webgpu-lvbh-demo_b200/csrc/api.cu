@@ -269,11 +269,11 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
     // unsorted keys go to keys_a, so that the three passes ping-pong keys_a -> result ->
     // scratch -> result
     uint32_t *keys_a = ctx->keys_a;
-    launch_morton(tri, n, hb, ctx->ctl, keys_a, ctx->epoch, s);
+    launch_morton(tri, n, hb, ctx->ctl, keys_a, ctx->epoch, ctx->lookback, s);
     if (profile) cudaEventRecord(ctx->ev[3], s);
-    launch_sort_pass(keys_a, nullptr, out->morton, out->leaf_index, n, 0, ctx->ctl, ctx->lookback, s);
-    launch_sort_pass(out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, n, 1, ctx->ctl, ctx->lookback, s);
-    launch_sort_pass(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 2, ctx->ctl, ctx->lookback, s);
+    launch_sort_pass(keys_a, nullptr, out->morton, out->leaf_index, n, 0, true, ctx->ctl, ctx->lookback, s);
+    launch_sort_pass(out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, n, 1, false, ctx->ctl, ctx->lookback, s);
+    launch_sort_pass(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 2, false, ctx->ctl, ctx->lookback, s);
     if (profile) cudaEventRecord(ctx->ev[4], s);
     launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
                 static_cast<float4 *>(out->nodes), out->parents, ctx->items, ctx->counts,

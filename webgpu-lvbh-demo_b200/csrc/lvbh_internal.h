@@ -26,6 +26,16 @@ constexpr int kSortTile = kSortThreads * kSortItems; // keys per tile (4096)
 
 __host__ __device__ inline uint32_t sort_tiles(uint32_t n) { return (n + kSortTile - 1) / kSortTile; }
 
+// The plain build's sort scratch: per tile of kSortTile keys its kDigits counts of the pass's
+// digit, per chunk of kSortChunkTiles tiles their sum, per chunk the output offsets.
+constexpr int kSortChunkTiles = 8;
+__host__ __device__ inline uint32_t sort_chunks(uint32_t n) {
+    return (sort_tiles(n) + kSortChunkTiles - 1) / kSortChunkTiles;
+}
+inline uint32_t *sort_chunk_sums(uint32_t *scratch, uint32_t n) {
+    return scratch + (size_t)sort_tiles(n) * kDigits;
+}
+
 // Tree/refit pass: leaves per block of the in-block tree pass (one thread each); open nodes a
 // block can leave to the straddling pass (at most 2 x the tree depth 64).
 constexpr int kEmitBlock = 256;
@@ -82,17 +92,19 @@ size_t ctx_device_bytes(const lvbh_ctx *ctx);
 
 // K1a: scene box over every vertex of the 48-byte triangle soup.
 void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s);
-// K1b: triangle box centroid -> Morton key (input order) + the four digit histograms; flags
+// K1b: triangle box centroid -> Morton key (input order), the global digit counts of all
+// three sort passes and the first pass's tile histograms and chunk sums (sort_scratch); flags
 // non-finite vertices in ctl->err and advances the build epoch *epoch used by K3c.
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl,
-                   uint32_t *keys_out, uint32_t *epoch, cudaStream_t s);
-// K2: one reduce-then-scan pass over 10-bit digit `pass` (0..2) of 30-bit keys (three
-// launches; the global digit counts come from ctl->hist).  vals_in == nullptr generates the
+                   uint32_t *keys_out, uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s);
+// K2: one reduce-then-scan pass over 10-bit digit `pass` (0..2) of 30-bit keys (the global
+// digit counts come from ctl->hist).  counted: the tile histograms and chunk sums of this
+// pass are already in scratch (K1b writes those of pass 0).  vals_in == nullptr generates the
 // identity.  scratch: sort_scratch_words(n) words, no initialisation needed.
 size_t sort_scratch_words(uint32_t n);
 void launch_sort_pass(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
-                      uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *scratch,
-                      cudaStream_t s);
+                      uint32_t *vals_out, uint32_t n, int pass, bool counted, Control *ctl,
+                      uint32_t *scratch, cudaStream_t s);
 // The same over 8-bit digit `pass` (0..3) of full 32-bit keys (counts in ctl->hist pass-major,
 // 256 per pass; look-back words kSortPasses32 * sort_tiles(n) * kDigits32).
 void launch_onesweep32(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,

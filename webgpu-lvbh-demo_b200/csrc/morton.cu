@@ -68,18 +68,26 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const float4 *__restrict__ 
     }
 }
 
-// K1b: per triangle box, centroid, quantisation and 30-bit Morton key, written in input order;
-// the digit histograms of all four sort passes are accumulated on the way.
+// K1b: per triangle box, centroid, quantisation and 30-bit Morton key, written in input order.
+// One block per chunk of kSortChunkTiles sort tiles: per tile each warp takes chunks of 32
+// triangles (96 consecutive float4, three coalesced 512-byte loads, transposed through shared
+// memory so that each lane owns a triangle); the digit counts of all three sort passes
+// accumulate over the block, and the counts of the first pass's digit per tile and per chunk
+// go straight to the sort's scratch, so the first sort pass starts from them.
 __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ tri, uint32_t n,
                                                      HostBounds hb, Control *__restrict__ ctl,
                                                      uint32_t *__restrict__ keys,
-                                                     uint32_t *__restrict__ epoch) {
+                                                     uint32_t *__restrict__ epoch,
+                                                     uint32_t *__restrict__ tile_hist,
+                                                     uint32_t *__restrict__ chunk_sum) {
+    constexpr int P = kDigits / kThreads;  // digits per thread in the per-tile counts
     __shared__ float4 stage[kWarps][96];
+    __shared__ uint32_t hist[kSortPasses][kDigits];
+    __shared__ uint32_t th[kDigits];
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
         const uint32_t e = *epoch + 1u;
         *epoch = e == 0u ? 1u : e;
     }
-    __shared__ uint32_t hist[kSortPasses][kDigits];
     for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) (&hist[0][0])[i] = 0;
 
     float umin[3], umax[3];
@@ -93,37 +101,59 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
             umax[a] = ord_lo_inv(ctl->bounds_ord[3 + a]);
         }
     }
-    __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t nv = 3ull * n;
-    const uint32_t chunks = (n + 31) / 32;
-    const uint32_t warps_total = gridDim.x * kWarps;
+    const uint32_t tiles = sort_tiles(n);
+    uint32_t acc[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) acc[j] = 0;
     bool bad = false;
-    for (uint32_t c = blockIdx.x * kWarps + warp; c < chunks; c += warps_total) {
-        const uint64_t base = 96ull * c;
+    for (int tt = 0; tt < kSortChunkTiles; ++tt) {
+        const uint32_t tile = blockIdx.x * kSortChunkTiles + tt;
+        if (tile >= tiles) break;  // uniform across the block
+        for (int i = threadIdx.x; i < kDigits; i += kThreads) th[i] = 0;
+        __syncthreads();
+        for (uint32_t c = warp; c < (uint32_t)kSortTile / 32; c += kWarps) {
+            const uint32_t t0 = tile * (uint32_t)kSortTile + 32u * c;
+            if (t0 >= n) break;
+            const uint64_t base = 3ull * t0;
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            const uint64_t e = base + 32 * r + lane;
-            stage[warp][32 * r + lane] = e < nv ? ld_stream(tri + e) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        __syncwarp();
-        const float4 v0 = stage[warp][3 * lane], v1 = stage[warp][3 * lane + 1],
-                     v2 = stage[warp][3 * lane + 2];
-        __syncwarp();
-        const uint32_t t = 32u * c + lane;
-        if (t < n) {
-            bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
-            // box.min = min(v0, min(v1, v2)); box.max = max(v0, max(v1, v2))   (:186-187)
-            const uint32_t qx = quantise(fminf(v0.x, fminf(v1.x, v2.x)), fmaxf(v0.x, fmaxf(v1.x, v2.x)), umin[0], umax[0]);
-            const uint32_t qy = quantise(fminf(v0.y, fminf(v1.y, v2.y)), fmaxf(v0.y, fmaxf(v1.y, v2.y)), umin[1], umax[1]);
-            const uint32_t qz = quantise(fminf(v0.z, fminf(v1.z, v2.z)), fmaxf(v0.z, fmaxf(v1.z, v2.z)), umin[2], umax[2]);
-            const uint32_t key = morton3(qx, qy, qz);
-            keys[t] = key;
+            for (int r = 0; r < 3; ++r) {
+                const uint64_t e = base + 32 * r + lane;
+                stage[warp][32 * r + lane] = e < nv ? ld_stream(tri + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            __syncwarp();
+            const float4 v0 = stage[warp][3 * lane], v1 = stage[warp][3 * lane + 1],
+                         v2 = stage[warp][3 * lane + 2];
+            __syncwarp();
+            const uint32_t t = t0 + lane;
+            if (t < n) {
+                bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
+                // box.min = min(v0, min(v1, v2)); box.max = max(v0, max(v1, v2))   (:186-187)
+                const uint32_t qx = quantise(fminf(v0.x, fminf(v1.x, v2.x)), fmaxf(v0.x, fmaxf(v1.x, v2.x)), umin[0], umax[0]);
+                const uint32_t qy = quantise(fminf(v0.y, fminf(v1.y, v2.y)), fmaxf(v0.y, fmaxf(v1.y, v2.y)), umin[1], umax[1]);
+                const uint32_t qz = quantise(fminf(v0.z, fminf(v1.z, v2.z)), fmaxf(v0.z, fmaxf(v1.z, v2.z)), umin[2], umax[2]);
+                const uint32_t key = morton3(qx, qy, qz);
+                keys[t] = key;
 #pragma unroll
-            for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (kDigitBits * p)) & (kDigits - 1)], 1u);
+                for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (kDigitBits * p)) & (kDigits - 1)], 1u);
+                atomicAdd(&th[key & (kDigits - 1)], 1u);
+            }
         }
+        __syncthreads();
+        uint32_t *row = tile_hist + (size_t)tile * kDigits + threadIdx.x * P;
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            const uint32_t c = th[threadIdx.x * P + j];
+            row[j] = c;
+            acc[j] += c;
+        }
+        __syncthreads();
     }
+    uint32_t *crow = chunk_sum + (size_t)blockIdx.x * kDigits + threadIdx.x * P;
+#pragma unroll
+    for (int j = 0; j < P; ++j) crow[j] = acc[j];
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
     __syncthreads();
     for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) {
@@ -285,13 +315,10 @@ void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s) 
 }
 
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl, uint32_t *keys,
-                   uint32_t *epoch, cudaStream_t s) {
-    const uint64_t chunks = (n + 31) / 32;
-    uint64_t blocks = (chunks + kWarps - 1) / kWarps;
-    const uint64_t cap = (uint64_t)sm_count() * 8;
-    if (blocks > cap) blocks = cap;
-    if (blocks == 0) blocks = 1;
-    k_morton<<<(unsigned)blocks, kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch);
+                   uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
+    if (n == 0) return;
+    k_morton<<<sort_chunks(n), kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch, sort_scratch,
+                                                 sort_chunk_sums(sort_scratch, n));
 }
 
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,

@@ -293,9 +293,7 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
     if (oob) atomicOr(&ctl->err, ERR_LOOKBACK_TIMEOUT);
 }
 
-constexpr int kChunkTiles = 8;  // tiles per chunk of the reduce-then-scan pass
-
-inline uint32_t sort_chunks(uint32_t n) { return (sort_tiles(n) + kChunkTiles - 1) / kChunkTiles; }
+constexpr int kChunkTiles = kSortChunkTiles;
 
 // Reduce: digit counts of every tile (tile_hist[tile][digit]) and of every chunk of kChunkTiles
 // tiles (chunk_sum[chunk][digit]).  One block per chunk; each thread owns P contiguous digits.
@@ -341,29 +339,34 @@ __global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ ke
 
 // Scan: chunk_off[c][d] = start of digit d in the pass's output (exclusive scan of the global
 // counts ghist over digits) + counts of digit d in chunks before c.  Block b covers digits
-// 32b .. 32b+31 (lane = digit); its 8 warps split the chunks.
+// 32b .. 32b+31 (lane = digit); its 32 warps split the chunks.
+constexpr int kScanThreads = 1024;
 template <int BITS>
-__global__ void __launch_bounds__(T) k_chunk_scan(const uint32_t *__restrict__ chunk_sum, uint32_t chunks,
-                                                  const uint32_t *__restrict__ ghist,
-                                                  uint32_t *__restrict__ chunk_off) {
-    constexpr int D = 1 << BITS, P = D / T;
-    __shared__ uint32_t s_warp[W];
+__global__ void __launch_bounds__(kScanThreads) k_chunk_scan(const uint32_t *__restrict__ chunk_sum,
+                                                             uint32_t chunks,
+                                                             const uint32_t *__restrict__ ghist,
+                                                             uint32_t *__restrict__ chunk_off) {
+    constexpr int D = 1 << BITS, SW = kScanThreads / 32;
+    static_assert(D == kScanThreads, "one digit per thread in the digit scan");
+    __shared__ uint32_t s_wsum[SW];
     __shared__ uint32_t s_base[32];
-    __shared__ uint32_t s_part[W][32];
+    __shared__ uint32_t s_part[SW][32];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // digit starts: exclusive scan of the global counts (thread tid holds digits tid*P..)
-    uint32_t g[P], gs = 0;
+    // digit starts: exclusive scan of the global counts, one digit per thread
+    const uint32_t g = __ldg(ghist + tid);
+    uint32_t incl = g;
 #pragma unroll
-    for (int j = 0; j < P; ++j) { g[j] = __ldg(ghist + tid * P + j); gs += g[j]; }
-    uint32_t run = block_exclusive_scan(gs, s_warp);
-    const int d0 = blockIdx.x * 32;
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-        const int dg = tid * P + j;
-        if (dg >= d0 && dg < d0 + 32) s_base[dg - d0] = run;
-        run += g[j];
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
     }
-    const uint32_t per = (chunks + W - 1) / W;
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    uint32_t woff = 0;
+    for (int w = 0; w < warp; ++w) woff += s_wsum[w];
+    const int d0 = blockIdx.x * 32;
+    if (tid >= d0 && tid < d0 + 32) s_base[tid - d0] = woff + incl - g;
+    const uint32_t per = (chunks + SW - 1) / SW;
     const uint32_t c0 = warp * per, c1 = min(chunks, c0 + per);
     const int d = d0 + lane;
     uint32_t sum = 0;
@@ -523,15 +526,16 @@ cudaError_t sort_init() {
 size_t sort_scratch_words(uint32_t n) { return ((size_t)sort_tiles(n) + 2ull * sort_chunks(n)) * kDigits; }
 
 void launch_sort_pass(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
-                      uint32_t *vals_out, uint32_t n, int pass, Control *ctl, uint32_t *scratch,
-                      cudaStream_t s) {
+                      uint32_t *vals_out, uint32_t n, int pass, bool counted, Control *ctl,
+                      uint32_t *scratch, cudaStream_t s) {
     if (n == 0) return;
     const uint32_t tiles = sort_tiles(n), chunks = sort_chunks(n);
     uint32_t *tile_hist = scratch;
-    uint32_t *chunk_sum = tile_hist + (size_t)tiles * kDigits;
+    uint32_t *chunk_sum = sort_chunk_sums(scratch, n);
     uint32_t *chunk_off = chunk_sum + (size_t)chunks * kDigits;
-    k_tile_hist<kDigitBits><<<chunks, T, 0, s>>>(keys_in, n, pass, tile_hist, chunk_sum);
-    k_chunk_scan<kDigitBits><<<kDigits / 32, T, 0, s>>>(chunk_sum, chunks, ctl->hist + pass * kDigits, chunk_off);
+    if (!counted) k_tile_hist<kDigitBits><<<chunks, T, 0, s>>>(keys_in, n, pass, tile_hist, chunk_sum);
+    k_chunk_scan<kDigitBits><<<kDigits / 32, kScanThreads, 0, s>>>(chunk_sum, chunks,
+                                                                   ctl->hist + pass * kDigits, chunk_off);
     k_scatter<kDigitBits><<<tiles, T, sizeof(SortSmem<kDigitBits>), s>>>(
         keys_in, vals_in, keys_out, vals_out, n, pass, tile_hist, chunk_off, ctl);
 }
