@@ -383,10 +383,11 @@ def run_batched(args, world, rank, local, clocks=None):
 
     def batched(profile=False, sync=False, graph=True, o=outs):
         return builder.build_batched(dtri, offs, outputs=o, stream=stream, sync=sync,
-                                     profile=profile, graph=graph)
+                                     profile=profile, graph=graph, autotune=True)
 
-    for _ in range(args.warmup):
+    for _ in range(args.warmup):  # the first build of this size histogram tunes
         batched(sync=True)
+    tuned = builder.tunables()
     torch.cuda.synchronize(dev)
     barrier(world)
     ev0.record(stream)
@@ -466,7 +467,10 @@ def run_batched(args, world, rank, local, clocks=None):
             "mprims_per_s": world * n / (ms * 1e-3) / 1e6,
             "per_mesh_loop_ms": loop, "per_mesh_builds_per_s": world * count / (base_ms * 1e-3),
             "speedup_vs_per_mesh": base_ms / ms, "identical_trees": bool(identical),
-            "stage_ms": stage_ms, "launches_per_batch": 11,
+            "stage_ms": stage_ms, "launches_per_batch": 11 if tuned["digit_bits"] == 10 else 12,
+            "tunables": {"chosen": {k: tuned[k] for k in ("digit_bits", "tree_block")},
+                         "candidates_ms": dict(zip(["10-bit/256", "10-bit/128", "8-bit/256", "8-bit/128"],
+                                                   tuned["candidates_ms"]))},
             "e2e": {"value": world * n / (e2e * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": e2e,
                     "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 64 * int(root_idx.numel())},
             "generate_s": round(t_gen, 1)}

@@ -73,6 +73,8 @@ extern "C" {
 #define LVBH_OUT_CALLER    0x4u  /* result pointers in *out are caller-owned device buffers to fill */
 #define LVBH_PROFILE       0x8u  /* record per-stage CUDA events; read them with lvbh_stage_times() */
 #define LVBH_NO_GRAPH      0x10u /* launch stage by stage instead of replaying a cached CUDA graph */
+#define LVBH_AUTOTUNE      0x20u /* lvbh_build_batched: pick the tunables by timing the candidates
+                                    on the first batch of each mesh-size histogram (cached) */
 
 /* Largest triangle count one build accepts (2^29: keeps every index sum of the tree search
  * inside int32 and the look-back counts inside their 30-bit field; a build this size needs
@@ -83,9 +85,9 @@ extern "C" {
 #define LVBH_STAGE_UPLOAD  0  /* host->device copy of the input (LVBH_INPUT_HOST only) */
 #define LVBH_STAGE_BOUNDS  1  /* scene box reduction (skipped when bounds are supplied) */
 #define LVBH_STAGE_MORTON  2  /* triangle centroid -> 30-bit Morton key + digit histograms */
-#define LVBH_STAGE_SORT    3  /* onesweep stable radix sort of (key, triangle index) */
-#define LVBH_STAGE_GATHER  4  /* leaf gather: sorted triangle rearrange + leaf boxes */
-#define LVBH_STAGE_TREE    5  /* radix tree + box refit of every node inside a 256-leaf block */
+#define LVBH_STAGE_SORT    3  /* stable LSD radix sort of (key, triangle index) */
+#define LVBH_STAGE_GATHER  4  /* empty: the leaf gather runs inside the tree stage */
+#define LVBH_STAGE_TREE    5  /* leaf gather + rearrange, radix tree + box refit inside each block */
 #define LVBH_STAGE_TOP     6  /* radix tree + box refit of the nodes that straddle blocks */
 #define LVBH_NUM_STAGES    7
 
@@ -160,6 +162,27 @@ LVBH_API int  lvbh_build_indexed(lvbh_ctx *ctx, const float *xyz, uint32_t num_v
 LVBH_API int  lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *seg_offsets,
                         uint32_t num_segs, const float *seg_bounds, float *bounds_out,
                         uint32_t flags, lvbh_result *out, void *stream);
+
+/* Tunables of batched builds (no counterpart in the reference, whose kernels hard-code
+ * WG_SIZE = 64 and 2-bit digits).  With LVBH_AUTOTUNE, lvbh_build_batched keys the meshes'
+ * size histogram (per power-of-two size class, the bit length of the number of meshes in it),
+ * and on the first batch with a new key times each candidate - digit width {10, 8} x tree block
+ * {256, 128} - on that batch itself, then builds every batch with that key with the fastest.
+ * Without it the defaults are used (10-bit digits, 256-leaf blocks).  Every choice gives the
+ * same result words. */
+typedef struct lvbh_tunables {
+    uint32_t digit_bits;        /* radix sort digit width: 10 (three passes) or 8 (four passes) */
+    uint32_t tree_block;        /* sorted leaves per tree block: 256 or 128 */
+    uint32_t tree_ctas_per_sm;  /* tree-pass CTAs per SM (persistent grid); 0 = as many as fit */
+    uint32_t reserved;
+} lvbh_tunables;
+/* Forces the tunables of later batched builds on this context; NULL returns to LVBH_AUTOTUNE /
+ * defaults. */
+LVBH_API int  lvbh_set_tunables(lvbh_ctx *ctx, const lvbh_tunables *t);
+/* The tunables of the context's last batched build and, when that build tuned, the times of
+ * the candidates (ms, up to 4, in the order listed above; *num_candidates = 0 otherwise). */
+LVBH_API int  lvbh_get_tunables(lvbh_ctx *ctx, lvbh_tunables *t, float *candidate_ms,
+                                uint32_t *num_candidates);
 
 /* Waits for the context's last build and returns its device-side status (LVBH_OK,
  * LVBH_EINVAL for non-finite vertices, LVBH_ETIMEOUT, LVBH_EDEVICE).  Fills out->bounds

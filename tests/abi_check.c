@@ -28,6 +28,9 @@ int main(void) {
     printf("scratch_1M %zu\n", lvbh_scratch_bytes(1u << 20));
     printf("batched_null_ctx %d\n", lvbh_build_batched(NULL, NULL, NULL, 0, NULL, NULL, 0, &r, NULL));
     printf("sizeof_server_config %zu\n", sizeof(lvbh_server_config));
+    printf("sizeof_tunables %zu\n", sizeof(lvbh_tunables));
+    printf("set_tunables_null %d\n", lvbh_set_tunables(NULL, NULL));
+    printf("get_tunables_null %d\n", lvbh_get_tunables(NULL, NULL, NULL, NULL));
     printf("sizeof_request_info %zu\n", sizeof(lvbh_request_info));
     printf("off_latency %zu\n", offsetof(lvbh_request_info, latency_ms));
     printf("sizeof_server_stats %zu\n", sizeof(lvbh_server_stats));

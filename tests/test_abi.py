@@ -51,13 +51,15 @@ def test_c_header_layout_and_host_errors(tmp_path):
     assert int(kv["sizeof_config"]) == ctypes.sizeof(nat.Config)
     assert "sm_100a" in kv["version"]
     assert int(kv["sizeof_server_config"]) == ctypes.sizeof(nat.ServerConfig)
+    assert int(kv["sizeof_tunables"]) == ctypes.sizeof(nat.Tunables) == 16
     assert int(kv["sizeof_request_info"]) == ctypes.sizeof(nat.RequestInfo)
     assert int(kv["off_latency"]) == nat.RequestInfo.latency_ms.offset
     assert int(kv["sizeof_server_stats"]) == ctypes.sizeof(nat.ServerStats)
     assert int(kv["off_max_batch_seen"]) == nat.ServerStats.max_batch_seen.offset
     for k in ("build_null_ctx", "indexed_null_ctx", "sync_null", "release_null", "create_null",
               "stage_null", "trace_null", "copy_null", "batched_null_ctx", "server_create_null",
-              "submit_null", "poll_null", "wait_null", "release_req_null", "stats_null"):
+              "submit_null", "poll_null", "wait_null", "release_req_null", "stats_null",
+              "set_tunables_null", "get_tunables_null"):
         assert int(kv[k]) == nat.EINVAL, k
     assert kv["server_error_null"] == "no server"
     assert kv["last_error_null"] == "no context"

@@ -141,3 +141,36 @@ def test_batched_empty(builder):
     res = builder.build_batched(torch.zeros((0, 12), dtype=torch.float32, device="cuda"), [0, 0, 0])
     assert res.nodes.shape[0] == 0
     np.testing.assert_array_equal(res.seg_bounds, np.zeros((2, 6), np.float32))
+
+
+@pytest.mark.parametrize("digit_bits,tree_block", [(10, 256), (10, 128), (8, 256), (8, 128)])
+def test_batched_every_tunable_choice_is_identical(builder, digit_bits, tree_block):
+    import torch
+    tri, offs = make_batch(EDGE_SIZES, seed=31)
+    builder.set_tunables(digit_bits=digit_bits, tree_block=tree_block)
+    try:
+        res = builder.build_batched(torch.from_numpy(tri).cuda(), offs)
+        t = builder.tunables()
+        assert (t["digit_bits"], t["tree_block"]) == (digit_bits, tree_block)
+    finally:
+        builder.set_tunables()
+    check_against_plain(builder, tri, offs, res)
+
+
+def test_autotune_times_candidates_and_caches(builder):
+    import torch
+    from lvbh import scenes
+    tri, offs = scenes.mesh_batch(count=96, seed=8)
+    t = torch.from_numpy(tri).cuda()
+    r1 = builder.build_batched(t, offs, autotune=True)
+    first = builder.tunables()
+    assert len(first["candidates_ms"]) == 4 and min(first["candidates_ms"]) > 0
+    cands = [(10, 256), (10, 128), (8, 256), (8, 128)]
+    best = cands[int(np.argmin(first["candidates_ms"]))]
+    assert (first["digit_bits"], first["tree_block"]) == best
+    r2 = builder.build_batched(t, offs, autotune=True)  # same histogram: cached, not re-timed
+    again = builder.tunables()
+    assert again == first
+    for f in FIELDS:
+        assert torch.equal(getattr(r1, f), getattr(r2, f)), f
+    check_against_plain(builder, tri, offs, r2)

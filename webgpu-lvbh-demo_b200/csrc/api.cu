@@ -8,6 +8,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 
 #include "lvbh.h"
@@ -60,10 +61,29 @@ struct GraphKey {
     bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
 
+// Tunables of a batched build and the histogram key the tuner caches them under: per
+// power-of-two size class of the meshes, the bit length of the number of meshes in it.
+struct Tunables {
+    int digit_bits = kDigitBits;
+    int log_block = kLogEmitBlock;
+    int tree_ctas = 0;
+};
+struct TuneKey {
+    uint8_t cls[33] = {};
+    bool operator<(const TuneKey &o) const { return std::memcmp(cls, o.cls, sizeof cls) < 0; }
+};
+struct Tuned {
+    Tunables t;
+    float ms[4] = {0.f, 0.f, 0.f, 0.f};  // the candidates' times (0 = not timed)
+    uint32_t candidates = 0;
+};
+constexpr Tunables kCandidates[4] = {{kDigitBits, 8, 0}, {kDigitBits, 7, 0}, {kDigitBits32, 8, 0},
+                                     {kDigitBits32, 7, 0}};
+
 struct BatchKey {
     const void *tri = nullptr;
     uint32_t total = 0, num_segs = 0, tiles = 0, blocks = 0;
-    int use_bounds = 0;
+    int use_bounds = 0, digit_bits = 0, log_block = 0, tree_ctas = 0;
     void *outs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     bool operator==(const BatchKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
@@ -113,6 +133,11 @@ struct lvbh_ctx {
     uint32_t *bh_ord = nullptr;
     BatchKey bkey;
     cudaGraphExec_t bgexec = nullptr;
+    // batched-build tunables: forced by the caller, or tuned per segment-size histogram
+    bool forced = false;
+    Tunables forced_t;
+    std::map<TuneKey, Tuned> tuned;
+    Tuned last_tuned;
     // last build, for lvbh_sync
     cudaStream_t last_stream = nullptr;
     lvbh_result *last_out = nullptr;
@@ -180,7 +205,7 @@ int ensure_batch(lvbh_ctx *ctx, uint32_t segs, uint32_t tiles, uint32_t blocks) 
     blocks = blocks > ctx->b_blocks ? blocks : ctx->b_blocks;
     free_batch(ctx);
     const size_t rows = align_up((segs + 1ull) * sizeof(SegRow));
-    const size_t ord = (size_t)segs * 6 * 4, hist = (size_t)segs * kSortPasses * kDigits * 4;
+    const size_t ord = (size_t)segs * 6 * 4, hist = (size_t)segs * kHistWords * 4;
     const size_t lb = (size_t)kSortPasses * tiles * kDigits * 4;
     const size_t zero = align_up(ord + hist + lb);
     const size_t bnd = align_up((size_t)segs * 6 * 4);
@@ -200,7 +225,7 @@ int ensure_batch(lvbh_ctx *ctx, uint32_t segs, uint32_t tiles, uint32_t blocks) 
     ctx->b_zero = reinterpret_cast<uint32_t *>(c);
     ctx->b_ord = ctx->b_zero;
     ctx->b_hist = ctx->b_ord + (size_t)segs * 6;
-    ctx->b_lookback = ctx->b_hist + (size_t)segs * kSortPasses * kDigits;
+    ctx->b_lookback = ctx->b_hist + (size_t)segs * kHistWords;
     c += zero;
     ctx->b_bounds = reinterpret_cast<float *>(c); c += bnd;
     ctx->b_items = reinterpret_cast<OpenItem *>(c); c += align_up((size_t)blocks * kOpenCap * sizeof(OpenItem));
@@ -293,7 +318,9 @@ void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool u
                         cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(reinterpret_cast<char *>(ctx->ctl) + offsetof(Control, err), 0,
                     sizeof(Control) - offsetof(Control, err), s);
-    const uint32_t *zero_end = ctx->b_lookback + (size_t)kSortPasses * bp.tiles * kDigits;
+    const bool wide = bp.digit_bits == kDigitBits;
+    const size_t lb_words = wide ? (size_t)kSortPasses * kDigits : (size_t)kSortPasses32 * kDigits32;
+    const uint32_t *zero_end = ctx->b_lookback + lb_words * bp.tiles;
     cudaMemsetAsync(ctx->b_zero, 0, (zero_end - ctx->b_zero) * sizeof(uint32_t), s);
     launch_seg_tables(ctx->b_rows, bp.num_segs, ctx->b_tile_seg, ctx->b_blk_seg, s);
     launch_bounds_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, s);
@@ -302,9 +329,18 @@ void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool u
     launch_morton_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, ctx->b_hist,
                         ctx->ctl, keys_a, ctx->epoch, s);
     if (profile) cudaEventRecord(ctx->ev[3], s);
-    launch_onesweep_batch(bp, keys_a, nullptr, out->morton, out->leaf_index, 0, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
-    launch_onesweep_batch(bp, out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, 1, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
-    launch_onesweep_batch(bp, ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, 2, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    // ping-pong so that the last pass lands in the result buffers
+    uint32_t *kb = ctx->keys_b, *vb = ctx->vals_b, *ko = out->morton, *vo = out->leaf_index;
+    if (wide) {
+        launch_onesweep_batch(bp, keys_a, nullptr, ko, vo, 0, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+        launch_onesweep_batch(bp, ko, vo, kb, vb, 1, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+        launch_onesweep_batch(bp, kb, vb, ko, vo, 2, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    } else {
+        launch_onesweep_batch(bp, keys_a, nullptr, kb, vb, 0, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+        launch_onesweep_batch(bp, kb, vb, ko, vo, 1, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+        launch_onesweep_batch(bp, ko, vo, kb, vb, 2, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+        launch_onesweep_batch(bp, kb, vb, ko, vo, 3, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
+    }
     if (profile) cudaEventRecord(ctx->ev[4], s);
     launch_emit_batch(bp, tri, out->leaf_index, out->morton, static_cast<float4 *>(out->tris),
                       static_cast<float4 *>(out->nodes), out->parents, ctx->b_items,
@@ -322,6 +358,9 @@ int launch_batch_graph(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bo
     key.tiles = bp.tiles;
     key.blocks = bp.blocks;
     key.use_bounds = use_bounds;
+    key.digit_bits = bp.digit_bits;
+    key.log_block = bp.log_block;
+    key.tree_ctas = bp.tree_ctas_per_sm;
     key.outs[0] = out->nodes; key.outs[1] = out->tris; key.outs[2] = out->parents;
     key.outs[3] = out->leaf_index; key.outs[4] = out->morton;
     if (!ctx->bgexec || !(key == ctx->bkey)) {
@@ -477,7 +516,7 @@ size_t ctx_device_bytes(const lvbh_ctx *ctx) {
     size_t batch = 0;
     if (ctx->b_dev) {
         batch = align_up((segs + 1ull) * sizeof(SegRow)) + align_up(tiles * 4ull) + align_up(blocks * 4ull) +
-                align_up((size_t)segs * 6 * 4 + (size_t)segs * kSortPasses * kDigits * 4 +
+                align_up((size_t)segs * 6 * 4 + (size_t)segs * kHistWords * 4 +
                          (size_t)kSortPasses * tiles * kDigits * 4) +
                 align_up((size_t)segs * 6 * 4) + align_up((size_t)blocks * kOpenCap * sizeof(OpenItem)) +
                 align_up(blocks * 4ull);
@@ -608,13 +647,17 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
     if (num_segs && !seg_offsets) return fail(ctx, LVBH_EINVAL, "seg_offsets is NULL");
     if (num_segs > (1u << 24)) return fail(ctx, LVBH_EINVAL, "num_segs exceeds 2^24");
     if (num_segs && seg_offsets[0] != 0) return fail(ctx, LVBH_EINVAL, "seg_offsets[0] must be 0");
-    uint64_t tiles = 0, blocks = 0;
+    uint64_t tiles = 0, blocks128 = 0;
+    TuneKey tkey;
     for (uint32_t i = 0; i < num_segs; ++i) {
         if (seg_offsets[i + 1] < seg_offsets[i]) return fail(ctx, LVBH_EINVAL, "seg_offsets must be non-decreasing");
         const uint32_t n = seg_offsets[i + 1] - seg_offsets[i];
         tiles += sort_tiles(n);
-        blocks += emit_groups(n);
+        blocks128 += emit_groups(n, 7);
+        const int c = n ? 32 - __builtin_clz(n) : 0;  // size class: bit length of n
+        if (tkey.cls[c] < 255) ++tkey.cls[c];
     }
+    for (uint8_t &v : tkey.cls) v = v ? (uint8_t)(32 - __builtin_clz(v)) : 0;
     const uint32_t total = num_segs ? seg_offsets[num_segs] : 0;
     if (total > LVBH_MAX_TRIS) return fail(ctx, LVBH_EINVAL, "total triangles exceed LVBH_MAX_TRIS");
     if (total && !tri_array) return fail(ctx, LVBH_EINVAL, "tri_array is NULL");
@@ -631,21 +674,24 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
         return LVBH_OK;
     }
     if (int rc = ensure_arena(ctx, total)) return rc;
-    if (int rc = ensure_batch(ctx, num_segs, (uint32_t)tiles, (uint32_t)blocks)) return rc;
+    if (int rc = ensure_batch(ctx, num_segs, (uint32_t)tiles, (uint32_t)blocks128)) return rc;
     if (ctx->pending) lvbh_sync(ctx);  // the pinned mirror may still be read by the previous build
-    // segment table: first triangle, first sort tile, first tree block per segment
-    uint32_t tile = 0, blk = 0;
-    for (uint32_t i = 0; i <= num_segs; ++i) {
-        ctx->bh_rows[i] = SegRow{seg_offsets[i], tile, blk, 0u};
-        if (i < num_segs) {
-            const uint32_t n = seg_offsets[i + 1] - seg_offsets[i];
-            tile += sort_tiles(n);
-            blk += (uint32_t)emit_groups(n);
-        }
-    }
     if (seg_bounds) std::memcpy(ctx->bh_bounds, seg_bounds, num_segs * 6ull * sizeof(float));
-    const BatchPlan bp{ctx->b_rows, ctx->b_tile_seg, ctx->b_blk_seg, num_segs, (uint32_t)tiles,
-                       (uint32_t)blocks, total};
+    // segment table for tree blocks of 2^log_block leaves: first triangle, first sort tile and
+    // first tree block per segment
+    auto plan = [&](const Tunables &t) {
+        uint32_t tile = 0, blk = 0;
+        for (uint32_t i = 0; i <= num_segs; ++i) {
+            ctx->bh_rows[i] = SegRow{seg_offsets[i], tile, blk, 0u};
+            if (i < num_segs) {
+                const uint32_t n = seg_offsets[i + 1] - seg_offsets[i];
+                tile += sort_tiles(n);
+                blk += (uint32_t)emit_groups(n, t.log_block);
+            }
+        }
+        return BatchPlan{ctx->b_rows, ctx->b_tile_seg, ctx->b_blk_seg, num_segs, (uint32_t)tiles,
+                         blk, total, t.digit_bits, t.log_block, t.tree_ctas};
+    };
     LVBH_CUDA(ctx, cudaMemsetAsync(&ctx->ctl->aux_err, 0, sizeof(uint32_t), s));
     const float4 *tri = reinterpret_cast<const float4 *>(tri_array);
     const bool profile = (flags & LVBH_PROFILE) != 0;
@@ -657,6 +703,38 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
     } else if (reinterpret_cast<uintptr_t>(tri_array) & 15u) {
         return fail(ctx, LVBH_EINVAL, "device tri_array must be 16-byte aligned");
     }
+    // the tunables: forced, tuned before for this size histogram, tuned now, or the defaults
+    Tuned choice;
+    if (ctx->forced) {
+        choice.t = ctx->forced_t;
+    } else if (flags & LVBH_AUTOTUNE) {
+        auto it = ctx->tuned.find(tkey);
+        if (it != ctx->tuned.end()) {
+            choice = it->second;
+        } else {
+            // time every candidate (second of two runs, stage by stage) on this very batch
+            cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[LVBH_NUM_STAGES];
+            float best = 0.f;
+            for (uint32_t c = 0; c < 4; ++c) {
+                const BatchPlan cp = plan(kCandidates[c]);
+                float ms = 0.f;
+                for (int rep = 0; rep < 2; ++rep) {
+                    LVBH_CUDA(ctx, cudaEventRecord(e0, s));
+                    enqueue_batch(ctx, tri, cp, seg_bounds != nullptr, out, s, false);
+                    LVBH_CUDA(ctx, cudaEventRecord(e1, s));
+                    LVBH_CUDA(ctx, cudaEventSynchronize(e1));
+                    LVBH_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+                }
+                choice.ms[c] = ms;
+                if (c == 0 || ms < best) { best = ms; choice.t = kCandidates[c]; }
+            }
+            choice.candidates = 4;
+            ctx->tuned[tkey] = choice;
+            if (profile) cudaEventRecord(ctx->ev[0], s);
+        }
+    }
+    ctx->last_tuned = choice;
+    const BatchPlan bp = plan(choice.t);
     if (profile || (flags & LVBH_NO_GRAPH)) {
         enqueue_batch(ctx, tri, bp, seg_bounds != nullptr, out, s, profile);
         cudaError_t e = cudaGetLastError();
@@ -680,6 +758,32 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
     ctx->pending = true;
     if (flags & LVBH_ASYNC) return LVBH_OK;
     return lvbh_sync(ctx);
+}
+
+int lvbh_set_tunables(lvbh_ctx *ctx, const lvbh_tunables *t) {
+    if (!ctx) return LVBH_EINVAL;
+    if (!t) {
+        ctx->forced = false;
+        return LVBH_OK;
+    }
+    if ((t->digit_bits != 8 && t->digit_bits != 10) || (t->tree_block != 128 && t->tree_block != 256) ||
+        t->tree_ctas_per_sm > 8)
+        return fail(ctx, LVBH_EINVAL, "tunables: digit_bits 8 or 10, tree_block 128 or 256, tree_ctas_per_sm <= 8");
+    ctx->forced = true;
+    ctx->forced_t = Tunables{(int)t->digit_bits, t->tree_block == 128 ? 7 : 8, (int)t->tree_ctas_per_sm};
+    return LVBH_OK;
+}
+
+int lvbh_get_tunables(lvbh_ctx *ctx, lvbh_tunables *t, float *candidate_ms, uint32_t *num_candidates) {
+    if (!ctx || !t) return LVBH_EINVAL;
+    const Tuned &c = ctx->last_tuned;
+    t->digit_bits = (uint32_t)c.t.digit_bits;
+    t->tree_block = 1u << c.t.log_block;
+    t->tree_ctas_per_sm = (uint32_t)c.t.tree_ctas;
+    t->reserved = 0;
+    if (num_candidates) *num_candidates = c.candidates;
+    for (uint32_t i = 0; candidate_ms && i < c.candidates; ++i) candidate_ms[i] = c.ms[i];
+    return LVBH_OK;
 }
 
 int lvbh_sync(lvbh_ctx *ctx) {

@@ -41,10 +41,25 @@ namespace lvbh {
 
 namespace {
 
-constexpr int EB = kEmitBlock;                 // level 1: leaves (threads) per CTA
-constexpr int kLogEB = 8;                      // EB == 1 << kLogEB
-static_assert(EB == 1 << kLogEB && 2 * kLogEB + 14 <= 32, "packed item ranges");
-constexpr int kTreeCtasPerSm = 4;             // resident K3b CTAs per SM (persistent grid)
+// Tree-pass geometry: blocks of 2^LOG sorted leaves (one thread each), resident CTAs per SM
+// of the persistent grid.  The plain build uses LOG = 8; a batched build may pick LOG = 7.
+template <int LOG>
+struct TreeGeo {
+    static constexpr int kLog = LOG;
+    static constexpr int EB = 1 << LOG;
+    static constexpr int kCtasPerSm = LOG == 8 ? 4 : 8;
+    static_assert(2 * LOG + 14 <= 32, "packed item ranges");
+    // packed local range and end separators of a climbing item:
+    // l | r << LOG | (d[l-1] + 1) << 2 LOG | (d[r] + 1) << 2 LOG + 7   (d + 1 <= 64)
+    static __device__ __forceinline__ uint32_t pack(int l, int r, int dl, int dr) {
+        return (uint32_t)l | ((uint32_t)r << LOG) | ((uint32_t)(dl + 1) << (2 * LOG)) |
+               ((uint32_t)(dr + 1) << (2 * LOG + 7));
+    }
+    static __device__ __forceinline__ int rl(uint32_t p) { return (int)(p & (EB - 1)); }
+    static __device__ __forceinline__ int rr(uint32_t p) { return (int)((p >> LOG) & (EB - 1)); }
+    static __device__ __forceinline__ int rdl(uint32_t p) { return (int)((p >> (2 * LOG)) & 127u) - 1; }
+    static __device__ __forceinline__ int rdr(uint32_t p) { return (int)(p >> (2 * LOG + 7)) - 1; }
+};
 constexpr int kTopLanes = 8;                   // K3c threads per block of K3b
 constexpr int kFreeClimb = 64;                 // K3b items left when compaction stops
 
@@ -57,13 +72,17 @@ struct Span {
     int b0;        // the block's first leaf within the segment
 };
 
+template <int LOG>
 struct OneSeg {
+    static constexpr int EB = 1 << LOG;
     int n;
     __device__ __forceinline__ int blocks() const { return (n + EB - 1) / EB; }
     __device__ __forceinline__ Span span(int blk) const { return Span{0, n, blk * EB}; }
 };
 
+template <int LOG>
 struct ManySegs {
+    static constexpr int EB = 1 << LOG;
     const SegRow *rows;       // num_segs + 1 rows
     const uint32_t *blk_seg;  // segment of each block
     int nblk;
@@ -77,8 +96,8 @@ struct ManySegs {
 };
 
 // K3b shared memory.  A climbing item is two float4: box min + link (node index, or
-// -(leaf + 1)), box max + its packed local range and end separators
-// (l | r << kLogEB | (d[l-1] + 1) << 2 kLogEB | (d[r] + 1) << 2 kLogEB + 7; d + 1 <= 64).
+// -(leaf + 1)), box max + its packed local range and end separators (TreeGeo::pack).
+template <int EB>
 struct ClimbSmem {
     float4 tri[2][EB][3];   // the gathered triangles of this block and the next (cp.async)
     float4 pend[2][2][EB];  // [side][min/max][split] the child parked at each split
@@ -94,21 +113,12 @@ struct ClimbSmem {
     int open;               // open items emitted
 };
 
-__device__ __forceinline__ uint32_t pack_range(int l, int r, int dl, int dr) {
-    return (uint32_t)l | ((uint32_t)r << kLogEB) | ((uint32_t)(dl + 1) << (2 * kLogEB)) |
-           ((uint32_t)(dr + 1) << (2 * kLogEB + 7));
-}
-__device__ __forceinline__ int range_l(uint32_t p) { return (int)(p & (EB - 1)); }
-__device__ __forceinline__ int range_r(uint32_t p) { return (int)((p >> kLogEB) & (EB - 1)); }
-__device__ __forceinline__ int range_dl(uint32_t p) { return (int)((p >> (2 * kLogEB)) & 127u) - 1; }
-__device__ __forceinline__ int range_dr(uint32_t p) { return (int)(p >> (2 * kLogEB + 7)) - 1; }
-
 // K3b: leaf gather, rearrange and the tree over blocks of EB sorted leaves (see the pass list
 // above).  Leaf t of a block gathers triangle perm[b0 + t]: its index is loaded two blocks
 // ahead, its three 16-byte rows are copied into shared memory one block ahead (cp.async, no
 // registers held meanwhile), then written to the output soup and reduced to the leaf box.
-template <class Segs>
-__global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
+template <int LOG, class Segs>
+__global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_tree_climb(Segs segs,
                                                     const uint32_t *__restrict__ keys_all,
                                                     const float4 *__restrict__ tri_all,
                                                     const uint32_t *__restrict__ perm_all,
@@ -116,8 +126,10 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
                                                     float4 *nodes_all, int32_t *parents_all,
                                                     OpenItem *out_items, uint32_t *out_counts,
                                                     Control *ctl) {
+    using G = TreeGeo<LOG>;
+    constexpr int EB = G::EB;
     extern __shared__ __align__(16) unsigned char smem[];
-    ClimbSmem &S = *reinterpret_cast<ClimbSmem *>(smem);
+    ClimbSmem<EB> &S = *reinterpret_cast<ClimbSmem<EB> *>(smem);
     const int t = threadIdx.x, lane = t & 31;
     const int nblk = segs.blocks();
     const uint32_t lt = lanemask_lt();
@@ -225,10 +237,10 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             const uint32_t pk = __float_as_uint(hi.w);
             OpenItem it;
             it.lo = lo;
-            it.hi = make_float4(hi.x, hi.y, hi.z, __int_as_float(range_dr(pk)));
-            it.xl = b0 + range_l(pk);
-            it.xr = b0 + range_r(pk);
-            it.pad0 = range_dl(pk);
+            it.hi = make_float4(hi.x, hi.y, hi.z, __int_as_float(G::rdr(pk)));
+            it.xl = b0 + G::rl(pk);
+            it.xr = b0 + G::rr(pk);
+            it.pad0 = G::rdl(pk);
             it.pad1 = 0;
             const int at = atomicAdd(&S.open, 1);
             if (at < kOpenCap) out[at] = it;
@@ -238,7 +250,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
         // parked sibling into the parent (returned in nlo/nhi, true unless it is the root).
         auto climb = [&](float4 lo, float4 hi, float4 &nlo, float4 &nhi) -> bool {
             const uint32_t pk = __float_as_uint(hi.w);
-            const int l = range_l(pk), r = range_r(pk), dl = range_dl(pk), dr = range_dr(pk);
+            const int l = G::rl(pk), r = G::rr(pk), dl = G::rdl(pk), dr = G::rdr(pk);
             const bool is_left = dr > dl;
             const int s = is_left ? r : l - 1;
             if (s < 0 || s > m - 2) {
@@ -251,8 +263,8 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             if (atom_or_acq_rel_cta(&S.mask[s], 1u << side) == 0u) return false;  // first parks
             const float4 slo = S.pend[side ^ 1][0][s], shi = S.pend[side ^ 1][1][s];
             const uint32_t spk = __float_as_uint(shi.w);
-            const int L = is_left ? l : range_l(spk), R = is_left ? range_r(spk) : r;
-            const int ndl = is_left ? dl : range_dl(spk), ndr = is_left ? range_dr(spk) : dr;
+            const int L = is_left ? l : G::rl(spk), R = is_left ? G::rr(spk) : r;
+            const int ndl = is_left ? dl : G::rdl(spk), ndr = is_left ? G::rdr(spk) : dr;
             const bool root = (b0 + L == 0) && (b0 + R == n - 1);
             const int P = root ? 0 : (ndr > ndl ? b0 + R : b0 + L);
             // the record: this child in slot `side`, the sibling in the other (f_1 = 2, f_2 = 0)
@@ -267,7 +279,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
             if (root) return false;
             nlo = make_float4(fminf(lo.x, slo.x), fminf(lo.y, slo.y), fminf(lo.z, slo.z), __int_as_float(P));
             nhi = make_float4(fmaxf(hi.x, shi.x), fmaxf(hi.y, shi.y), fmaxf(hi.z, shi.z),
-                              __uint_as_float(pack_range(L, R, ndl, ndr)));
+                              __uint_as_float(G::pack(L, R, ndl, ndr)));
             return true;
         };
         // the items that climb on go to queue oq, counted in S.cnt[oc] (warp-aggregated)
@@ -288,7 +300,7 @@ __global__ void __launch_bounds__(EB, kTreeCtasPerSm) k_tree_climb(Segs segs,
         bool cont = false;
         if (active)
             cont = climb(leaf_lo, make_float4(leaf_hi0.x, leaf_hi0.y, leaf_hi0.z,
-                                              __uint_as_float(pack_range(t, t, dval(t - 1), dval(t)))),
+                                              __uint_as_float(G::pack(t, t, dval(t - 1), dval(t)))),
                          nlo, nhi);
         append(cont, nlo, nhi, 0, 0);
         // later steps: the merged parents, compacted.  Once at most kFreeClimb items are left,
@@ -432,18 +444,21 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
     }
 }
 
-inline size_t leaves_smem_bytes() { return sizeof(ClimbSmem); }
+template <int LOG>
+inline size_t leaves_smem_bytes() { return sizeof(ClimbSmem<TreeGeo<LOG>::EB>); }
 
-template <class Segs>
+template <int LOG, class Segs>
 void launch_emit_impl(Segs segs, int groups, const float4 *tri, const uint32_t *perm,
                       const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
                       OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
                       uint8_t *pend_d, const uint32_t *epoch, Control *ctl, bool top,
-                      cudaStream_t s, cudaEvent_t *ev) {
+                      cudaStream_t s, cudaEvent_t *ev, int ctas_per_sm) {
     if (ev) cudaEventRecord(ev[0], s);  // the leaf gather runs inside the tree pass
-    const int grid = min(groups, sm_count() * kTreeCtasPerSm);
-    k_tree_climb<<<grid, EB, leaves_smem_bytes(), s>>>(segs, keys, tri, perm, otri, nodes, parents,
-                                                        items, counts, ctl);
+    const int per_sm = ctas_per_sm > 0 && ctas_per_sm < TreeGeo<LOG>::kCtasPerSm ? ctas_per_sm
+                                                                                : TreeGeo<LOG>::kCtasPerSm;
+    const int grid = min(groups, sm_count() * per_sm);
+    k_tree_climb<LOG, Segs><<<grid, TreeGeo<LOG>::EB, leaves_smem_bytes<LOG>(), s>>>(
+        segs, keys, tri, perm, otri, nodes, parents, items, counts, ctl);
     if (ev) cudaEventRecord(ev[1], s);
     if (top)
         k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, counts, nodes,
@@ -453,9 +468,8 @@ void launch_emit_impl(Segs segs, int groups, const float4 *tri, const uint32_t *
 }
 
 template <class K>
-cudaError_t prefer_shared(K kernel) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)leaves_smem_bytes());
+cudaError_t prefer_shared(K kernel, size_t bytes) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared);
@@ -463,12 +477,13 @@ cudaError_t prefer_shared(K kernel) {
 
 }  // namespace
 
-size_t emit_groups(uint32_t n) { return (n + EB - 1) / EB; }
+size_t emit_groups(uint32_t n, int log_eb) { return (n + (1u << log_eb) - 1) >> log_eb; }
 
 cudaError_t emit_init() {
-    cudaError_t e = prefer_shared(k_tree_climb<OneSeg>);
-    if (e != cudaSuccess) return e;
-    return prefer_shared(k_tree_climb<ManySegs>);
+    cudaError_t e = prefer_shared(k_tree_climb<8, OneSeg<8>>, leaves_smem_bytes<8>());
+    if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, ManySegs<8>>, leaves_smem_bytes<8>());
+    if (e == cudaSuccess) e = prefer_shared(k_tree_climb<7, ManySegs<7>>, leaves_smem_bytes<7>());
+    return e;
 }
 
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
@@ -476,9 +491,10 @@ void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, 
                  uint32_t *counts, uint32_t *arrive, float4 *pend, uint8_t *pend_d,
                  const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev) {
     if (n == 0) return;
-    const int groups = (int)emit_groups(n);
-    launch_emit_impl(OneSeg{(int)n}, groups, tri, perm, keys, otri, nodes, parents, items, counts,
-                     arrive, pend, pend_d, epoch, ctl, groups > 1, s, ev);
+    const int groups = (int)emit_groups(n, kLogEmitBlock);
+    launch_emit_impl<kLogEmitBlock>(OneSeg<kLogEmitBlock>{(int)n}, groups, tri, perm, keys, otri,
+                                    nodes, parents, items, counts, arrive, pend, pend_d, epoch,
+                                    ctl, groups > 1, s, ev, 0);
 }
 
 void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
@@ -487,9 +503,14 @@ void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *p
                        uint8_t *pend_d, const uint32_t *epoch, Control *ctl, cudaStream_t s,
                        cudaEvent_t *ev) {
     if (bp.blocks == 0) return;
-    launch_emit_impl(ManySegs{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks, tri, perm, keys,
-                     otri, nodes, parents, items, counts, arrive, pend, pend_d, epoch, ctl, true, s,
-                     ev);
+    if (bp.log_block == 7)
+        launch_emit_impl<7>(ManySegs<7>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks, tri,
+                            perm, keys, otri, nodes, parents, items, counts, arrive, pend, pend_d,
+                            epoch, ctl, true, s, ev, bp.tree_ctas_per_sm);
+    else
+        launch_emit_impl<8>(ManySegs<8>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks, tri,
+                            perm, keys, otri, nodes, parents, items, counts, arrive, pend, pend_d,
+                            epoch, ctl, true, s, ev, bp.tree_ctas_per_sm);
 }
 
 }  // namespace lvbh

@@ -38,7 +38,8 @@ inline uint32_t *sort_chunk_sums(uint32_t *scratch, uint32_t n) {
 
 // Tree/refit pass: leaves per block of the in-block tree pass (one thread each); open nodes a
 // block can leave to the straddling pass (at most 2 x the tree depth 64).
-constexpr int kEmitBlock = 256;
+constexpr int kLogEmitBlock = 8;  // the plain build's tree blocks (a batched build may use 7)
+constexpr int kEmitBlock = 1 << kLogEmitBlock;
 constexpr int kOpenCap = 128;
 
 // A complete subtree handed from one level of the tree pass to the next: box min + link,
@@ -81,6 +82,9 @@ struct BatchPlan {
     const uint32_t *tile_seg;  // segment of each sort tile (device, `tiles` entries)
     const uint32_t *blk_seg;   // segment of each tree block (device, `blocks` entries)
     uint32_t num_segs, tiles, blocks, total;
+    int digit_bits;            // sort digit width: 10 (three passes) or 8 (four passes)
+    int log_block;             // tree blocks of 2^log_block leaves: 8 or 7
+    int tree_ctas_per_sm;      // persistent tree grid: CTAs per SM (0 = the most that fit)
 };
 
 int sm_count();
@@ -115,7 +119,7 @@ cudaError_t sort_init();  // once per device, before the first launch
 // -> BVH nodes, parent links, sorted triangles.  Scratch: items (emit_groups(n) * kOpenCap)
 // and counts (emit_groups(n)), arrive (n words, zero or older epochs), pend (2n float4),
 // pend_d (n bytes); *epoch is this build's epoch (advanced by K1b).
-size_t emit_groups(uint32_t n);
+size_t emit_groups(uint32_t n, int log_eb = kLogEmitBlock);
 cudaError_t emit_init();  // once per device, before the first launch
 // ev (may be nullptr): three events, recorded before K3b, after K3b and after K3c.
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
@@ -131,6 +135,7 @@ void launch_seg_tables(const SegRow *rows, uint32_t num_segs, uint32_t *tile_seg
                        uint32_t *blk_seg, cudaStream_t s);
 void launch_bounds_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,
                          uint32_t *seg_ord, cudaStream_t s);
+// seg_hist: kHistWords per segment, pass-major (bp.digit_bits wide digits).
 void launch_morton_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,
                          const uint32_t *seg_ord, uint32_t *seg_hist, Control *ctl,
                          uint32_t *keys_out, uint32_t *epoch, cudaStream_t s);

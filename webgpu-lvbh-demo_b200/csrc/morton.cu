@@ -205,6 +205,7 @@ __global__ void __launch_bounds__(kThreads) k_bounds_batch(const float4 *__restr
 // Batched K1b: one block per sort tile; each warp takes chunks of 32 triangles of the tile
 // (the same transposed 16-byte loads as k_morton), quantises them with the segment's bounds
 // and adds the tile's digit counts to the segment's histograms.
+template <int BITS>
 __global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restrict__ tri,
                                                            const SegRow *__restrict__ rows,
                                                            const uint32_t *__restrict__ tile_seg,
@@ -214,13 +215,15 @@ __global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restr
                                                            Control *__restrict__ ctl,
                                                            uint32_t *__restrict__ keys,
                                                            uint32_t *__restrict__ epoch) {
+    constexpr int D = 1 << BITS, NP = BITS == kDigitBits ? kSortPasses : kSortPasses32;
+    static_assert(NP * D <= kHistWords, "per-segment counts");
     __shared__ float4 stage[kWarps][96];
-    __shared__ uint32_t hist[kSortPasses][kDigits];
+    __shared__ uint32_t hist[NP][D];
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
         const uint32_t e = *epoch + 1u;
         *epoch = e == 0u ? 1u : e;
     }
-    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) (&hist[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < NP * D; i += kThreads) (&hist[0][0])[i] = 0;
     const uint32_t tile = blockIdx.x, sg = __ldg(tile_seg + tile);
     const uint32_t t0 = __ldg(&rows[sg].tri), t1 = __ldg(&rows[sg + 1].tri);
     const uint32_t first = t0 + (tile - __ldg(&rows[sg].tile)) * (uint32_t)kSortTile;
@@ -262,13 +265,13 @@ __global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restr
             const uint32_t key = morton3(qx, qy, qz);
             keys[first + t] = key;
 #pragma unroll
-            for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (kDigitBits * p)) & (kDigits - 1)], 1u);
+            for (int p = 0; p < NP; ++p) atomicAdd(&hist[p][(key >> (BITS * p)) & (D - 1)], 1u);
         }
     }
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
     __syncthreads();
-    uint32_t *h = seg_hist + (size_t)sg * kSortPasses * kDigits;
-    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) {
+    uint32_t *h = seg_hist + (size_t)sg * kHistWords;
+    for (int i = threadIdx.x; i < NP * D; i += kThreads) {
         const uint32_t c = (&hist[0][0])[i];
         if (c) atomicAdd(h + i, c);
     }
@@ -343,8 +346,12 @@ void launch_morton_batch(const BatchPlan &bp, const float4 *tri, const float *ho
                          const uint32_t *seg_ord, uint32_t *seg_hist, Control *ctl,
                          uint32_t *keys_out, uint32_t *epoch, cudaStream_t s) {
     if (bp.tiles == 0) return;
-    k_morton_batch<<<bp.tiles, kThreads, 0, s>>>(tri, bp.rows, bp.tile_seg, host_bounds, seg_ord,
-                                                 seg_hist, ctl, keys_out, epoch);
+    if (bp.digit_bits == kDigitBits32)
+        k_morton_batch<kDigitBits32><<<bp.tiles, kThreads, 0, s>>>(tri, bp.rows, bp.tile_seg, host_bounds,
+                                                                   seg_ord, seg_hist, ctl, keys_out, epoch);
+    else
+        k_morton_batch<kDigitBits><<<bp.tiles, kThreads, 0, s>>>(tri, bp.rows, bp.tile_seg, host_bounds,
+                                                                 seg_ord, seg_hist, ctl, keys_out, epoch);
 }
 
 }  // namespace lvbh

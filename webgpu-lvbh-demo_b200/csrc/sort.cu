@@ -82,17 +82,18 @@ struct OneSegSort {
     }
 };
 
+template <int BITS>
 struct ManySegSort {
     const SegRow *rows;
     const uint32_t *tile_seg;
-    const uint32_t *seg_hist;  // [segment][pass][digit]
+    const uint32_t *seg_hist;  // kHistWords per segment: [pass][digit]
     int pass;
     __device__ __forceinline__ TileSpan span(uint32_t tile) const {
         const uint32_t sg = __ldg(tile_seg + tile);
         const uint32_t t0 = __ldg(&rows[sg].tri), t1 = __ldg(&rows[sg + 1].tri);
         const uint32_t first = __ldg(&rows[sg].tile);
         return TileSpan{t0, t1 - t0, (tile - first) * (uint32_t)kSortTile, first,
-                        seg_hist + ((size_t)sg * kSortPasses + pass) * kDigits};
+                        seg_hist + (size_t)sg * kHistWords + pass * (1 << BITS)};
     }
 };
 
@@ -515,7 +516,8 @@ cudaError_t allow_smem() {
 }  // namespace
 
 cudaError_t sort_init() {
-    cudaError_t e = allow_smem<kDigitBits, ManySegSort>();
+    cudaError_t e = allow_smem<kDigitBits, ManySegSort<kDigitBits>>();
+    if (e == cudaSuccess) e = allow_smem<kDigitBits32, ManySegSort<kDigitBits32>>();
     if (e == cudaSuccess) e = allow_smem<kDigitBits32, OneSegSort>();
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_scatter<kDigitBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -554,8 +556,14 @@ void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const u
                            const uint32_t *seg_hist, Control *ctl, uint32_t *lookback,
                            cudaStream_t s) {
     if (bp.tiles == 0) return;
-    launch<kDigitBits>(ManySegSort{bp.rows, bp.tile_seg, seg_hist, pass}, bp.tiles, keys_in, vals_in,
-                       keys_out, vals_out, pass, ctl, lookback + (size_t)pass * bp.tiles * kDigits, s);
+    if (bp.digit_bits == kDigitBits32)
+        launch<kDigitBits32>(ManySegSort<kDigitBits32>{bp.rows, bp.tile_seg, seg_hist, pass}, bp.tiles,
+                             keys_in, vals_in, keys_out, vals_out, pass, ctl,
+                             lookback + (size_t)pass * bp.tiles * kDigits32, s);
+    else
+        launch<kDigitBits>(ManySegSort<kDigitBits>{bp.rows, bp.tile_seg, seg_hist, pass}, bp.tiles,
+                           keys_in, vals_in, keys_out, vals_out, pass, ctl,
+                           lookback + (size_t)pass * bp.tiles * kDigits, s);
 }
 
 }  // namespace lvbh

@@ -25,8 +25,8 @@ from typing import Optional
 import numpy as np
 
 from . import _native
-from ._native import (ASYNC, INPUT_HOST, NO_GRAPH, OUT_CALLER, PROFILE, STAGE_NAMES, LvbhError,
-                      version)
+from ._native import (ASYNC, AUTOTUNE, INPUT_HOST, NO_GRAPH, OUT_CALLER, PROFILE, STAGE_NAMES,
+                      LvbhError, version)
 
 __all__ = ["initBVHBuild", "BVHBuilder", "BuildResult", "BatchResult", "LvbhError", "version",
            "trace"]
@@ -217,7 +217,7 @@ class BVHBuilder:
                          outputs, stream, sync, profile, keep=(xyz, idx3))
 
     def build_batched(self, tri, offsets, seg_bounds=None, outputs=None, stream=None, sync=True,
-                      profile=False, graph=True) -> BatchResult:
+                      profile=False, graph=True, autotune=False) -> BatchResult:
         """Many meshes in one build.  tri: (sum N, 12) float32 host array or CUDA tensor with
         the meshes end to end; offsets: num_meshes + 1 triangle offsets (offsets[0] = 0);
         seg_bounds: (M, 6) float32 per-mesh MODEL_BOUNDS or None (each mesh's own box)."""
@@ -248,7 +248,7 @@ class BVHBuilder:
         sb = None if seg_bounds is None else np.ascontiguousarray(seg_bounds, dtype=np.float32).reshape(m, 6)
         bout = np.zeros((m, 6), dtype=np.float32)
         flags = OUT_CALLER | (INPUT_HOST if host else 0) | (0 if sync else ASYNC) \
-            | (PROFILE if profile else 0) | (0 if graph else NO_GRAPH)
+            | (PROFILE if profile else 0) | (0 if graph else NO_GRAPH) | (AUTOTUNE if autotune else 0)
         rc = _native.lib.lvbh_build_batched(
             self._ctx, ptr, offs32.ctypes.data_as(ctypes.c_void_p), m,
             None if sb is None else sb.ctypes.data_as(ctypes.c_void_p),
@@ -263,6 +263,27 @@ class BVHBuilder:
         else:
             self._pending = (r, res, (tri, offs32, sb, bout), profile)
         return res
+
+    def set_tunables(self, digit_bits=None, tree_block=None, tree_ctas_per_sm=0):
+        """Force the batched-build tunables (digit_bits 10 or 8, tree_block 256 or 128);
+        no arguments = back to LVBH_AUTOTUNE / the defaults."""
+        if digit_bits is None and tree_block is None:
+            _native.check(self._ctx, _native.lib.lvbh_set_tunables(self._ctx, None))
+            return
+        t = _native.Tunables(digit_bits=digit_bits or 10, tree_block=tree_block or 256,
+                             tree_ctas_per_sm=tree_ctas_per_sm)
+        _native.check(self._ctx, _native.lib.lvbh_set_tunables(self._ctx, ctypes.byref(t)))
+
+    def tunables(self) -> dict:
+        """The tunables of the last batched build, and the candidates' times when it tuned."""
+        t = _native.Tunables()
+        ms = (ctypes.c_float * 4)()
+        nc = ctypes.c_uint32()
+        _native.check(self._ctx, _native.lib.lvbh_get_tunables(self._ctx, ctypes.byref(t), ms,
+                                                               ctypes.byref(nc)))
+        return {"digit_bits": t.digit_bits, "tree_block": t.tree_block,
+                "tree_ctas_per_sm": t.tree_ctas_per_sm,
+                "candidates_ms": [float(x) for x in ms[:nc.value]]}
 
     def _run(self, fn, head, n, bounds, flags, outputs, stream, sync, profile, keep):
         if self._pending is not None:

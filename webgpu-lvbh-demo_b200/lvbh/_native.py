@@ -18,7 +18,7 @@ STATUS_NAMES = {OK: "LVBH_OK", EINVAL: "LVBH_EINVAL", ENOMEM: "LVBH_ENOMEM",
 NOALLOC_MAX_KEYS = 1 << 20
 
 # build flags
-INPUT_HOST, ASYNC, OUT_CALLER, PROFILE, NO_GRAPH = 0x1, 0x2, 0x4, 0x8, 0x10
+INPUT_HOST, ASYNC, OUT_CALLER, PROFILE, NO_GRAPH, AUTOTUNE = 0x1, 0x2, 0x4, 0x8, 0x10, 0x20
 MAX_TRIS = 1 << 29
 NUM_STAGES = 7
 STAGE_NAMES = ("upload", "bounds", "morton", "sort", "gather", "tree", "top")
@@ -43,6 +43,11 @@ class Result(ctypes.Structure):
                 ("parents", ctypes.c_void_p), ("leaf_index", ctypes.c_void_p),
                 ("morton", ctypes.c_void_p), ("bounds", ctypes.c_float * 6),
                 ("owned", ctypes.c_uint32)]
+
+
+class Tunables(ctypes.Structure):
+    _fields_ = [("digit_bits", ctypes.c_uint32), ("tree_block", ctypes.c_uint32),
+                ("tree_ctas_per_sm", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -83,6 +88,11 @@ def _load():
     L.lvbh_build_indexed.argtypes = [vp, vp, u32, vp, u32, vp, u32, ctypes.POINTER(Result), vp]
     L.lvbh_build_batched.restype = i32
     L.lvbh_build_batched.argtypes = [vp, vp, vp, u32, vp, vp, u32, ctypes.POINTER(Result), vp]
+    L.lvbh_set_tunables.restype = i32
+    L.lvbh_set_tunables.argtypes = [vp, ctypes.POINTER(Tunables)]
+    L.lvbh_get_tunables.restype = i32
+    L.lvbh_get_tunables.argtypes = [vp, ctypes.POINTER(Tunables), ctypes.POINTER(ctypes.c_float),
+                                    ctypes.POINTER(ctypes.c_uint32)]
     L.lvbh_sync.restype = i32
     L.lvbh_sync.argtypes = [vp]
     L.lvbh_release.restype = i32
