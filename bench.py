@@ -476,6 +476,67 @@ def run_batched(args, world, rank, local, clocks=None):
             "generate_s": round(t_gen, 1)}
 
 
+def run_trace(args, world, rank, local):
+    """Closest-hit traversal throughput (the consumer of the BVH layout, pathtracer.js:495-628):
+    the 2,097,152-triangle displaced sphere built once, then `args.rays` rays per step (origins
+    on a radius-3 sphere, directions toward [-1, 1]^3) traced through lvbh_trace, CUDA events
+    around each call; the CPU restatement traces a sample on all host cores."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import lvbh
+    from lvbh import _native, scenes
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    tri = scenes.sphere_mesh(1024, seed=1)
+    builder = lvbh.BVHBuilder(local)
+    res = builder.build_soup(torch.from_numpy(tri).to(dev))
+    rays = scenes.sphere_rays(args.rays, seed=11)
+    drays = torch.from_numpy(rays).to(dev)
+    n = tri.shape[0]
+    prim = torch.empty(args.rays, dtype=torch.int32, device=dev)
+    t = torch.empty(args.rays, dtype=torch.float32, device=dev)
+    st = torch.empty(args.rays, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ptrs = [ctypes.c_void_p(x.data_ptr()) for x in (res.nodes, res.tris, drays, prim, t, st)]
+
+    def step():
+        _native.check(builder.ctx, _native.lib.lvbh_trace(builder.ctx, ptrs[0], ptrs[1], n, ptrs[2],
+                                                          args.rays, ptrs[3], ptrs[4], ptrs[5],
+                                                          ctypes.c_void_p(stream.cuda_stream)))
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = max_over_ranks(statistics.median(times), world)
+    hits = int((prim >= 0).sum().item())
+    out = {"workload": "sphere_mesh_2M_trace", "rays": args.rays, "ms_per_step": ms,
+           "mrays_per_s": world * args.rays / (ms * 1e-3) / 1e6, "hit_fraction": hits / args.rays,
+           "max_stack": int(st.max().item())}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        ref = res.to_numpy()
+        sample = rays[: min(args.rays, 1 << 18)]
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.trace(ref["nodes"], ref["tris"], sample, threads=cores)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": sample.shape[0] / dt / 1e6, "unit": "Mrays/s", "cores": cores,
+                               "kind": "port", "sample": f"{sample.shape[0]:,} rays of the same set"}
+    builder.close()
+    return out
+
+
 def percentiles(x):
     import numpy as np
     a = np.asarray(x, dtype=np.float64)
@@ -625,6 +686,7 @@ def main():
     ap.add_argument("--serve-min-requests", type=int, default=1000)
     ap.add_argument("--serve-max-requests", type=int, default=100_000)
     ap.add_argument("--serve-pool", type=int, default=4)
+    ap.add_argument("--rays", type=int, default=1 << 22)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -634,6 +696,10 @@ def main():
             run_reference(args, world, rank)
         elif args.workload == "batch":
             out = run_batched(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(out), flush=True)
+        elif args.workload == "trace":
+            out = run_trace(args, world, rank, local)
             if rank == 0:
                 print(json.dumps(out), flush=True)
         elif args.workload == "served":

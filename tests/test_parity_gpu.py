@@ -230,15 +230,8 @@ def test_clustered_16M(builder):
 
 
 def make_rays(n, seed, radius=3.0):
-    rng = np.random.Generator(np.random.PCG64(seed))
-    o = rng.standard_normal((n, 3))
-    o = o / np.linalg.norm(o, axis=1, keepdims=True) * radius
-    d = rng.uniform(-1.0, 1.0, (n, 3)) - o
-    d /= np.linalg.norm(d, axis=1, keepdims=True)
-    rays = np.zeros((n, 8), dtype=np.float32)
-    rays[:, 0:3] = o
-    rays[:, 4:7] = d
-    return rays
+    from lvbh import scenes
+    return scenes.sphere_rays(n, seed, radius)
 
 
 def check_tree_properties(tri, got):

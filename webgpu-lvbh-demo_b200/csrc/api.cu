@@ -109,6 +109,7 @@ struct lvbh_ctx {
     void *stage = nullptr;
     // pinned readback of the control block head
     uint32_t *host_ctl = nullptr;
+    uint32_t *trace_counter = nullptr;  // ray counter of the persistent traversal
     cudaEvent_t ev[LVBH_NUM_STAGES + 1] = {};
     bool ev_valid = false;
     // cached graph of the last build shape
@@ -568,6 +569,7 @@ void lvbh_destroy(lvbh_ctx *ctx) {
     for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     if (ctx->host_ctl) cudaFreeHost(ctx->host_ctl);
+    if (ctx->trace_counter) cudaFree(ctx->trace_counter);
     cudaGetLastError();
     delete ctx;
 }
@@ -885,8 +887,10 @@ int lvbh_trace(lvbh_ctx *ctx, const void *nodes, const void *tris, uint32_t num_
     if (num_tris && (!nodes || !tris)) return fail(ctx, LVBH_EINVAL, "NULL tree buffer");
     DeviceGuard g(ctx->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!ctx->trace_counter) LVBH_CUDA(ctx, cudaMalloc(&ctx->trace_counter, sizeof(uint32_t)));
     launch_trace(static_cast<const float4 *>(nodes), static_cast<const float4 *>(tris), num_tris,
-                 reinterpret_cast<const float4 *>(rays), num_rays, hit_prim, hit_t, max_stack, s);
+                 reinterpret_cast<const float4 *>(rays), num_rays, hit_prim, hit_t, max_stack,
+                 ctx->trace_counter, s);
     LVBH_CUDA(ctx, cudaGetLastError());
     LVBH_CUDA(ctx, cudaStreamSynchronize(s));
     return LVBH_OK;

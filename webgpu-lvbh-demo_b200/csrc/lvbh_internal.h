@@ -153,9 +153,9 @@ void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *p
 // *err and gathers zeros instead of reading out of bounds.
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,
                            uint32_t n, float4 *tri, uint32_t *err, cudaStream_t s);
-// K5: closest-hit traversal (validation consumer).
+// K5: closest-hit traversal (persistent, rays fetched from *counter, which it zeroes first).
 void launch_trace(const float4 *nodes, const float4 *tris, uint32_t n, const float4 *rays,
                   uint32_t num_rays, int32_t *hit_prim, float *hit_t, uint32_t *max_stack,
-                  cudaStream_t s);
+                  uint32_t *counter, cudaStream_t s);
 
 }  // namespace lvbh

@@ -14,6 +14,8 @@ it with the shapes, sizes and value distributions of the five build workloads:
   mesh_batch        many independent uniform_soup meshes of log-uniform sizes, each inside
                     its own random box with corners uniform in [-100, 100]^3
   request_sizes     log-uniform request sizes for the build server
+  sphere_rays       rays for the sphere: origins uniform on a radius-3 sphere, directions
+                    toward uniform points in [-1, 1]^3
 
 All randomness comes from numpy's PCG64 generator seeded by the caller.  Every scene is
 returned as the reference's 48-byte triangle layout: float32 array (N, 12), vertices at
@@ -137,6 +139,20 @@ def mesh_batch(count: int = 4096, lo: int = 64, hi: int = 262_144, seed: int = 3
         soup[offsets[m]:offsets[m + 1]] = uniform_soup(int(sizes[m]), seed=seed * 100_003 + m,
                                                        lo=lo_c, hi=hi_c)
     return soup, offsets
+
+
+def sphere_rays(n: int = 1 << 20, seed: int = 11, radius: float = 3.0) -> np.ndarray:
+    """(n, 8) float32 rays {ox, oy, oz, 0, dx, dy, dz, 0}: origins uniform on a sphere of the
+    given radius, unit directions toward points uniform in [-1, 1]^3."""
+    rng = _rng(seed)
+    o = rng.standard_normal((n, 3))
+    o = o / np.linalg.norm(o, axis=1, keepdims=True) * radius
+    d = rng.uniform(-1.0, 1.0, (n, 3)) - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros((n, 8), dtype=np.float32)
+    rays[:, 0:3] = o
+    rays[:, 4:7] = d
+    return rays
 
 
 def request_sizes(count: int = 100_000, lo: int = 1024, hi: int = 4_194_304, seed: int = 4) -> np.ndarray:
