@@ -356,11 +356,12 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
 // the block's open items (a block leaves about 8) through the remaining splits.  At a split the
 // first arriving child parks its box, link and far range end in pend[] and its far end's
 // separator in pend_d[], both at its own index (r when it is a left child, l when a right child -
-// no two pending children ever share one), fences, and exchanges the build's epoch into the
-// split's arrival word; the second, seeing the epoch already there, reads its sibling back,
+// no two pending children ever share one), and exchanges the build's epoch into the split's
+// arrival word with release-acquire semantics; the second, seeing the epoch already there,
+// reads its sibling back,
 // merges, and has the parent's range, both end separators and so its Karras index without
 // touching the keys.  A completed record and its two parent links are stored after the next
-// split's exchange, so the fence before that exchange waits for the two parked rows only.
+// split's exchange, so that exchange's release waits for the parked rows only.
 // Nothing waits, so the kernel cannot hang; climbs are bounded and every index is
 // range-checked.  The epoch makes the arrival words reusable without clearing: a word left by
 // an older build never equals the current epoch.
@@ -413,11 +414,9 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
             pend[2ull * own] = h0;
             pend[2ull * own + 1] = h1;
             pend_d[own] = (uint8_t)((is_left ? dl : dr) + 1);
-            fence_acq_rel_gpu();
-            const bool first = atomicExch(arrive + s, epoch) != epoch;
+            const bool first = atom_exch_acq_rel_gpu(arrive + s, epoch) != epoch;
             flush();
             if (first) { done = true; break; }  // the sibling completes the parent
-            fence_acq_rel_gpu();
             const float4 g0 = __ldcg(pend + 2ull * sib), g1 = __ldcg(pend + 2ull * sib + 1);
             const int gd = (int)__ldcg(pend_d + sib) - 1;
             const int sib_ref = __float_as_int(g0.w), sib_far = __float_as_int(g1.w);

@@ -81,6 +81,14 @@ __device__ __forceinline__ uint32_t atom_or_acq_rel_cta(uint32_t *p, uint32_t v)
     return old;
 }
 
+// Global-memory atomic exchange with acquire-release semantics at GPU scope (the park / merge
+// handshake across CTAs, as atom_or_acq_rel_cta is within one).
+__device__ __forceinline__ uint32_t atom_exch_acq_rel_gpu(uint32_t *p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.exch.b32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Relaxed gpu-scope load / store of a 32-bit word another CTA publishes.
 __device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t *p) {
     uint32_t v;
