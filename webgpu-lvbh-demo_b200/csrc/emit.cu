@@ -338,16 +338,15 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
                 emit(S.pend[side][0][t], S.pend[side][1][t]);
             }
         }
-        __syncthreads();
-        if (active) {
+        if (active) {  // the climb is over (barrier above): the staged links are final
             if (S.par[t] >= 0) parents[k] = S.par[t];
             if (S.par[EB + t] >= 0) parents[n + k] = S.par[EB + t];
         }
-        if (t == 0) {
+        __syncthreads();  // every open item counted; the next block may overwrite shared memory
+        if (t == 0) {  // before thread 0 itself resets the counter for the next block
             out_counts[blk] = (uint32_t)min(S.open, kOpenCap);
             if (S.open > kOpenCap) atomicOr(&ctl->err, ERR_CLIMB);
         }
-        __syncthreads();  // before the next block overwrites shared memory
     }
     if (bad_perm) atomicOr(&ctl->err, ERR_CLIMB);
 }
