@@ -66,6 +66,7 @@ extern "C" {
 #define LVBH_EBUSY     5  /* serving: queue full / request not finished yet */
 #define LVBH_EDEVICE   6  /* a kernel reported an inconsistent structure (bounded climb exceeded) */
 #define LVBH_ERANGE    7  /* a size beyond a fixed capacity (lvbh_sort_pairs_noalloc) */
+#define LVBH_EPARSE    8  /* lvbh_parse_obj: the text is one the reference's OBJ parser throws on */
 
 /* ---- build flags ------------------------------------------------------------------- */
 #define LVBH_INPUT_HOST    0x1u  /* input pointers are host memory: copied to the device inside the call */
@@ -305,6 +306,27 @@ LVBH_API int  lvbh_sort_pairs_noalloc(const uint32_t *keys_in, uint32_t num_keys
 LVBH_API int  lvbh_trace(lvbh_ctx *ctx, const void *nodes, const void *tris, uint32_t num_tris,
                 const float *rays, uint32_t num_rays, int32_t *hit_prim, float *hit_t,
                 uint32_t *max_stack, void *stream);
+
+/* ---- producer: OBJ text -> TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS ------------------------
+ * Replaces parseObj(file) (scripts/obj/parse-obj.js:3-88) and the OBJFile parser it calls
+ * (scripts/obj/obj-file-parser.js:19-193), the step main.js:72-73 runs before build().  The
+ * text (UTF-8 bytes, as FileReader.readAsText reads them) is parsed on the GPU with the
+ * reference's results: model 0's faces fan-triangulated, y and z swapped, as 12 float32 per
+ * triangle with pad 3.1415, two floor triangles appended; bounds6 the six doubles of BOUNDS
+ * (min xyz, max xyz) with Math.min / Math.max semantics.
+ *   text      `bytes` bytes, device memory, or host memory with LVBH_INPUT_HOST
+ *   bytes     at most LVBH_OBJ_MAX_BYTES
+ *   tri_out   receives a device pointer to *num_tris x 12 floats, owned by ctx and valid until
+ *             the next lvbh_parse_obj on ctx or lvbh_destroy (pass it to lvbh_build_soup)
+ *   err_line  where the reference throws: the 1-based line of the statement it rejects, or 0
+ *             for a failure found after parsing (no model; a face index naming no vertex)
+ *   stream    cudaStream_t or NULL; the call returns once the soup is complete
+ * Returns LVBH_OK, LVBH_EPARSE (with *err_line, and the reason in lvbh_last_error),
+ * LVBH_EINVAL (NULL pointer, size beyond LVBH_OBJ_MAX_BYTES), LVBH_ENOMEM or LVBH_ECUDA. */
+#define LVBH_OBJ_MAX_BYTES ((uint64_t)0xFFFFFE00u)
+LVBH_API int  lvbh_parse_obj(lvbh_ctx *ctx, const char *text, uint64_t bytes, uint32_t flags,
+                             const float **tri_out, uint32_t *num_tris, double *bounds6,
+                             uint64_t *err_line, void *stream);
 
 #ifdef __cplusplus
 }

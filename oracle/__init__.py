@@ -35,9 +35,9 @@ def build_lib() -> str:
 def lib():
     global _lib
     if _lib is None:
-        src = os.path.join(_HERE, "lvbh_oracle.cpp")
-        if not os.path.exists(_LIB_PATH) or (
-                os.path.exists(src) and os.path.getmtime(src) > os.path.getmtime(_LIB_PATH)):
+        srcs = [os.path.join(_HERE, f) for f in ("lvbh_oracle.cpp", "obj_oracle.cpp")]
+        if not os.path.exists(_LIB_PATH) or any(
+                os.path.exists(f) and os.path.getmtime(f) > os.path.getmtime(_LIB_PATH) for f in srcs):
             build_lib()
         L = ctypes.CDLL(_LIB_PATH)
         vp = ctypes.c_void_p
@@ -53,6 +53,9 @@ def lib():
         L.oracle_build.argtypes = [_f32p, u32, vp, ctypes.c_int, vp, vp, vp, vp, vp, vp]
         L.oracle_build.restype = ctypes.c_int
         L.oracle_trace.argtypes = [_u32p, _f32p, u32, _f32p, u32, _i32p, _f32p, _u32p, ctypes.c_int]
+        L.oracle_parse_obj.argtypes = [ctypes.c_char_p, ctypes.c_uint64, vp, ctypes.c_uint64,
+                                       ctypes.POINTER(ctypes.c_uint64), vp, ctypes.POINTER(ctypes.c_int64)]
+        L.oracle_parse_obj.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -155,3 +158,30 @@ def trace(nodes, tris, rays, threads: int = 0):
     st = np.empty(r, dtype=np.uint32)
     lib().oracle_trace(nodes, tris, tris.shape[0], rays, r, prim, t, st, threads)
     return prim, t, st
+
+
+class ObjThrows(ValueError):
+    """The reference's parseObj throws on this text; .line is the 1-based line of the statement
+    (0: a failure after parsing - no model, or a face index naming no vertex)."""
+
+    def __init__(self, line: int):
+        super().__init__(f"the reference throws (line {line})")
+        self.line = line
+
+
+def parse_obj(text):
+    """OBJ text (str or bytes) -> (tri (N, 12) float32, bounds (6,) float64) as parseObj
+    (scripts/obj/parse-obj.js) and build()'s Float32Array produce them, or raises ObjThrows
+    where the reference throws."""
+    data = text.encode() if isinstance(text, str) else bytes(text)
+    n = ctypes.c_uint64()
+    line = ctypes.c_int64()
+    b = np.empty(6, dtype=np.float64)
+    rc = lib().oracle_parse_obj(data, len(data), None, 0, ctypes.byref(n), _ptr(b), ctypes.byref(line))
+    if rc != 0:
+        raise ObjThrows(int(line.value))
+    tri = np.empty((n.value, 12), dtype=np.float32)
+    rc = lib().oracle_parse_obj(data, len(data), _ptr(tri), n.value, ctypes.byref(n), _ptr(b),
+                                ctypes.byref(line))
+    assert rc == 0
+    return tri, b

@@ -36,6 +36,13 @@ int main(void) {
     printf("sizeof_server_stats %zu\n", sizeof(lvbh_server_stats));
     printf("off_max_batch_seen %zu\n", offsetof(lvbh_server_stats, max_batch_seen));
     {
+        const float *tri = NULL;
+        uint32_t n = 0;
+        double b6[6];
+        uint64_t line = 7;
+        printf("parse_obj_null_ctx %d\n", lvbh_parse_obj(NULL, "v 0 0 0\n", 8, LVBH_INPUT_HOST, &tri, &n, b6, &line, NULL));
+    }
+    {
         uint64_t t = 0;
         printf("server_create_null %d\n", lvbh_server_create(NULL, NULL));
         printf("submit_null %d\n", lvbh_submit(NULL, NULL, 0, NULL, 0, &t));

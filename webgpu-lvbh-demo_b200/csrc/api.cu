@@ -110,6 +110,7 @@ struct lvbh_ctx {
     // pinned readback of the control block head
     uint32_t *host_ctl = nullptr;
     uint32_t *trace_counter = nullptr;  // ray counter of the persistent traversal
+    ObjScratch obj;                     // OBJ ingest buffers (the parsed soup among them)
     cudaEvent_t ev[LVBH_NUM_STAGES + 1] = {};
     bool ev_valid = false;
     // cached graph of the last build shape
@@ -570,6 +571,7 @@ void lvbh_destroy(lvbh_ctx *ctx) {
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     if (ctx->host_ctl) cudaFreeHost(ctx->host_ctl);
     if (ctx->trace_counter) cudaFree(ctx->trace_counter);
+    obj_free(ctx->obj);
     cudaGetLastError();
     delete ctx;
 }
@@ -894,6 +896,20 @@ int lvbh_trace(lvbh_ctx *ctx, const void *nodes, const void *tris, uint32_t num_
     LVBH_CUDA(ctx, cudaGetLastError());
     LVBH_CUDA(ctx, cudaStreamSynchronize(s));
     return LVBH_OK;
+}
+
+int lvbh_parse_obj(lvbh_ctx *ctx, const char *text, uint64_t bytes, uint32_t flags,
+                   const float **tri_out, uint32_t *num_tris, double *bounds6, uint64_t *err_line,
+                   void *stream) {
+    if (!ctx) return LVBH_EINVAL;
+    if (!tri_out || !num_tris || !bounds6 || !err_line) return fail(ctx, LVBH_EINVAL, "NULL output pointer");
+    *err_line = 0;
+    if (bytes && !text) return fail(ctx, LVBH_EINVAL, "text is NULL");
+    if (bytes > LVBH_OBJ_MAX_BYTES) return fail(ctx, LVBH_EINVAL, "text exceeds LVBH_OBJ_MAX_BYTES");
+    DeviceGuard g(ctx->device);
+    if (ctx->pending) LVBH_CUDA(ctx, cudaStreamSynchronize(ctx->last_stream));
+    return obj_parse(ctx->obj, text, bytes, (flags & LVBH_INPUT_HOST) != 0, tri_out, num_tris, bounds6,
+                     err_line, static_cast<cudaStream_t>(stream), ctx->err);
 }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 struct lvbh_ctx;
@@ -157,5 +158,22 @@ void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t 
 void launch_trace(const float4 *nodes, const float4 *tris, uint32_t n, const float4 *rays,
                   uint32_t num_rays, int32_t *hit_prim, float *hit_t, uint32_t *max_stack,
                   uint32_t *counter, cudaStream_t s);
+
+// OBJ ingest (obj.cu): device memory of one parse, grown on demand and held by the context.
+struct ObjScratch {
+    void *text = nullptr;  // staged host text, newline counts, control block
+    size_t text_bytes = 0;
+    void *lines = nullptr;  // per-line arrays
+    size_t lines_bytes = 0;
+    void *soup = nullptr;  // model-0 vertices (double) and the triangle soup
+    size_t soup_bytes = 0;
+    void *host = nullptr;  // pinned readback
+};
+// OBJ text -> triangle soup + bounds (lvbh_parse_obj).  *err_line: the 1-based line whose
+// statement the parser rejects, 0 for a failure found after parsing (LVBH_EINVAL for both).
+int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text,
+              const float **tri_out, uint32_t *num_tris, double *bounds6, uint64_t *err_line,
+              cudaStream_t s, std::string &err);
+void obj_free(ObjScratch &sc);
 
 }  // namespace lvbh

@@ -1,0 +1,863 @@
+// obj.cu - OBJ text -> the build's 48-byte triangle soup and MODEL_BOUNDS, on the device.
+//
+// Replaces parseObj(file) (scripts/obj/parse-obj.js:3-88) and the OBJFile parser it calls
+// (scripts/obj/obj-file-parser.js:19-193), which the demo runs on the main thread before every
+// build (main.js:72-73).  The text is parsed in parallel, one thread per line, with the
+// reference's semantics:
+//   * lines split on '\n' and cut at the first '#'; tokens separated by runs of JavaScript
+//     whitespace (`\s`: ASCII \t \n \v \f \r and space, and the UTF-8 forms of U+00A0, U+1680,
+//     U+2000-200A, U+2028, U+2029, U+202F, U+205F, U+3000, U+FEFF); keyword lower-cased;
+//   * the statements the parser checks fail the parse where the reference throws: g and s with
+//     other than one argument (:101-105, :196-201), l with fewer than two vertices or a vertex
+//     of more than two '/'-parts (:132-151), f with fewer than three vertices, a vertex of more
+//     than three parts or a vertex index parseInt()s to 0 (:153-186);
+//   * only model 0 counts (parse-obj.js:17-60): the default model when a v / vt / vn / l / f
+//     statement precedes the first `o` (_currentModel, :82-91), else the model the first `o`
+//     opens; negative face indices count back from that model's vertices so far, and every
+//     index must name one of its vertices (else the reference's array read throws);
+//   * vertices are parsed as JavaScript's parseFloat does (longest decimal prefix, correctly
+//     rounded), exactly on the device for every decimal exponent within 10^+-27 (see
+//     dec_to_double); the rare rest is re-parsed on the host by the C library's correctly
+//     rounded strtod;
+//   * faces are fan-triangulated from their first vertex, y and z swapped, stored as float32
+//     (round to nearest even, the Float32Array of build-bvh.js:14-21), pad 3.1415; bounds are
+//     Math.min / Math.max over the faces' vertices in double (NaN absorbs, -0 below +0) from
+//     +-1e30, and two floor triangles lie at z_min + .01 (parse-obj.js:62-76).
+// Passes: newlines per 4 KB chunk -> scan -> line starts; per-line classify and check; the
+// model-0 line range; a 64-bit scan of (vertex count | triangle count) over it; vertices;
+// faces -> soup + bounds.  Each pass streams the text from HBM once; its bound is HBM.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "lvbh.h"
+#include "lvbh_internal.h"
+
+namespace lvbh {
+
+namespace {
+
+typedef unsigned __int128 u128;
+
+constexpr int kT = 256;
+constexpr int kChunk = 4096;  // text bytes per newline-count block (16 per thread)
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kT * kScanItems;
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+enum : uint8_t { LT_NONE = 0, LT_O, LT_G, LT_V, LT_VT, LT_VN, LT_L, LT_S, LT_F };
+
+// Device state of one parse (set to its initial values by the host before the passes).
+struct ObjCtl {
+    uint32_t err_line;    // smallest 0-based line whose statement throws (kNone: none)
+    uint32_t first_o;     // first `o` line (kNone: none)
+    uint32_t second_o;    // the next `o` line after it
+    uint32_t first_need;  // first v / vt / vn / l / f line (creates the default model)
+    uint32_t bad_index;   // a model-0 face names no vertex
+    uint32_t num_hard;    // vertex lines left to the host parser
+    uint32_t newlines;
+    uint32_t pad;
+    unsigned long long totals;  // model-0 vertices (low 32 bits) and triangles (high 32 bits)
+    unsigned long long bmin[3], bmax[3];  // ordered doubles (ord64)
+    uint32_t nan_min[3], nan_max[3];
+};
+
+// A vertex line the device leaves to the host: its text [start, end) and vertex rank.  The same
+// slot then carries the host's exact coordinates back (HardFix).
+struct HardLine {
+    unsigned long long start, end;
+    uint32_t vi, pad0;
+    uint32_t pad1, pad2;
+};
+struct HardFix {
+    double xyz[3];
+    uint32_t vi, pad;
+};
+static_assert(sizeof(HardLine) == sizeof(HardFix), "hard-line slot");
+
+// Length in bytes of the JavaScript whitespace character at s[i] (0: none), the line ending
+// at e.  A UTF-8 lead byte always starts a new character for the decoder of readAsText (an
+// unfinished sequence before it becomes U+FFFD), so checking every byte position finds exactly
+// the whitespace characters the decoded string holds.
+__host__ __device__ __forceinline__ int ws_len(const uint8_t *s, uint64_t i, uint64_t e) {
+    const uint8_t c = s[i];
+    if (c == ' ' || (c >= 9 && c <= 13)) return 1;
+    if (c < 0xC2) return 0;
+    if (c == 0xC2) return (i + 1 < e && s[i + 1] == 0xA0) ? 2 : 0;
+    if (i + 2 >= e) return 0;
+    const uint8_t c1 = s[i + 1], c2 = s[i + 2];
+    switch (c) {
+        case 0xE1: return (c1 == 0x9A && c2 == 0x80) ? 3 : 0;
+        case 0xE2:
+            if (c1 == 0x80) return ((c2 >= 0x80 && c2 <= 0x8A) || c2 == 0xA8 || c2 == 0xA9 || c2 == 0xAF) ? 3 : 0;
+            return (c1 == 0x81 && c2 == 0x9F) ? 3 : 0;
+        case 0xE3: return (c1 == 0x80 && c2 == 0x80) ? 3 : 0;
+        case 0xEF: return (c1 == 0xBB && c2 == 0xBF) ? 3 : 0;
+    }
+    return 0;
+}
+
+// Next token of s[i, e): false when none is left; else [a, b).
+__host__ __device__ __forceinline__ bool next_token(const uint8_t *s, uint64_t &i, uint64_t e,
+                                                    uint64_t &a, uint64_t &b) {
+    while (i < e) {
+        const int w = ws_len(s, i, e);
+        if (!w) break;
+        i += w;
+    }
+    if (i >= e) return false;
+    a = i;
+    while (i < e && !ws_len(s, i, e)) ++i;
+    b = i;
+    return true;
+}
+
+// Order-preserving map of doubles (-0 below +0) for 64-bit atomic min / max.
+__device__ __forceinline__ unsigned long long ord64(double d) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(d);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+__constant__ double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,
+                                  1e8,  1e9,  1e10, 1e11, 1e12, 1e13, 1e14, 1e15,
+                                  1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+__device__ __forceinline__ int bitlen128(u128 x) {
+    const unsigned long long hi = (unsigned long long)(x >> 64), lo = (unsigned long long)x;
+    return hi ? 128 - __clzll((long long)hi) : 64 - __clzll((long long)lo);
+}
+
+// (x + f) * 2^e2 rounded to the nearest double, ties to even; x has more than 53 bits or
+// f == 0, f in [0, 1) is represented by `sticky` = (f != 0).  The result is a normal double.
+__device__ double round_scaled(u128 x, int e2, bool sticky) {
+    const int nb = bitlen128(x);
+    unsigned long long mant;
+    int shift = 0;
+    if (nb <= 53) {
+        mant = (unsigned long long)x;
+    } else {
+        shift = nb - 53;
+        mant = (unsigned long long)(x >> shift);
+        const u128 rem = x & (((u128)1 << shift) - 1), half = (u128)1 << (shift - 1);
+        if (rem > half || (rem == half && (sticky || (mant & 1)))) ++mant;
+        if (mant == (1ull << 53)) { mant >>= 1; ++shift; }
+    }
+    const double p2 = __longlong_as_double((long long)(e2 + shift + 1023) << 52);
+    return __dmul_rn(__ull2double_rn(mant), p2);  // both exact
+}
+
+// w * 10^q correctly rounded (w >= 1): false when q lies outside the device's exact range.
+// |q| <= 22 with w <= 2^53 is one IEEE multiply or divide of exact doubles (Clinger, "How to
+// read floating point numbers accurately", 1990).  Otherwise, for |q| <= 27 (5^27 < 2^63): the
+// exact integer w * 5^q scaled by 2^q, or the 128-bit quotient (w * 2^(64 + lz)) / 5^-q with
+// its remainder as the sticky bit, rounded once.
+__device__ bool dec_to_double(unsigned long long w, int q, double &out) {
+    if (w <= (1ull << 53) && q >= -22 && q <= 22) {
+        out = q >= 0 ? __dmul_rn((double)w, kPow10[q]) : __ddiv_rn((double)w, kPow10[-q]);
+        return true;
+    }
+    if (q < -27 || q > 27) return false;
+    unsigned long long p5 = 1;
+    for (int k = 0; k < (q >= 0 ? q : -q); ++k) p5 *= 5;
+    if (q >= 0) {
+        out = round_scaled((u128)w * p5, q, false);
+        return true;
+    }
+    const int lz = __clzll((long long)w);
+    const u128 n = (u128)(w << lz) << 64;
+    const u128 quo = n / p5;
+    const u128 rem = n - quo * p5;
+    out = round_scaled(quo, q - 64 - lz, rem != 0);  // 2^-(64 + lz) * 2^q * 5^q = 10^q / 2^(64+lz)
+    return true;
+}
+
+// parseFloat of the whitespace-free token s[p, q): true with the double in out, false when the
+// host has to parse it (decimal exponent beyond +-27, or more than 19 significant digits whose
+// dropped tail could change the rounding).
+__device__ bool parse_float(const uint8_t *__restrict__ s, uint64_t p, uint64_t q, double &out) {
+    uint64_t i = p;
+    bool neg = false;
+    if (i < q && (s[i] == '+' || s[i] == '-')) { neg = s[i] == '-'; ++i; }
+    if (q - i >= 8 && s[i] == 'I' && s[i + 1] == 'n' && s[i + 2] == 'f' && s[i + 3] == 'i' &&
+        s[i + 4] == 'n' && s[i + 5] == 'i' && s[i + 6] == 't' && s[i + 7] == 'y') {
+        out = neg ? -INFINITY : INFINITY;
+        return true;
+    }
+    unsigned long long m = 0;
+    int nd = 0;
+    long long dexp = 0;
+    bool any = false, inexact = false;
+    while (i < q && s[i] >= '0' && s[i] <= '9') {
+        const int d = s[i] - '0';
+        any = true;
+        if (nd < 19) {
+            if (m || d) { m = m * 10 + d; ++nd; }
+        } else {
+            ++dexp;
+            inexact |= d != 0;
+        }
+        ++i;
+    }
+    if (i < q && s[i] == '.') {
+        ++i;
+        while (i < q && s[i] >= '0' && s[i] <= '9') {
+            const int d = s[i] - '0';
+            any = true;
+            if (nd < 19) {
+                if (m || d) { m = m * 10 + d; ++nd; }
+                --dexp;
+            } else {
+                inexact |= d != 0;
+            }
+            ++i;
+        }
+    }
+    if (!any) {
+        out = NAN;
+        return true;
+    }
+    long long e10 = 0;
+    if (i < q && (s[i] == 'e' || s[i] == 'E')) {
+        uint64_t j = i + 1;
+        bool eneg = false;
+        if (j < q && (s[j] == '+' || s[j] == '-')) { eneg = s[j] == '-'; ++j; }
+        long long ev = 0;
+        int ed = 0;
+        while (j < q && s[j] >= '0' && s[j] <= '9') {
+            if (ev < 1000000000ll) ev = ev * 10 + (s[j] - '0');
+            ++j;
+            ++ed;
+        }
+        if (ed) e10 = eneg ? -ev : ev;
+    }
+    if (m == 0) {
+        out = neg ? -0.0 : 0.0;
+        return true;
+    }
+    const long long e = e10 + dexp;
+    if (e < -27 || e > 27) return false;
+    double v;
+    if (!dec_to_double(m, (int)e, v)) return false;
+    if (inexact) {  // the value lies strictly between m * 10^e and (m + 1) * 10^e
+        double hi;
+        if (!dec_to_double(m + 1, (int)e, hi) || hi != v) return false;
+    }
+    out = neg ? -v : v;
+    return true;
+}
+
+// parseInt (radix undefined) of s[p, q): sign, optional 0x / 0X, longest digit prefix; NaN
+// when there is no digit.
+__device__ double parse_int(const uint8_t *__restrict__ s, uint64_t p, uint64_t q) {
+    uint64_t i = p;
+    bool neg = false;
+    if (i < q && (s[i] == '+' || s[i] == '-')) { neg = s[i] == '-'; ++i; }
+    int radix = 10;
+    if (i + 1 < q && s[i] == '0' && (s[i + 1] == 'x' || s[i + 1] == 'X')) { radix = 16; i += 2; }
+    double v = 0.0;
+    int digits = 0;
+    for (; i < q; ++i) {
+        const uint8_t c = s[i];
+        int d;
+        if (c >= '0' && c <= '9') d = c - '0';
+        else if (radix == 16 && c >= 'a' && c <= 'f') d = c - 'a' + 10;
+        else if (radix == 16 && c >= 'A' && c <= 'F') d = c - 'A' + 10;
+        else break;
+        v = __dadd_rn(__dmul_rn(v, (double)radix), (double)d);  // exact below 2^53
+        ++digits;
+    }
+    if (!digits) return NAN;
+    return neg ? -v : v;
+}
+
+// Line l: its bytes [p, e) after the comment cut.
+__device__ __forceinline__ void line_span(const uint8_t *s, uint64_t n, const uint64_t *line_start,
+                                          uint32_t L, uint32_t l, uint64_t &p, uint64_t &e) {
+    p = line_start[l];
+    const uint64_t q = l + 1 < L ? line_start[l + 1] - 1 : n;
+    e = q;
+    for (uint64_t i = p; i < q; ++i)
+        if (s[i] == '#') { e = i; break; }
+}
+
+__device__ __forceinline__ uint8_t lower(uint8_t c) { return (c >= 'A' && c <= 'Z') ? c + 32 : c; }
+
+__device__ uint8_t keyword(const uint8_t *s, uint64_t a, uint64_t b) {
+    const uint64_t n = b - a;
+    if (n == 1) {
+        switch (lower(s[a])) {
+            case 'o': return LT_O;
+            case 'g': return LT_G;
+            case 'v': return LT_V;
+            case 'l': return LT_L;
+            case 's': return LT_S;
+            case 'f': return LT_F;
+        }
+    } else if (n == 2 && lower(s[a]) == 'v') {
+        if (lower(s[a + 1]) == 't') return LT_VT;
+        if (lower(s[a + 1]) == 'n') return LT_VN;
+    }
+    return LT_NONE;
+}
+
+// Exclusive scan of one value per thread across the block (blockDim.x a multiple of 32).
+template <typename U>
+__device__ __forceinline__ U block_scan(U x, U *s_warp, U *total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    U incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const U y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    U off = 0, all = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+        off += i < warp ? s_warp[i] : (U)0;
+        all += s_warp[i];
+    }
+    __syncthreads();
+    if (total) *total = all;
+    return off + incl - x;
+}
+
+// Smallest value over the warp into *dst (atomically), skipping kNone and values that cannot
+// lower it, so that one word shared by the grid sees few atomics.
+__device__ __forceinline__ void warp_min_into(uint32_t v, uint32_t *dst) {
+    v = __reduce_min_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31) == 0 && v != kNone && v < *(volatile uint32_t *)dst) atomicMin(dst, v);
+}
+
+// Newlines per kChunk bytes.
+__global__ void __launch_bounds__(kT) k_nl_count(const uint8_t *__restrict__ s, uint64_t n,
+                                                 uint32_t *__restrict__ cnt) {
+    __shared__ uint32_t w[kT / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * kChunk + threadIdx.x * 16;
+    uint32_t c = 0;
+    if (base + 16 <= n) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(s + base);
+        const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t x = words[k] ^ 0x0A0A0A0Au;  // zero bytes where '\n' was
+            c += __popc(~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu));
+        }
+    } else {
+        for (int k = 0; k < 16; ++k) c += (base + k < n && s[base + k] == '\n') ? 1u : 0u;
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int i = 0; i < kT / 32; ++i) t += w[i];
+        cnt[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of v[0, n) in place by one block; *total = the sum.
+template <typename U>
+__global__ void __launch_bounds__(1024) k_scan_small(U *v, uint32_t n, U *total) {
+    __shared__ U s_warp[32];
+    U carry = 0;
+    for (uint32_t b = 0; b < n; b += 1024) {
+        const uint32_t i = b + threadIdx.x;
+        const U x = i < n ? v[i] : (U)0;
+        U all;
+        const U ex = block_scan<U>(x, s_warp, &all);
+        if (i < n) v[i] = carry + ex;
+        carry += all;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// Line starts: the newline at byte k (rank r over the text) starts line r + 1 at k + 1.
+__global__ void __launch_bounds__(kT) k_nl_write(const uint8_t *__restrict__ s, uint64_t n,
+                                                 const uint32_t *__restrict__ base,
+                                                 uint64_t *__restrict__ line_start) {
+    __shared__ uint32_t s_warp[kT / 32];
+    const uint64_t p = (uint64_t)blockIdx.x * kChunk + threadIdx.x * 16;
+    uint8_t b[16];
+    if (p + 16 <= n) {
+        *reinterpret_cast<uint4 *>(b) = *reinterpret_cast<const uint4 *>(s + p);
+    } else {
+        for (int k = 0; k < 16; ++k) b[k] = p + k < n ? s[p + k] : 0;
+    }
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) c += b[k] == '\n';
+    uint32_t r = base[blockIdx.x] + block_scan<uint32_t>(c, s_warp, nullptr);
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        if (b[k] == '\n') line_start[++r] = p + k + 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) line_start[0] = 0;
+}
+
+// Per line: statement type, the checks the reference's parser makes, the triangles a face
+// fans into, and the first `o` and model-creating lines.
+__global__ void __launch_bounds__(kT) k_lines(const uint8_t *__restrict__ s, uint64_t n,
+                                              const uint64_t *__restrict__ line_start, uint32_t L,
+                                              uint8_t *__restrict__ type, uint32_t *__restrict__ fans,
+                                              ObjCtl *__restrict__ ctl) {
+    const uint32_t l = blockIdx.x * kT + threadIdx.x;
+    uint8_t t = LT_NONE;
+    bool bad = false;
+    if (l < L) {
+        uint64_t p, e;
+        line_span(s, n, line_start, L, l, p, e);
+        uint64_t i = p, a = 0, b = 0;
+        if (next_token(s, i, e, a, b)) t = keyword(s, a, b);
+        uint32_t ntok = 1, fan = 0;
+        if (t != LT_NONE) {
+            while (next_token(s, i, e, a, b)) {
+                ++ntok;
+                if (t == LT_L || t == LT_F) {
+                    int slashes = 0;
+                    uint64_t first_end = b;
+                    for (uint64_t k = a; k < b; ++k)
+                        if (s[k] == '/') {
+                            if (!slashes) first_end = k;
+                            ++slashes;
+                        }
+                    if (t == LT_L && slashes > 1) bad = true;
+                    if (t == LT_F && (slashes > 2 || parse_int(s, a, first_end) == 0.0)) bad = true;
+                }
+            }
+            if ((t == LT_G || t == LT_S) && ntok != 2) bad = true;
+            if (t == LT_L && ntok < 3) bad = true;
+            if (t == LT_F) {
+                if (ntok < 4) bad = true;
+                else fan = ntok - 3;
+            }
+        }
+        type[l] = t;
+        fans[l] = fan;
+    }
+    warp_min_into(bad ? l : kNone, &ctl->err_line);
+    warp_min_into(t == LT_O ? l : kNone, &ctl->first_o);
+    const bool need = t == LT_V || t == LT_VT || t == LT_VN || t == LT_L || t == LT_F;
+    warp_min_into(need ? l : kNone, &ctl->first_need);
+}
+
+// The first `o` line after line fo.
+__global__ void __launch_bounds__(kT) k_second_o(const uint8_t *__restrict__ type, uint32_t L,
+                                                 uint32_t fo, ObjCtl *__restrict__ ctl) {
+    const uint32_t l = blockIdx.x * kT + threadIdx.x;
+    warp_min_into(l < L && l > fo && type[l] == LT_O ? l : kNone, &ctl->second_o);
+}
+
+// Packed count of a model-0 line: one vertex (low 32 bits) or a face's triangles (high).
+__device__ __forceinline__ unsigned long long line_count(const uint8_t *type, const uint32_t *fans,
+                                                         uint32_t l) {
+    const uint8_t t = type[l];
+    return t == LT_V ? 1ull : t == LT_F ? (unsigned long long)fans[l] << 32 : 0ull;
+}
+
+// Tile sums of the packed counts of lines [a, a + m).
+__global__ void __launch_bounds__(kT) k_scan_up(const uint8_t *__restrict__ type,
+                                                const uint32_t *__restrict__ fans, uint32_t a,
+                                                uint32_t m, unsigned long long *__restrict__ sums) {
+    __shared__ unsigned long long s_warp[kT / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    unsigned long long t = 0;
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < m) t += line_count(type, fans, a + (uint32_t)(base + k));
+    unsigned long long all;
+    block_scan<unsigned long long>(t, s_warp, &all);
+    if (threadIdx.x == 0) sums[blockIdx.x] = all;
+}
+
+// pre[i]: exclusive prefix of the packed counts for line a + i.
+__global__ void __launch_bounds__(kT) k_scan_down(const uint8_t *__restrict__ type,
+                                                  const uint32_t *__restrict__ fans, uint32_t a,
+                                                  uint32_t m, const unsigned long long *__restrict__ sums,
+                                                  unsigned long long *__restrict__ pre) {
+    __shared__ unsigned long long s_warp[kT / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    unsigned long long x[kScanItems], t = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        x[k] = base + k < m ? line_count(type, fans, a + (uint32_t)(base + k)) : 0ull;
+        t += x[k];
+    }
+    unsigned long long run = sums[blockIdx.x] + block_scan<unsigned long long>(t, s_warp, nullptr);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < m) pre[base + k] = run;
+        run += x[k];
+    }
+}
+
+// Model-0 vertex lines -> doubles at their rank; numbers outside the device's exact range are
+// listed for the host.
+__global__ void __launch_bounds__(kT) k_vertices(const uint8_t *__restrict__ s, uint64_t n,
+                                                 const uint64_t *__restrict__ line_start, uint32_t L,
+                                                 const uint8_t *__restrict__ type, uint32_t a, uint32_t m,
+                                                 const unsigned long long *__restrict__ pre,
+                                                 double *__restrict__ verts, HardLine *__restrict__ hard,
+                                                 ObjCtl *__restrict__ ctl) {
+    const uint32_t i = blockIdx.x * kT + threadIdx.x;
+    if (i >= m || type[a + i] != LT_V) return;
+    const uint32_t l = a + i;
+    uint64_t p, e;
+    line_span(s, n, line_start, L, l, p, e);
+    uint64_t k = p, ta = 0, tb = 0;
+    next_token(s, k, e, ta, tb);  // the keyword
+    double xyz[3] = {0.0, 0.0, 0.0};
+    bool ok = true;
+    for (int c = 0; c < 3; ++c) {
+        if (!next_token(s, k, e, ta, tb)) break;
+        ok &= parse_float(s, ta, tb, xyz[c]);
+    }
+    const uint32_t vi = (uint32_t)(pre[i] & 0xFFFFFFFFull);
+    verts[3ull * vi] = xyz[0];
+    verts[3ull * vi + 1] = xyz[1];
+    verts[3ull * vi + 2] = xyz[2];
+    if (!ok) {
+        const uint32_t h = atomicAdd(&ctl->num_hard, 1u);
+        hard[h] = HardLine{p, e, vi, 0u, 0u, 0u};
+    }
+}
+
+__global__ void __launch_bounds__(kT) k_patch(const HardFix *__restrict__ fix, uint32_t count,
+                                              double *__restrict__ verts) {
+    const uint32_t i = blockIdx.x * kT + threadIdx.x;
+    if (i >= count) return;
+    const HardFix f = fix[i];
+    verts[3ull * f.vi] = f.xyz[0];
+    verts[3ull * f.vi + 1] = f.xyz[1];
+    verts[3ull * f.vi + 2] = f.xyz[2];
+}
+
+// float32 of a coordinate as Float32Array stores it (NaN as the quiet NaN 0x7FC00000).
+__device__ __forceinline__ float to_f32(double d) {
+    return isnan(d) ? __int_as_float(0x7FC00000) : __double2float_rn(d);
+}
+
+// Model-0 faces -> fan triangles (y and z swapped, float32, pad 3.1415) and the bounds.
+__global__ void __launch_bounds__(kT) k_faces(const uint8_t *__restrict__ s, uint64_t n,
+                                              const uint64_t *__restrict__ line_start, uint32_t L,
+                                              const uint8_t *__restrict__ type, uint32_t a, uint32_t m,
+                                              const unsigned long long *__restrict__ pre, uint32_t nverts,
+                                              const double *__restrict__ verts, float4 *__restrict__ tri,
+                                              ObjCtl *__restrict__ ctl) {
+    const uint32_t i = blockIdx.x * kT + threadIdx.x;
+    unsigned long long mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0ull, 0ull, 0ull};
+    bool nan_seen[3] = {false, false, false};
+    if (i < m && type[a + i] == LT_F) {
+        const uint32_t l = a + i;
+        uint64_t p, e;
+        line_span(s, n, line_start, L, l, p, e);
+        const double before = (double)(uint32_t)(pre[i] & 0xFFFFFFFFull);  // model-0 vertices so far
+        unsigned long long out = pre[i] >> 32;
+        uint64_t k = p, ta = 0, tb = 0;
+        next_token(s, k, e, ta, tb);  // the keyword
+        const float pad = __double2float_rn(3.1415);
+        float4 r = make_float4(0.f, 0.f, 0.f, pad), prev = r;
+        int nv = 0;
+        bool bad = false;
+        while (next_token(s, k, e, ta, tb)) {
+            uint64_t fe = tb;
+            for (uint64_t j = ta; j < tb; ++j)
+                if (s[j] == '/') { fe = j; break; }
+            double idx = parse_int(s, ta, fe);
+            if (idx < 0.0) idx = __dadd_rn(__dadd_rn(before, 1.0), idx);
+            const double vk = __dsub_rn(idx, 1.0);
+            if (!(vk >= 0.0) || vk != floor(vk) || vk >= (double)nverts) { bad = true; break; }
+            const double *v = verts + 3ull * (unsigned long long)vk;
+            const double c[3] = {v[0], v[2], v[1]};  // x, then the file's z as y and y as z
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+                if (isnan(c[ax])) { nan_seen[ax] = true; continue; }
+                const unsigned long long o = ord64(c[ax]);
+                mn[ax] = o < mn[ax] ? o : mn[ax];
+                mx[ax] = o > mx[ax] ? o : mx[ax];
+            }
+            const float4 cur = make_float4(to_f32(c[0]), to_f32(c[1]), to_f32(c[2]), pad);
+            if (nv == 0) {
+                r = cur;
+            } else if (nv >= 2) {
+                float4 *o = tri + 3ull * out;
+                o[0] = r;
+                o[1] = prev;
+                o[2] = cur;
+                ++out;
+            }
+            prev = cur;
+            ++nv;
+        }
+        if (bad) atomicOr(&ctl->bad_index, 1u);
+    }
+    __shared__ unsigned long long s_mn[3][kT / 32], s_mx[3][kT / 32];
+    __shared__ int s_nan[3][kT / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        unsigned long long lo = mn[ax], hi = mx[ax];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long lo2 = __shfl_xor_sync(0xFFFFFFFFu, lo, o);
+            const unsigned long long hi2 = __shfl_xor_sync(0xFFFFFFFFu, hi, o);
+            lo = lo2 < lo ? lo2 : lo;
+            hi = hi2 > hi ? hi2 : hi;
+        }
+        const int nan_any = __any_sync(0xFFFFFFFFu, nan_seen[ax]);
+        if (lane == 0) { s_mn[ax][warp] = lo; s_mx[ax][warp] = hi; s_nan[ax][warp] = nan_any; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        const int ax = threadIdx.x;
+        unsigned long long lo = ~0ull, hi = 0ull;
+        int nan_any = 0;
+        for (int w = 0; w < kT / 32; ++w) {
+            lo = s_mn[ax][w] < lo ? s_mn[ax][w] : lo;
+            hi = s_mx[ax][w] > hi ? s_mx[ax][w] : hi;
+            nan_any |= s_nan[ax][w];
+        }
+        if (lo != ~0ull && lo < *(volatile unsigned long long *)&ctl->bmin[ax]) atomicMin(&ctl->bmin[ax], lo);
+        if (hi != 0ull && hi > *(volatile unsigned long long *)&ctl->bmax[ax]) atomicMax(&ctl->bmax[ax], hi);
+        if (nan_any && !*(volatile uint32_t *)&ctl->nan_min[ax]) {
+            atomicOr(&ctl->nan_min[ax], 1u);
+            atomicOr(&ctl->nan_max[ax], 1u);
+        }
+    }
+}
+
+// parseFloat of a whitespace-free token on the host, for the numbers the device leaves to it:
+// the C library's correctly rounded strtod on the longest decimal prefix.
+double host_parse_float(const uint8_t *t, size_t len) {
+    size_t i = 0;
+    bool neg = false;
+    if (i < len && (t[i] == '+' || t[i] == '-')) { neg = t[i] == '-'; ++i; }
+    if (len - i >= 8 && std::memcmp(t + i, "Infinity", 8) == 0) return neg ? -INFINITY : INFINITY;
+    const size_t st = i;
+    size_t digits = 0;
+    while (i < len && t[i] >= '0' && t[i] <= '9') { ++i; ++digits; }
+    if (i < len && t[i] == '.') {
+        ++i;
+        while (i < len && t[i] >= '0' && t[i] <= '9') { ++i; ++digits; }
+    }
+    if (!digits) return NAN;
+    size_t end = i;
+    if (i < len && (t[i] == 'e' || t[i] == 'E')) {
+        size_t j = i + 1;
+        if (j < len && (t[j] == '+' || t[j] == '-')) ++j;
+        size_t ed = 0;
+        while (j < len && t[j] >= '0' && t[j] <= '9') { ++j; ++ed; }
+        if (ed) end = j;
+    }
+    const std::string lit(reinterpret_cast<const char *>(t) + st, end - st);
+    const double v = std::strtod(lit.c_str(), nullptr);
+    return neg ? -v : v;
+}
+
+double ord64_inv(unsigned long long o) {
+    const unsigned long long u = (o >> 63) ? (o & 0x7FFFFFFFFFFFFFFFull) : ~o;
+    double d;
+    std::memcpy(&d, &u, 8);
+    return d;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Grow one scratch block to at least `need` bytes (contents are not kept).
+cudaError_t grow(void *&p, size_t &have, size_t need) {
+    if (need <= have) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    have = 0;
+    const cudaError_t e = cudaMalloc(&p, need);
+    if (e == cudaSuccess) have = need;
+    return e;
+}
+
+}  // namespace
+
+int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, const float **tri_out,
+              uint32_t *num_tris, double *bounds6, uint64_t *err_line, cudaStream_t s,
+              std::string &err) {
+    auto cuda = [&](cudaError_t e, const char *what) -> int {
+        if (e == cudaSuccess) return LVBH_OK;
+        cudaGetLastError();
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? LVBH_ENOMEM : LVBH_ECUDA;
+    };
+#define OBJ_CUDA(call, what)                          \
+    do {                                              \
+        if (int rc_ = cuda((call), what)) return rc_; \
+    } while (0)
+    auto reject = [&](uint64_t line, const std::string &msg) {
+        *err_line = line;
+        err = msg;
+        return LVBH_EPARSE;
+    };
+    *err_line = 0;
+    if (!sc.host) OBJ_CUDA(cudaMallocHost(&sc.host, sizeof(ObjCtl) + 256), "cudaMallocHost");
+    ObjCtl *hc = static_cast<ObjCtl *>(sc.host);
+    float *floor_tri = reinterpret_cast<float *>(static_cast<char *>(sc.host) + 256);
+    // text (staged when it is host memory or not 16-byte aligned), control block, newline
+    // counts per chunk
+    const uint32_t chunks = (uint32_t)((bytes + kChunk - 1) / kChunk);
+    const bool stage = host_text || (reinterpret_cast<uintptr_t>(text) & 15u);
+    const size_t text_part = stage ? align256(bytes) : 0;
+    OBJ_CUDA(grow(sc.text, sc.text_bytes, text_part + align256(sizeof(ObjCtl)) + align256((chunks + 1) * 4ull)),
+             "cudaMalloc(obj text)");
+    const uint8_t *d_text = reinterpret_cast<const uint8_t *>(text);
+    char *c = static_cast<char *>(sc.text);
+    if (stage) {
+        if (bytes) OBJ_CUDA(cudaMemcpyAsync(c, text, bytes, host_text ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s),
+                            "cudaMemcpyAsync(text)");
+        d_text = reinterpret_cast<const uint8_t *>(c);
+        c += text_part;
+    }
+    ObjCtl *ctl = reinterpret_cast<ObjCtl *>(c);
+    uint32_t *cnt = reinterpret_cast<uint32_t *>(c + align256(sizeof(ObjCtl)));
+    std::memset(hc, 0, sizeof(ObjCtl));
+    hc->err_line = hc->first_o = hc->second_o = hc->first_need = kNone;
+    for (int a = 0; a < 3; ++a) hc->bmin[a] = ~0ull;
+    OBJ_CUDA(cudaMemcpyAsync(ctl, hc, sizeof(ObjCtl), cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(ctl)");
+    if (chunks) {
+        k_nl_count<<<chunks, kT, 0, s>>>(d_text, bytes, cnt);
+        k_scan_small<uint32_t><<<1, 1024, 0, s>>>(cnt, chunks, &ctl->newlines);
+        OBJ_CUDA(cudaGetLastError(), "k_nl_count");
+        OBJ_CUDA(cudaMemcpyAsync(&hc->newlines, &ctl->newlines, 4, cudaMemcpyDeviceToHost, s), "readback");
+    }
+    OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const uint32_t L = hc->newlines + 1;
+    // per-line arrays: starts, types, fan counts; then (model-0 range only) prefixes
+    const size_t lines_need = align256((L + 1ull) * 8) + align256(L) + align256(L * 4ull) +
+                              align256(L * 8ull) + align256(((L + (uint64_t)kScanTile - 1) / kScanTile + 1) * 8);
+    OBJ_CUDA(grow(sc.lines, sc.lines_bytes, lines_need), "cudaMalloc(obj lines)");
+    char *cl = static_cast<char *>(sc.lines);
+    uint64_t *line_start = reinterpret_cast<uint64_t *>(cl);
+    cl += align256((L + 1ull) * 8);
+    uint8_t *type = reinterpret_cast<uint8_t *>(cl);
+    cl += align256(L);
+    uint32_t *fans = reinterpret_cast<uint32_t *>(cl);
+    cl += align256(L * 4ull);
+    unsigned long long *pre = reinterpret_cast<unsigned long long *>(cl);
+    cl += align256(L * 8ull);
+    unsigned long long *sums = reinterpret_cast<unsigned long long *>(cl);
+    if (chunks) k_nl_write<<<chunks, kT, 0, s>>>(d_text, bytes, cnt, line_start);
+    else OBJ_CUDA(cudaMemsetAsync(line_start, 0, 8, s), "cudaMemsetAsync");
+    const uint32_t lb = (uint32_t)((L + (uint64_t)kT - 1) / kT);
+    k_lines<<<lb, kT, 0, s>>>(d_text, bytes, line_start, L, type, fans, ctl);
+    OBJ_CUDA(cudaGetLastError(), "k_lines");
+    OBJ_CUDA(cudaMemcpyAsync(hc, ctl, sizeof(ObjCtl), cudaMemcpyDeviceToHost, s), "readback");
+    OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (hc->err_line != kNone)
+        return reject(hc->err_line + 1ull, "line " + std::to_string(hc->err_line + 1ull) +
+                                                ": a statement the OBJ parser rejects");
+    // model 0: the default model when a model-creating statement precedes the first `o`, else
+    // the model that `o` opens (up to the next `o`)
+    const uint32_t fo = hc->first_o, fn = hc->first_need;
+    uint32_t m0a, m0b;
+    if (fn != kNone && (fo == kNone || fn < fo)) {
+        m0a = 0;
+        m0b = fo == kNone ? L : fo;
+    } else if (fo != kNone) {
+        k_second_o<<<lb, kT, 0, s>>>(type, L, fo, ctl);
+        OBJ_CUDA(cudaGetLastError(), "k_second_o");
+        OBJ_CUDA(cudaMemcpyAsync(&hc->second_o, &ctl->second_o, 4, cudaMemcpyDeviceToHost, s), "readback");
+        OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        m0a = fo;
+        m0b = hc->second_o == kNone ? L : hc->second_o;
+    } else {
+        return reject(0, "the OBJ text defines no model");
+    }
+    const uint32_t m = m0b - m0a;
+    const uint32_t tiles = (uint32_t)((m + (uint64_t)kScanTile - 1) / kScanTile);
+    const uint32_t mb = (uint32_t)((m + (uint64_t)kT - 1) / kT);
+    k_scan_up<<<tiles, kT, 0, s>>>(type, fans, m0a, m, sums);
+    k_scan_small<unsigned long long><<<1, 1024, 0, s>>>(sums, tiles, &ctl->totals);
+    k_scan_down<<<tiles, kT, 0, s>>>(type, fans, m0a, m, sums, pre);
+    OBJ_CUDA(cudaGetLastError(), "k_scan");
+    OBJ_CUDA(cudaMemcpyAsync(&hc->totals, &ctl->totals, 8, cudaMemcpyDeviceToHost, s), "readback");
+    OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    const uint32_t nverts = (uint32_t)(hc->totals & 0xFFFFFFFFull);
+    const uint64_t nfan = hc->totals >> 32;
+    if (nfan + 2 > LVBH_MAX_TRIS) return reject(0, "the OBJ text makes more than LVBH_MAX_TRIS triangles");
+    const uint32_t ntri = (uint32_t)nfan + 2;
+    // the soup first (16-byte aligned), then the vertices and the hard-line slots
+    const size_t tbytes = align256(ntri * 48ull), vbytes = align256(nverts * 24ull);
+    OBJ_CUDA(grow(sc.soup, sc.soup_bytes, tbytes + vbytes + align256(nverts * (size_t)sizeof(HardLine))),
+             "cudaMalloc(obj soup)");
+    float4 *tri = static_cast<float4 *>(sc.soup);
+    double *verts = reinterpret_cast<double *>(static_cast<char *>(sc.soup) + tbytes);
+    HardLine *hard = reinterpret_cast<HardLine *>(static_cast<char *>(sc.soup) + tbytes + vbytes);
+    if (nverts) {
+        k_vertices<<<mb, kT, 0, s>>>(d_text, bytes, line_start, L, type, m0a, m, pre, verts, hard, ctl);
+        OBJ_CUDA(cudaGetLastError(), "k_vertices");
+        OBJ_CUDA(cudaMemcpyAsync(&hc->num_hard, &ctl->num_hard, 4, cudaMemcpyDeviceToHost, s), "readback");
+        OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    }
+    // numbers outside the device's exact range: the host parses their lines
+    const uint32_t nh = nverts ? hc->num_hard : 0;
+    if (nh) {
+        std::vector<HardLine> hl(nh);
+        OBJ_CUDA(cudaMemcpyAsync(hl.data(), hard, nh * sizeof(HardLine), cudaMemcpyDeviceToHost, s), "readback");
+        OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        std::vector<HardFix> fix(nh);
+        std::vector<uint8_t> buf;
+        for (uint32_t h = 0; h < nh; ++h) {
+            const uint64_t len = hl[h].end - hl[h].start;
+            const uint8_t *ln = reinterpret_cast<const uint8_t *>(text) + hl[h].start;
+            if (!host_text) {
+                buf.resize(len);
+                if (len) OBJ_CUDA(cudaMemcpy(buf.data(), d_text + hl[h].start, len, cudaMemcpyDeviceToHost), "readback");
+                ln = buf.data();
+            }
+            uint64_t k = 0, ta = 0, tb = 0;
+            next_token(ln, k, len, ta, tb);  // the keyword
+            HardFix f{{0.0, 0.0, 0.0}, hl[h].vi, 0u};
+            for (int a = 0; a < 3; ++a) {
+                if (!next_token(ln, k, len, ta, tb)) break;
+                f.xyz[a] = host_parse_float(ln + ta, tb - ta);
+            }
+            fix[h] = f;
+        }
+        HardFix *dfix = reinterpret_cast<HardFix *>(hard);
+        OBJ_CUDA(cudaMemcpyAsync(dfix, fix.data(), nh * sizeof(HardFix), cudaMemcpyHostToDevice, s),
+                 "cudaMemcpyAsync(fix)");
+        k_patch<<<(nh + kT - 1) / kT, kT, 0, s>>>(dfix, nh, verts);
+        OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");  // `fix` is pageable host memory
+    }
+    if (nfan) k_faces<<<mb, kT, 0, s>>>(d_text, bytes, line_start, L, type, m0a, m, pre, nverts, verts, tri, ctl);
+    OBJ_CUDA(cudaGetLastError(), "k_faces");
+    OBJ_CUDA(cudaMemcpyAsync(hc, ctl, sizeof(ObjCtl), cudaMemcpyDeviceToHost, s), "readback");
+    OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (hc->bad_index) return reject(0, "a face of model 0 names a vertex the model does not have");
+    // bounds: Math.min / Math.max from 1e30 / -1e30 over the faces' vertices
+    for (int a = 0; a < 3; ++a) {
+        const double lo = hc->bmin[a] == ~0ull ? 1e30 : ord64_inv(hc->bmin[a]);
+        const double hi = hc->bmax[a] == 0ull ? -1e30 : ord64_inv(hc->bmax[a]);
+        bounds6[a] = hc->nan_min[a] ? NAN : (lo < 1e30 ? lo : 1e30);
+        bounds6[3 + a] = hc->nan_max[a] ? NAN : (hi > -1e30 ? hi : -1e30);
+    }
+    // the floor: two triangles at z_min + .01, 10000 out in x and y (parse-obj.js:62-76)
+    const double fh = bounds6[2] + .01;
+    const float pad = (float)3.1415, h = (float)fh, f = 10000.f;
+    const float ft[24] = {-f, -f, h, pad, f, -f, h, pad, -f, f, h, pad,
+                          f,  -f, h, pad, f, f,  h, pad, -f, f, h, pad};
+    std::memcpy(floor_tri, ft, sizeof ft);
+    OBJ_CUDA(cudaMemcpyAsync(tri + 3ull * nfan, floor_tri, sizeof ft, cudaMemcpyHostToDevice, s),
+             "cudaMemcpyAsync(floor)");
+    OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    *tri_out = reinterpret_cast<const float *>(tri);
+    *num_tris = ntri;
+#undef OBJ_CUDA
+    return LVBH_OK;
+}
+
+void obj_free(ObjScratch &sc) {
+    if (sc.text) cudaFree(sc.text);
+    if (sc.lines) cudaFree(sc.lines);
+    if (sc.soup) cudaFree(sc.soup);
+    if (sc.host) cudaFreeHost(sc.host);
+    sc = ObjScratch{};
+}
+
+}  // namespace lvbh

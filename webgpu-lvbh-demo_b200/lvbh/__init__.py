@@ -28,8 +28,8 @@ from . import _native
 from ._native import (ASYNC, AUTOTUNE, INPUT_HOST, NO_GRAPH, OUT_CALLER, PROFILE, STAGE_NAMES,
                       LvbhError, version)
 
-__all__ = ["initBVHBuild", "BVHBuilder", "BuildResult", "BatchResult", "LvbhError", "version",
-           "trace"]
+__all__ = ["initBVHBuild", "BVHBuilder", "BuildResult", "BatchResult", "LvbhError", "ObjError",
+           "version", "trace", "parseObj"]
 
 
 def _torch():
@@ -341,6 +341,68 @@ class BVHBuilder:
         return prim, t, st
 
 
+    def parse_obj(self, text, stream=None) -> dict:
+        """parseObj(file) (scripts/obj/parse-obj.js:3-88) on the GPU.
+
+        text: the file's bytes (bytes, str as UTF-8, a uint8 numpy array, or a uint8 CUDA
+        tensor).  Returns {"NUM_TRIS", "TRI_ARR", "BOUNDS"} as the reference does, TRI_ARR as a
+        (NUM_TRIS, 12) float32 CUDA tensor (pad 3.1415, floor included) and BOUNDS as
+        {"min": [x, y, z], "max": [x, y, z]} doubles.  Where the reference throws, raises
+        ObjError with .line (1-based; 0 for a failure found after parsing).
+        """
+        torch = _torch()
+        keep = None
+        flags = 0
+        if isinstance(text, torch.Tensor):
+            if not text.is_cuda:
+                text = text.numpy()
+            else:
+                keep = text.contiguous().view(torch.uint8).reshape(-1)
+                ptr, nbytes = keep.data_ptr(), keep.numel()
+        if keep is None:
+            if isinstance(text, str):
+                text = text.encode("utf-8")
+            keep = np.ascontiguousarray(np.frombuffer(text, dtype=np.uint8) if isinstance(text, (bytes, bytearray))
+                                        else np.asarray(text, dtype=np.uint8).reshape(-1))
+            ptr, nbytes = keep.ctypes.data, keep.size
+            flags = INPUT_HOST
+        tri = ctypes.c_void_p()
+        n = ctypes.c_uint32()
+        b6 = (ctypes.c_double * 6)()
+        line = ctypes.c_uint64()
+        rc = _native.lib.lvbh_parse_obj(self._ctx, ctypes.c_void_p(ptr if nbytes else 0), nbytes, flags,
+                                        ctypes.byref(tri), ctypes.byref(n), b6, ctypes.byref(line),
+                                        _stream_ptr(stream, self.device))
+        if rc == _native.EPARSE:
+            raise ObjError(int(line.value), _native.lib.lvbh_last_error(self._ctx).decode())
+        _native.check(self._ctx, rc)
+        soup = _device_floats(tri.value, n.value * 12, self.device).clone().reshape(n.value, 12)
+        return {"NUM_TRIS": n.value, "TRI_ARR": soup,
+                "BOUNDS": {"min": [b6[0], b6[1], b6[2]], "max": [b6[3], b6[4], b6[5]]}}
+
+
+class ObjError(LvbhError):
+    """The OBJ text is one the reference's parser throws on."""
+
+    def __init__(self, line: int, message: str):
+        super().__init__(_native.EPARSE, message)
+        self.line = line
+
+
+class _DeviceArray:
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<f4", "data": (ptr, False),
+                                         "version": 3}
+
+
+def _device_floats(ptr, count, device):
+    """A float32 CUDA tensor viewing `count` floats at device address `ptr` (no copy)."""
+    torch = _torch()
+    if count == 0:
+        return torch.zeros(0, dtype=torch.float32, device=device)
+    return torch.as_tensor(_DeviceArray(ptr, count), device=device)
+
+
 def initBVHBuild(device=0) -> BVHBuilder:  # noqa: N802
     """initBVHBuild(device) -> object with .build (scripts/bvh/build-bvh.js:1-10)."""
     return BVHBuilder(device)
@@ -348,3 +410,8 @@ def initBVHBuild(device=0) -> BVHBuilder:  # noqa: N802
 
 def trace(builder: BVHBuilder, res: BuildResult, rays):
     return builder.trace(res, rays)
+
+
+def parseObj(builder: BVHBuilder, file) -> dict:  # noqa: N802
+    """parseObj(file) (scripts/obj/parse-obj.js:3-88) on the builder's GPU."""
+    return builder.parse_obj(file)

@@ -11,10 +11,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblvbh.so")
 
 # status codes (include/lvbh.h)
-OK, EINVAL, ENOMEM, ETIMEOUT, ECUDA, EBUSY, EDEVICE, ERANGE = 0, 1, 2, 3, 4, 5, 6, 7
+OK, EINVAL, ENOMEM, ETIMEOUT, ECUDA, EBUSY, EDEVICE, ERANGE, EPARSE = 0, 1, 2, 3, 4, 5, 6, 7, 8
 STATUS_NAMES = {OK: "LVBH_OK", EINVAL: "LVBH_EINVAL", ENOMEM: "LVBH_ENOMEM",
                 ETIMEOUT: "LVBH_ETIMEOUT", ECUDA: "LVBH_ECUDA", EBUSY: "LVBH_EBUSY",
-                EDEVICE: "LVBH_EDEVICE", ERANGE: "LVBH_ERANGE"}
+                EDEVICE: "LVBH_EDEVICE", ERANGE: "LVBH_ERANGE",
+                EPARSE: "LVBH_EPARSE"}
 NOALLOC_MAX_KEYS = 1 << 20
 
 # build flags
@@ -125,6 +126,9 @@ def _load():
     L.lvbh_server_last_error.argtypes = [vp]
     L.lvbh_trace.restype = i32
     L.lvbh_trace.argtypes = [vp, vp, vp, u32, vp, u32, vp, vp, vp, vp]
+    L.lvbh_parse_obj.restype = i32
+    L.lvbh_parse_obj.argtypes = [vp, vp, ctypes.c_uint64, u32, ctypes.POINTER(vp), ctypes.POINTER(u32),
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64), vp]
     return L
 
 

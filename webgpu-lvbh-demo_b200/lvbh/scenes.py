@@ -16,6 +16,9 @@ it with the shapes, sizes and value distributions of the five build workloads:
   request_sizes     log-uniform request sizes for the build server
   sphere_rays       rays for the sphere: origins uniform on a radius-3 sphere, directions
                     toward uniform points in [-1, 1]^3
+  obj_text          an indexed mesh written as the OBJ text an exporter writes (one `o`,
+                    `v x y z` with six decimals, `s off`, `f a b c`), the input of the
+                    OBJ ingest (parse-obj.js)
 
 All randomness comes from numpy's PCG64 generator seeded by the caller.  Every scene is
 returned as the reference's 48-byte triangle layout: float32 array (N, 12), vertices at
@@ -179,3 +182,13 @@ def obj_like_with_floor(n: int = 4096, seed: int = 5):
                       [s, -s, h, PAD, s, s, h, PAD, -s, s, h, PAD]], dtype=np.float32)
     bounds = np.concatenate([mn, mx]).astype(np.float32)
     return np.concatenate([tri, floor]), bounds
+
+
+def obj_text(xyz: np.ndarray, idx3: np.ndarray, name: str = "mesh") -> bytes:
+    """Indexed mesh (V, 3) + (F, 3) 0-based -> OBJ text (UTF-8 bytes): a comment line, `o name`,
+    one `v` line per vertex with six decimals, `s off`, one `f` line per triangle (1-based)."""
+    head = f"# synthetic mesh: {xyz.shape[0]} vertices, {idx3.shape[0]} faces\no {name}\n"
+    v = "\n".join("v %.6f %.6f %.6f" % (float(a), float(b), float(c)) for a, b, c in xyz.tolist())
+    f = "\n".join("f %d %d %d" % (a + 1, b + 1, c + 1) for a, b, c in idx3.tolist())
+    return (head + v + "\ns off\n" + f + "\n").encode()
+
