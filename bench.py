@@ -21,9 +21,12 @@ Prints one JSON line (rank 0).  Fields beyond the base contract:
   served        the build server under Poisson arrivals at 200..5000 requests/s (sizes
                 log-uniform in 1,024..4,194,304): p50/p99/p99.9 latency and builds/s beside the
                 plain per-request builder on the same arrival trace (1 GPU only)
+  trace         closest-hit traversal of 4,194,304 rays through the built 2M-triangle sphere
+  obj           OBJ ingest: the sphere's 80 MB OBJ text -> soup + bounds on the GPU, and end to
+                end through parse + build from pinned host text, beside the oracle's parse
 Under torchrun (N > 1) each rank builds its own replica (the build has no shardable exchange).
 
-    python bench.py --workload batch | served     the batched / served part alone
+    python bench.py --workload batch | served | trace | obj     one part alone
 """
 from __future__ import annotations
 
@@ -335,12 +338,18 @@ def run_ours(args, world, rank, local):
     builder.close()
     del dtri, outs, htri
     torch.cuda.empty_cache()
-    batched = served = None
+    batched = served = obj = trace = None
     if not args.no_batched:
         batched = run_batched(args, world, rank, local)
         torch.cuda.empty_cache()
     if not args.no_served and world == 1:
         served = run_served(args, world, rank, local)
+        torch.cuda.empty_cache()
+    if not args.no_trace:
+        trace = run_trace(args, world, rank, local)
+        torch.cuda.empty_cache()
+    if not args.no_obj:
+        obj = run_obj(args, world, rank, local)
     if rank != 0:
         return
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -351,7 +360,7 @@ def run_ours(args, world, rank, local):
                        "l2": "input soup 805 MB > 126 MB L2; no flush", "graph": True},
             "gpu_launches": LAUNCHES_PER_BUILD * args.steps,
             "roofline": roofline, "stage_ms": stage_ms, "cpu_baseline": cpu, "e2e": e2e_line,
-            "clocks": clock_summary, "batched": batched, "served": served}
+            "clocks": clock_summary, "batched": batched, "served": served, "trace": trace, "obj": obj}
     print(json.dumps(line), flush=True)
 
 
@@ -537,6 +546,94 @@ def run_trace(args, world, rank, local):
     return out
 
 
+def run_obj(args, world, rank, local):
+    """OBJ ingest (parseObj, parse-obj.js:3-88, the step main.js:72-73 runs before each build):
+    the 2,097,152-triangle displaced sphere written as an exporter writes it (1,050,625 `v`
+    lines with six decimals, 2,097,152 `f` lines; 80 MB) and parsed by lvbh_parse_obj.
+    Device-resident text per step, CUDA events around the call (which includes its host
+    round trips); end to end from pinned host text through parse, build and the root record
+    back on the host; the oracle's single-threaded parse of the same text as the CPU baseline
+    (the reference's parser is single-threaded JavaScript)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import lvbh
+    from lvbh import _native, empty_outputs, scenes
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    xyz, idx = scenes.sphere_mesh(1024, seed=1, indexed=True)
+    text = scenes.obj_text(xyz, idx)
+    nbytes = len(text)
+    dtext = torch.frombuffer(bytearray(text), dtype=torch.uint8).to(dev)
+    htext = torch.frombuffer(bytearray(text), dtype=torch.uint8).pin_memory()
+    ntri = idx.shape[0] + 2
+    builder = lvbh.BVHBuilder(local, reserve_tris=ntri)
+    stream = torch.cuda.current_stream(dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    tri = ctypes.c_void_p()
+    n = ctypes.c_uint32()
+    b6 = (ctypes.c_double * 6)()
+    line = ctypes.c_uint64()
+
+    def parse(ptr, flags):
+        _native.check(builder.ctx, _native.lib.lvbh_parse_obj(builder.ctx, ptr, nbytes, flags, ctypes.byref(tri),
+                                                              ctypes.byref(n), b6, ctypes.byref(line), sptr))
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    dptr = ctypes.c_void_p(dtext.data_ptr())
+    for _ in range(args.warmup):
+        parse(dptr, 0)
+    assert n.value == ntri
+    ms = max_over_ranks(statistics.median([timed(lambda: parse(dptr, 0)) for _ in range(args.steps)]), world)
+
+    outs = empty_outputs(ntri, dev)
+    hroot = torch.empty(16, dtype=torch.int32).pin_memory()
+    hptr = ctypes.c_void_p(htext.data_ptr())
+
+    def obj_to_bvh():
+        parse(hptr, _native.INPUT_HOST)
+        soup = lvbh._device_floats(tri.value, 12 * n.value, dev)
+        bounds32 = np.array(list(b6), dtype=np.float32)
+        builder.build_soup(soup, bounds32, outputs=outs, stream=stream, sync=True)
+        hroot.copy_(outs["nodes"][0], non_blocking=True)
+
+    for _ in range(args.warmup):
+        obj_to_bvh()
+    e2e = max_over_ranks(statistics.median([timed(obj_to_bvh) for _ in range(args.steps)]), world)
+    peak, peak_kind = load_peaks()
+    alg = nbytes + 48 * ntri  # text read once, soup written once
+    out = {"workload": "sphere_mesh_2M_obj", "text_bytes": nbytes, "num_tris": ntri,
+           "parse_ms": ms, "parse_gbs": world * nbytes / (ms * 1e-3) / 1e9,
+           "parse_mtris_per_s": world * ntri / (ms * 1e-3) / 1e6,
+           "roofline": {"bound": "hbm", "scope": "whole parse (text read once + soup written once)",
+                        "algorithmic_bytes": alg, "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak,
+                        "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind},
+           "e2e": {"what": "pinned host text -> parse -> build -> root record on the host",
+                   "ms_per_step": e2e, "value": world * nbytes / (e2e * 1e-3) / 1e6, "unit": "MB/s of OBJ text",
+                   "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": 64}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        t0 = time.perf_counter()
+        ref_tri, _ = oracle.parse_obj(text)
+        dt = time.perf_counter() - t0
+        got = lvbh._device_floats(tri.value, 12 * n.value, dev).cpu().numpy().reshape(-1, 12)
+        out["same_as_oracle"] = bool(np.array_equal(got.view(np.uint32), ref_tri.view(np.uint32)))
+        out["cpu_baseline"] = {"value": nbytes / dt / 1e6, "unit": "MB/s of OBJ text", "cores": 1, "kind": "port",
+                               "sample": "the whole 80 MB text, parse only", "ms": dt * 1e3}
+    builder.close()
+    return out
+
+
 def percentiles(x):
     import numpy as np
     a = np.asarray(x, dtype=np.float64)
@@ -681,6 +778,8 @@ def main():
     ap.add_argument("--batch-meshes", type=int, default=4096)
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-obj", action="store_true")
+    ap.add_argument("--no-trace", action="store_true")
     ap.add_argument("--serve-rates", default="200,500,1000,2000,5000")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-min-requests", type=int, default=1000)
@@ -700,6 +799,10 @@ def main():
                 print(json.dumps(out), flush=True)
         elif args.workload == "trace":
             out = run_trace(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(out), flush=True)
+        elif args.workload == "obj":
+            out = run_obj(args, world, rank, local)
             if rank == 0:
                 print(json.dumps(out), flush=True)
         elif args.workload == "served":

@@ -113,15 +113,17 @@ def test_parse_float_exact(builder):
         a, b, c = nums[i:i + 3]
         text = f"v {a} {b} {c}\nv {a} {b} {c}\nv {a} {b} {c}\nf 1 2 3\n"
         got = check_same(builder, text, "host", f"numbers {a} {b} {c}")
-        want = np.array([float(a), float(c), float(b)])
+        v = np.array([float(a), float(c), float(b)])
+        # BOUNDS start at +-1e30 (parse-obj.js:10-16): the value shows in min, max or both
+        want = np.concatenate([np.where(v < 1e30, v, 1e30), np.where(v > -1e30, v, -1e30)])
+        want[np.concatenate([np.isnan(v), np.isnan(v)])] = np.nan
         _, bounds = got
-        assert same_f64(bounds[:3], want), (a, b, c, bounds[:3], want)
+        assert same_f64(bounds, want), (a, b, c, bounds, want)
 
 
 def test_sphere_obj_then_build(builder):
     """OBJ text of a 525k-triangle mesh -> device soup -> build, against oracle parse -> oracle
     build: main.js's path (parseObj, then build(TRI_ARR, NUM_TRIS, BOUNDS))."""
-    import torch
     from lvbh import scenes
     from test_parity_gpu import assert_same
     xyz, idx = scenes.sphere_mesh(512, seed=3, indexed=True)
@@ -132,7 +134,6 @@ def test_sphere_obj_then_build(builder):
     res = builder.build_soup(out["TRI_ARR"], bounds32).to_numpy()
     ref = oracle.build(tri, bounds32, threads=0)
     assert_same(res, ref, "sphere build")
-    del torch
 
 
 def test_reuse_and_growth(builder):
