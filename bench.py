@@ -564,7 +564,7 @@ def run_obj(args, world, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    xyz, idx = scenes.sphere_mesh(1024, seed=1, indexed=True)
+    xyz, idx = scenes.sphere_mesh(args.obj_quads, seed=1, indexed=True)
     text = scenes.obj_text(xyz, idx)
     nbytes = len(text)
     dtext = torch.frombuffer(bytearray(text), dtype=torch.uint8).to(dev)
@@ -612,7 +612,8 @@ def run_obj(args, world, rank, local):
     e2e = max_over_ranks(statistics.median([timed(obj_to_bvh) for _ in range(args.steps)]), world)
     peak, peak_kind = load_peaks()
     alg = nbytes + 48 * ntri  # text read once, soup written once
-    out = {"workload": "sphere_mesh_2M_obj", "text_bytes": nbytes, "num_tris": ntri,
+    wname = "sphere_mesh_2M_obj" if args.obj_quads == 1024 else f"sphere_mesh_{2 * args.obj_quads ** 2}_obj"
+    out = {"workload": wname, "text_bytes": nbytes, "num_tris": ntri,
            "parse_ms": ms, "parse_gbs": world * nbytes / (ms * 1e-3) / 1e9,
            "parse_mtris_per_s": world * ntri / (ms * 1e-3) / 1e6,
            "roofline": {"bound": "hbm", "scope": "whole parse (text read once + soup written once)",
@@ -786,6 +787,7 @@ def main():
     ap.add_argument("--serve-max-requests", type=int, default=100_000)
     ap.add_argument("--serve-pool", type=int, default=4)
     ap.add_argument("--rays", type=int, default=1 << 22)
+    ap.add_argument("--obj-quads", type=int, default=1024)  # OBJ workload: sphere grid side
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -117,4 +117,21 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// Adds one count per valid lane to the shared-memory histogram h at bin d, one atomic per run
+// of equal bins over consecutive lanes: the run's first lane adds its length.  Input in
+// spatially coherent order (a mesh's triangles, keys grouped by the previous sort digit) gives
+// long runs, which plain per-lane atomics would serialise on one bin.  All 32 lanes call it.
+__device__ __forceinline__ void add_runs(uint32_t *h, uint32_t d, bool valid) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t dv = valid ? d : 0xFFFFFFFFu;  // invalid lanes form runs of their own
+    const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, dv, 1);
+    const bool head = lane == 0 || dv != up;
+    const uint32_t heads = __ballot_sync(0xFFFFFFFFu, head);
+    if (head && valid) {
+        const uint32_t after = heads & ~((2u << lane) - 1u);  // heads of the lanes above
+        const int next = after ? __ffs(after) - 1 : 32;
+        atomicAdd(h + d, (uint32_t)(next - lane));
+    }
+}
+
 }  // namespace lvbh

@@ -28,10 +28,24 @@ constexpr int kSortTile = kSortThreads * kSortItems; // keys per tile (4096)
 __host__ __device__ inline uint32_t sort_tiles(uint32_t n) { return (n + kSortTile - 1) / kSortTile; }
 
 // The plain build's sort scratch: per tile of kSortTile keys its kDigits counts of the pass's
-// digit, per chunk of kSortChunkTiles tiles their sum, per chunk the output offsets.
+// digit, per chunk of sort_chunk_tiles(n) tiles their sum, per chunk the output offsets.  A
+// chunk is one block of the per-chunk kernels (Morton keys, tile histograms): 8 tiles when that
+// still gives kChunkFill blocks (two per SM), fewer for smaller sorts.
 constexpr int kSortChunkTiles = 8;
+constexpr uint32_t kChunkFill = 296;
+__host__ __device__ inline uint32_t sort_chunk_tiles(uint32_t n) {
+    const uint32_t t = sort_tiles(n);
+    return t >= 8 * kChunkFill ? 8u : t >= 4 * kChunkFill ? 4u : t >= 2 * kChunkFill ? 2u : 1u;
+}
 __host__ __device__ inline uint32_t sort_chunks(uint32_t n) {
-    return (sort_tiles(n) + kSortChunkTiles - 1) / kSortChunkTiles;
+    const uint32_t ct = sort_chunk_tiles(n);
+    return (sort_tiles(n) + ct - 1) / ct;
+}
+// An upper bound of sort_chunks(m) over every m <= n (scratch sized for n serves them all).
+inline uint32_t sort_chunks_bound(uint32_t n) {
+    const uint32_t t = sort_tiles(n), c8 = (t + 7) / 8, lo = 2 * kChunkFill;
+    const uint32_t b = c8 > lo ? c8 : lo;
+    return b < t ? b : t;
 }
 inline uint32_t *sort_chunk_sums(uint32_t *scratch, uint32_t n) {
     return scratch + (size_t)sort_tiles(n) * kDigits;

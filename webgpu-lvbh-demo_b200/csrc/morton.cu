@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const float4 *__restrict__ 
 }
 
 // K1b: per triangle box, centroid, quantisation and 30-bit Morton key, written in input order.
-// One block per chunk of kSortChunkTiles sort tiles: per tile each warp takes chunks of 32
+// One block per chunk of sort_chunk_tiles(n) sort tiles: per tile each warp takes chunks of 32
 // triangles (96 consecutive float4, three coalesced 512-byte loads, transposed through shared
 // memory so that each lane owns a triangle); the digit counts of all three sort passes
 // accumulate over the block, and the counts of the first pass's digit per tile and per chunk
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const float4 *__restrict__ 
 __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ tri, uint32_t n,
                                                      HostBounds hb, Control *__restrict__ ctl,
                                                      uint32_t *__restrict__ keys,
-                                                     uint32_t *__restrict__ epoch,
+                                                     uint32_t *__restrict__ epoch, uint32_t chunk_tiles,
                                                      uint32_t *__restrict__ tile_hist,
                                                      uint32_t *__restrict__ chunk_sum) {
     constexpr int P = kDigits / kThreads;  // digits per thread in the per-tile counts
@@ -109,8 +109,8 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
 #pragma unroll
     for (int j = 0; j < P; ++j) acc[j] = 0;
     bool bad = false;
-    for (int tt = 0; tt < kSortChunkTiles; ++tt) {
-        const uint32_t tile = blockIdx.x * kSortChunkTiles + tt;
+    for (uint32_t tt = 0; tt < chunk_tiles; ++tt) {
+        const uint32_t tile = blockIdx.x * chunk_tiles + tt;
         if (tile >= tiles) break;  // uniform across the block
         for (int i = threadIdx.x; i < kDigits; i += kThreads) th[i] = 0;
         __syncthreads();
@@ -128,18 +128,20 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
                          v2 = stage[warp][3 * lane + 2];
             __syncwarp();
             const uint32_t t = t0 + lane;
-            if (t < n) {
+            const bool valid = t < n;
+            uint32_t key = 0;
+            if (valid) {
                 bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
                 // box.min = min(v0, min(v1, v2)); box.max = max(v0, max(v1, v2))   (:186-187)
                 const uint32_t qx = quantise(fminf(v0.x, fminf(v1.x, v2.x)), fmaxf(v0.x, fmaxf(v1.x, v2.x)), umin[0], umax[0]);
                 const uint32_t qy = quantise(fminf(v0.y, fminf(v1.y, v2.y)), fmaxf(v0.y, fmaxf(v1.y, v2.y)), umin[1], umax[1]);
                 const uint32_t qz = quantise(fminf(v0.z, fminf(v1.z, v2.z)), fmaxf(v0.z, fmaxf(v1.z, v2.z)), umin[2], umax[2]);
-                const uint32_t key = morton3(qx, qy, qz);
+                key = morton3(qx, qy, qz);
                 keys[t] = key;
-#pragma unroll
-                for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (kDigitBits * p)) & (kDigits - 1)], 1u);
-                atomicAdd(&th[key & (kDigits - 1)], 1u);
             }
+#pragma unroll
+            for (int p = 0; p < kSortPasses; ++p) add_runs(hist[p], (key >> (kDigitBits * p)) & (kDigits - 1), valid);
+            add_runs(th, key & (kDigits - 1), valid);
         }
         __syncthreads();
         uint32_t *row = tile_hist + (size_t)tile * kDigits + threadIdx.x * P;
@@ -257,16 +259,18 @@ __global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restr
                      v2 = stage[warp][3 * lane + 2];
         __syncwarp();
         const uint32_t t = 32u * c + lane;
-        if (t < cnt) {
+        const bool valid = t < cnt;
+        uint32_t key = 0;
+        if (valid) {
             bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
             const uint32_t qx = quantise(fminf(v0.x, fminf(v1.x, v2.x)), fmaxf(v0.x, fmaxf(v1.x, v2.x)), umin[0], umax[0]);
             const uint32_t qy = quantise(fminf(v0.y, fminf(v1.y, v2.y)), fmaxf(v0.y, fmaxf(v1.y, v2.y)), umin[1], umax[1]);
             const uint32_t qz = quantise(fminf(v0.z, fminf(v1.z, v2.z)), fmaxf(v0.z, fmaxf(v1.z, v2.z)), umin[2], umax[2]);
-            const uint32_t key = morton3(qx, qy, qz);
+            key = morton3(qx, qy, qz);
             keys[first + t] = key;
-#pragma unroll
-            for (int p = 0; p < NP; ++p) atomicAdd(&hist[p][(key >> (BITS * p)) & (D - 1)], 1u);
         }
+#pragma unroll
+        for (int p = 0; p < NP; ++p) add_runs(hist[p], (key >> (BITS * p)) & (D - 1), valid);
     }
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
     __syncthreads();
@@ -320,7 +324,7 @@ void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s) 
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl, uint32_t *keys,
                    uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
     if (n == 0) return;
-    k_morton<<<sort_chunks(n), kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch, sort_scratch,
+    k_morton<<<sort_chunks(n), kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch, sort_chunk_tiles(n), sort_scratch,
                                                  sort_chunk_sums(sort_scratch, n));
 }
 

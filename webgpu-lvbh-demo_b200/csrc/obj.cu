@@ -42,7 +42,7 @@ namespace {
 typedef unsigned __int128 u128;
 
 constexpr int kT = 256;
-constexpr int kChunk = 4096;  // text bytes per newline-count block (16 per thread)
+constexpr int kChunk = kT * 64;  // text bytes per newline-count block (64 per thread)
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kT * kScanItems;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
@@ -64,7 +64,8 @@ struct ObjCtl {
     uint32_t nan_min[3], nan_max[3];
 };
 
-// A vertex line the device leaves to the host: its text [start, end) and vertex rank.  The same
+// A vertex line the device leaves to the host: its text [start, end) (up to its comment, or
+// further when the device stopped reading before it) and vertex rank.  The same
 // slot then carries the host's exact coordinates back (HardFix).
 struct HardLine {
     unsigned long long start, end;
@@ -81,7 +82,8 @@ static_assert(sizeof(HardLine) == sizeof(HardFix), "hard-line slot");
 // at e.  A UTF-8 lead byte always starts a new character for the decoder of readAsText (an
 // unfinished sequence before it becomes U+FFFD), so checking every byte position finds exactly
 // the whitespace characters the decoded string holds.
-__host__ __device__ __forceinline__ int ws_len(const uint8_t *s, uint64_t i, uint64_t e) {
+template <typename S>
+__host__ __device__ __forceinline__ int ws_len(const S &s, uint64_t i, uint64_t e) {
     const uint8_t c = s[i];
     if (c == ' ' || (c >= 9 && c <= 13)) return 1;
     if (c < 0xC2) return 0;
@@ -100,8 +102,9 @@ __host__ __device__ __forceinline__ int ws_len(const uint8_t *s, uint64_t i, uin
 }
 
 // Next token of s[i, e): false when none is left; else [a, b).
-__host__ __device__ __forceinline__ bool next_token(const uint8_t *s, uint64_t &i, uint64_t e,
-                                                    uint64_t &a, uint64_t &b) {
+template <typename S>
+__host__ __device__ __forceinline__ bool next_token(const S &s, uint64_t &i, uint64_t e, uint64_t &a,
+                                                    uint64_t &b) {
     while (i < e) {
         const int w = ws_len(s, i, e);
         if (!w) break;
@@ -173,121 +176,217 @@ __device__ bool dec_to_double(unsigned long long w, int q, double &out) {
     return true;
 }
 
-// parseFloat of the whitespace-free token s[p, q): true with the double in out, false when the
-// host has to parse it (decimal exponent beyond +-27, or more than 19 significant digits whose
-// dropped tail could change the rounding).
-__device__ bool parse_float(const uint8_t *__restrict__ s, uint64_t p, uint64_t q, double &out) {
-    uint64_t i = p;
+// ---- Line scanning on the device.  A line is b[0, e): b is its first byte in a block's
+// shared-memory window or in global memory (each kernel inlines the scan once per case, so the
+// window case compiles to shared-memory loads), positions are 32-bit, and the first '#' ends the
+// line (cut when the scan reaches it).
+
+// Bytes of the JavaScript whitespace character at b[i] (0: none).
+__device__ __forceinline__ uint32_t ws32(const uint8_t *b, uint32_t i, uint32_t e) {
+    const uint32_t c = b[i];
+    if (c <= 32) return (c == 32 || c - 9u <= 4u) ? 1u : 0u;
+    if (c < 0xC2) return 0;
+    return (uint32_t)ws_len(b, (uint64_t)i, (uint64_t)e);  // the multi-byte forms
+}
+
+// Skips whitespace from i: false at the end of the content (the line's end, or a '#', which
+// then becomes the end).
+__device__ __forceinline__ bool skip_ws(const uint8_t *b, uint32_t &i, uint32_t &e) {
+    while (i < e) {
+        if (b[i] == '#') {
+            e = i;
+            return false;
+        }
+        const uint32_t w = ws32(b, i, e);
+        if (!w) return true;
+        i += w;
+    }
+    return false;
+}
+
+// Moves i to the end of the token it is in (whitespace, '#' or the end); returns the number of
+// '/' bytes passed.
+__device__ __forceinline__ uint32_t skip_token(const uint8_t *b, uint32_t &i, uint32_t &e) {
+    uint32_t slashes = 0;
+    while (i < e) {
+        const uint32_t c = b[i];
+        if (c == '#') {
+            e = i;
+            break;
+        }
+        if ((c <= 32 || c >= 0xC2) && ws32(b, i, e)) break;
+        slashes += c == '/';
+        ++i;
+    }
+    return slashes;
+}
+
+constexpr long long kIdxNaN = -0x7FFFFFFFFFFFFFFFll - 1;  // parseInt found no digit
+constexpr long long kIdxHuge = kIdxNaN + 1;               // |value| >= 2^53: names no vertex
+
+// parseInt (radix undefined) from b[i]: sign, optional 0x / 0X, the longest digit run (what
+// parseInt makes of a face vertex's first '/'-part, which ends where the digits do); i is left
+// after the digits.  Values of 2^53 and more name no vertex and are not 0, so they collapse to
+// kIdxHuge.
+__device__ __forceinline__ long long parse_index(const uint8_t *b, uint32_t &i, uint32_t e) {
     bool neg = false;
-    if (i < q && (s[i] == '+' || s[i] == '-')) { neg = s[i] == '-'; ++i; }
-    if (q - i >= 8 && s[i] == 'I' && s[i + 1] == 'n' && s[i + 2] == 'f' && s[i + 3] == 'i' &&
-        s[i + 4] == 'n' && s[i + 5] == 'i' && s[i + 6] == 't' && s[i + 7] == 'y') {
+    if (i < e && (b[i] == '+' || b[i] == '-')) {
+        neg = b[i] == '-';
+        ++i;
+    }
+    uint32_t radix = 10;
+    if (i + 1 < e && b[i] == '0' && (b[i + 1] | 0x20u) == 'x') {
+        radix = 16;
+        i += 2;
+    }
+    unsigned long long v = 0;
+    uint32_t digits = 0;
+    while (i < e) {
+        const uint32_t c = b[i];
+        uint32_t d;
+        if (c - '0' <= 9u) d = c - '0';
+        else if (radix == 16 && (c | 0x20u) - 'a' <= 5u) d = (c | 0x20u) - 'a' + 10;
+        else break;
+        v = v < (1ull << 53) ? v * radix + d : v;
+        ++digits;
+        ++i;
+    }
+    if (!digits) return kIdxNaN;
+    if (v >= (1ull << 53)) return kIdxHuge;
+    return neg ? -(long long)v : (long long)v;
+}
+
+__constant__ uint32_t kPow10u[10] = {1u, 10u, 100u, 1000u, 10000u, 100000u, 1000000u, 10000000u,
+                                     100000000u, 1000000000u};
+
+// parseFloat from b[i], a token's first byte: true with the double in out, false when the host
+// parses it (decimal exponent beyond +-27, or more than 19 significant digits whose dropped
+// tail could change the rounding); i is left where the literal ends.  Significant digits
+// accumulate nine at a time in 32 bits.
+__device__ __forceinline__ bool parse_number(const uint8_t *b, uint32_t &i, uint32_t e, double &out) {
+    bool neg = false;
+    if (i < e && (b[i] == '+' || b[i] == '-')) {
+        neg = b[i] == '-';
+        ++i;
+    }
+    if (i + 8 <= e && b[i] == 'I' && b[i + 1] == 'n' && b[i + 2] == 'f' && b[i + 3] == 'i' &&
+        b[i + 4] == 'n' && b[i + 5] == 'i' && b[i + 6] == 't' && b[i + 7] == 'y') {
+        i += 8;
         out = neg ? -INFINITY : INFINITY;
         return true;
     }
-    unsigned long long m = 0;
-    int nd = 0;
+    unsigned long long m = 0;  // folded significant digits
+    uint32_t acc = 0, na = 0;  // digits not folded yet (at most 9)
+    uint32_t nd = 0;           // significant digits kept (at most 19)
     long long dexp = 0;
-    bool any = false, inexact = false;
-    while (i < q && s[i] >= '0' && s[i] <= '9') {
-        const int d = s[i] - '0';
+    bool any = false, inexact = false, frac = false;
+    while (i < e) {
+        const uint32_t c = b[i];
+        const uint32_t d = c - '0';
+        if (d > 9u) {
+            if (c == '.' && !frac) {
+                frac = true;
+                ++i;
+                continue;
+            }
+            break;
+        }
         any = true;
         if (nd < 19) {
-            if (m || d) { m = m * 10 + d; ++nd; }
+            if (nd | d) {
+                acc = acc * 10 + d;
+                ++nd;
+                if (++na == 9) {
+                    m = m * 1000000000ull + acc;
+                    acc = 0;
+                    na = 0;
+                }
+            }
+            dexp -= frac;
         } else {
-            ++dexp;
+            dexp += !frac;
             inexact |= d != 0;
         }
         ++i;
-    }
-    if (i < q && s[i] == '.') {
-        ++i;
-        while (i < q && s[i] >= '0' && s[i] <= '9') {
-            const int d = s[i] - '0';
-            any = true;
-            if (nd < 19) {
-                if (m || d) { m = m * 10 + d; ++nd; }
-                --dexp;
-            } else {
-                inexact |= d != 0;
-            }
-            ++i;
-        }
     }
     if (!any) {
         out = NAN;
         return true;
     }
+    m = m * kPow10u[na] + acc;
     long long e10 = 0;
-    if (i < q && (s[i] == 'e' || s[i] == 'E')) {
-        uint64_t j = i + 1;
+    if (i < e && (b[i] | 0x20u) == 'e') {
+        uint32_t j = i + 1;
         bool eneg = false;
-        if (j < q && (s[j] == '+' || s[j] == '-')) { eneg = s[j] == '-'; ++j; }
+        if (j < e && (b[j] == '+' || b[j] == '-')) {
+            eneg = b[j] == '-';
+            ++j;
+        }
         long long ev = 0;
-        int ed = 0;
-        while (j < q && s[j] >= '0' && s[j] <= '9') {
-            if (ev < 1000000000ll) ev = ev * 10 + (s[j] - '0');
+        uint32_t ed = 0;
+        while (j < e && b[j] - '0' <= 9u) {
+            if (ev < 1000000000ll) ev = ev * 10 + (b[j] - '0');
             ++j;
             ++ed;
         }
-        if (ed) e10 = eneg ? -ev : ev;
+        if (ed) {
+            e10 = eneg ? -ev : ev;
+            i = j;
+        }
     }
     if (m == 0) {
         out = neg ? -0.0 : 0.0;
         return true;
     }
-    const long long e = e10 + dexp;
-    if (e < -27 || e > 27) return false;
+    const long long q = e10 + dexp;
+    if (q < -27 || q > 27) return false;
     double v;
-    if (!dec_to_double(m, (int)e, v)) return false;
-    if (inexact) {  // the value lies strictly between m * 10^e and (m + 1) * 10^e
+    if (!dec_to_double(m, (int)q, v)) return false;
+    if (inexact) {  // the value lies strictly between m * 10^q and (m + 1) * 10^q
         double hi;
-        if (!dec_to_double(m + 1, (int)e, hi) || hi != v) return false;
+        if (!dec_to_double(m + 1, (int)q, hi) || hi != v) return false;
     }
     out = neg ? -v : v;
     return true;
 }
 
-// parseInt (radix undefined) of s[p, q): sign, optional 0x / 0X, longest digit prefix; NaN
-// when there is no digit.
-__device__ double parse_int(const uint8_t *__restrict__ s, uint64_t p, uint64_t q) {
-    uint64_t i = p;
-    bool neg = false;
-    if (i < q && (s[i] == '+' || s[i] == '-')) { neg = s[i] == '-'; ++i; }
-    int radix = 10;
-    if (i + 1 < q && s[i] == '0' && (s[i + 1] == 'x' || s[i + 1] == 'X')) { radix = 16; i += 2; }
-    double v = 0.0;
-    int digits = 0;
-    for (; i < q; ++i) {
-        const uint8_t c = s[i];
-        int d;
-        if (c >= '0' && c <= '9') d = c - '0';
-        else if (radix == 16 && c >= 'a' && c <= 'f') d = c - 'a' + 10;
-        else if (radix == 16 && c >= 'A' && c <= 'F') d = c - 'A' + 10;
-        else break;
-        v = __dadd_rn(__dmul_rn(v, (double)radix), (double)d);  // exact below 2^53
-        ++digits;
-    }
-    if (!digits) return NAN;
-    return neg ? -v : v;
+// Line l: its bytes [p, q) (without the '\n').
+__device__ __forceinline__ void line_bytes(uint64_t n, const uint64_t *line_start, uint32_t L, uint32_t l,
+                                           uint64_t &p, uint64_t &q) {
+    p = line_start[l];
+    q = l + 1 < L ? line_start[l + 1] - 1 : n;
 }
 
-// Line l: its bytes [p, e) after the comment cut.
-__device__ __forceinline__ void line_span(const uint8_t *s, uint64_t n, const uint64_t *line_start,
-                                          uint32_t L, uint32_t l, uint64_t &p, uint64_t &e) {
-    p = line_start[l];
-    const uint64_t q = l + 1 < L ? line_start[l + 1] - 1 : n;
-    e = q;
-    for (uint64_t i = p; i < q; ++i)
-        if (s[i] == '#') { e = i; break; }
+constexpr int kLineBlock = 256;     // lines per block of the per-line kernels
+constexpr int kWindow = 24 * 1024;  // text bytes a block stages in shared memory
+
+// Stages the text of lines [l0, l0 + cnt) into win (as much as fits, from the 16-byte boundary
+// at or below the first line's start) with coalesced 16-byte loads; [w0, w1) is what it holds.
+// Every thread of the block calls it.
+__device__ void stage_lines(const uint8_t *__restrict__ text, uint64_t n, const uint64_t *__restrict__ line_start,
+                            uint32_t L, uint32_t l0, uint32_t cnt, uint8_t *win, uint64_t &w0, uint64_t &w1) {
+    const uint64_t a = line_start[l0] & ~15ull;
+    const uint64_t z = l0 + cnt < L ? line_start[l0 + cnt] : n;
+    const uint64_t e = z < a + kWindow ? z : a + kWindow;
+    for (uint64_t c = a + 16ull * threadIdx.x; c < e; c += 16ull * blockDim.x) {
+        if (c + 16 <= n) {
+            *reinterpret_cast<uint4 *>(win + (c - a)) = __ldcs(reinterpret_cast<const uint4 *>(text + c));
+        } else {
+            for (int k = 0; k < 16; ++k)
+                if (c + k < n) win[c - a + k] = text[c + k];
+        }
+    }
+    w0 = a;
+    w1 = e;
+    __syncthreads();
 }
 
 __device__ __forceinline__ uint8_t lower(uint8_t c) { return (c >= 'A' && c <= 'Z') ? c + 32 : c; }
 
-__device__ uint8_t keyword(const uint8_t *s, uint64_t a, uint64_t b) {
-    const uint64_t n = b - a;
+__device__ __forceinline__ uint8_t keyword(const uint8_t *b, uint32_t a, uint32_t z) {
+    const uint32_t n = z - a;
     if (n == 1) {
-        switch (lower(s[a])) {
+        switch (lower(b[a])) {
             case 'o': return LT_O;
             case 'g': return LT_G;
             case 'v': return LT_V;
@@ -295,9 +394,9 @@ __device__ uint8_t keyword(const uint8_t *s, uint64_t a, uint64_t b) {
             case 's': return LT_S;
             case 'f': return LT_F;
         }
-    } else if (n == 2 && lower(s[a]) == 'v') {
-        if (lower(s[a + 1]) == 't') return LT_VT;
-        if (lower(s[a + 1]) == 'n') return LT_VN;
+    } else if (n == 2 && lower(b[a]) == 'v') {
+        if (lower(b[a + 1]) == 't') return LT_VT;
+        if (lower(b[a + 1]) == 'n') return LT_VN;
     }
     return LT_NONE;
 }
@@ -331,24 +430,37 @@ __device__ __forceinline__ void warp_min_into(uint32_t v, uint32_t *dst) {
     if ((threadIdx.x & 31) == 0 && v != kNone && v < *(volatile uint32_t *)dst) atomicMin(dst, v);
 }
 
-// Newlines per kChunk bytes.
+// The 64 text bytes of thread threadIdx.x of chunk blockIdx.x (zero past the end): four
+// 16-byte loads; newline count by a SWAR zero-byte test on each word.
+__device__ __forceinline__ void load64(const uint8_t *__restrict__ s, uint64_t n, uint64_t p, uint4 (&v)[4]) {
+    if (p + 64 <= n) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = __ldcs(reinterpret_cast<const uint4 *>(s + p) + j);
+    } else {
+        uint8_t *b = reinterpret_cast<uint8_t *>(v);
+        for (int k = 0; k < 64; ++k) b[k] = p + k < n ? s[p + k] : 0;
+    }
+}
+
+__device__ __forceinline__ uint32_t newlines_in(uint32_t w) {
+    const uint32_t x = w ^ 0x0A0A0A0Au;  // zero bytes where '\n' was
+    return __popc(~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu));
+}
+
+__device__ __forceinline__ uint32_t newlines64(const uint4 (&v)[4]) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) c += newlines_in(v[j].x) + newlines_in(v[j].y) + newlines_in(v[j].z) + newlines_in(v[j].w);
+    return c;
+}
+
+// Newlines per kChunk bytes (64 per thread).
 __global__ void __launch_bounds__(kT) k_nl_count(const uint8_t *__restrict__ s, uint64_t n,
                                                  uint32_t *__restrict__ cnt) {
     __shared__ uint32_t w[kT / 32];
-    const uint64_t base = (uint64_t)blockIdx.x * kChunk + threadIdx.x * 16;
-    uint32_t c = 0;
-    if (base + 16 <= n) {
-        const uint4 v = *reinterpret_cast<const uint4 *>(s + base);
-        const uint32_t words[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const uint32_t x = words[k] ^ 0x0A0A0A0Au;  // zero bytes where '\n' was
-            c += __popc(~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu));
-        }
-    } else {
-        for (int k = 0; k < 16; ++k) c += (base + k < n && s[base + k] == '\n') ? 1u : 0u;
-    }
-    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    uint4 v[4];
+    load64(s, n, (uint64_t)blockIdx.x * kChunk + threadIdx.x * 64ull, v);
+    const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, newlines64(v));
     if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = c;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -358,20 +470,22 @@ __global__ void __launch_bounds__(kT) k_nl_count(const uint8_t *__restrict__ s, 
     }
 }
 
-// Exclusive scan of v[0, n) in place by one block; *total = the sum.
+// Exclusive scan of v[0, n) in place by one block, each thread over a run of consecutive
+// entries; *total = the sum.
 template <typename U>
 __global__ void __launch_bounds__(1024) k_scan_small(U *v, uint32_t n, U *total) {
     __shared__ U s_warp[32];
-    U carry = 0;
-    for (uint32_t b = 0; b < n; b += 1024) {
-        const uint32_t i = b + threadIdx.x;
-        const U x = i < n ? v[i] : (U)0;
-        U all;
-        const U ex = block_scan<U>(x, s_warp, &all);
-        if (i < n) v[i] = carry + ex;
-        carry += all;
+    const uint32_t per = (n + 1023) / 1024, b = threadIdx.x * per, e = min(n, b + per);
+    U sum = 0;
+    for (uint32_t i = b; i < e; ++i) sum += v[i];
+    U all;
+    U run = block_scan<U>(sum, s_warp, &all);
+    for (uint32_t i = b; i < e; ++i) {
+        const U x = v[i];
+        v[i] = run;
+        run += x;
     }
-    if (threadIdx.x == 0) *total = carry;
+    if (threadIdx.x == 0) *total = all;
 }
 
 // Line starts: the newline at byte k (rank r over the text) starts line r + 1 at k + 1.
@@ -379,66 +493,85 @@ __global__ void __launch_bounds__(kT) k_nl_write(const uint8_t *__restrict__ s, 
                                                  const uint32_t *__restrict__ base,
                                                  uint64_t *__restrict__ line_start) {
     __shared__ uint32_t s_warp[kT / 32];
-    const uint64_t p = (uint64_t)blockIdx.x * kChunk + threadIdx.x * 16;
-    uint8_t b[16];
-    if (p + 16 <= n) {
-        *reinterpret_cast<uint4 *>(b) = *reinterpret_cast<const uint4 *>(s + p);
-    } else {
-        for (int k = 0; k < 16; ++k) b[k] = p + k < n ? s[p + k] : 0;
+    const uint64_t p = (uint64_t)blockIdx.x * kChunk + threadIdx.x * 64ull;
+    uint4 v[4];
+    load64(s, n, p, v);
+    uint32_t r = base[blockIdx.x] + block_scan<uint32_t>(newlines64(v), s_warp, nullptr);
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(v);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        uint32_t m = ~(((w[j] ^ 0x0A0A0A0Au) & 0x7F7F7F7Fu) + 0x7F7F7F7Fu | (w[j] ^ 0x0A0A0A0Au) | 0x7F7F7F7Fu);
+        while (m) {  // one bit (7, 15, 23 or 31) per newline byte, in text order
+            const int byte = (__ffs(m) - 1) >> 3;
+            line_start[++r] = p + 4 * j + byte + 1;
+            m &= m - 1;
+        }
     }
-    uint32_t c = 0;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) c += b[k] == '\n';
-    uint32_t r = base[blockIdx.x] + block_scan<uint32_t>(c, s_warp, nullptr);
-#pragma unroll
-    for (int k = 0; k < 16; ++k)
-        if (b[k] == '\n') line_start[++r] = p + k + 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) line_start[0] = 0;
 }
 
-// Per line: statement type, the checks the reference's parser makes, the triangles a face
-// fans into, and the first `o` and model-creating lines.
-__global__ void __launch_bounds__(kT) k_lines(const uint8_t *__restrict__ s, uint64_t n,
-                                              const uint64_t *__restrict__ line_start, uint32_t L,
-                                              uint8_t *__restrict__ type, uint32_t *__restrict__ fans,
-                                              ObjCtl *__restrict__ ctl) {
-    const uint32_t l = blockIdx.x * kT + threadIdx.x;
-    uint8_t t = LT_NONE;
+struct LineClass {
+    uint8_t type;
+    bool bad;
+    uint32_t fan;
+};
+
+// Statement type of the line b[0, len), whether the reference's parser throws on it (g / s
+// with other than one argument, l with fewer than two vertices or a vertex of more than two
+// '/'-parts, f with fewer than three vertices, a vertex of more than three parts or a first
+// part parseInt()s to 0 or -0), and the triangles a face fans into.
+__device__ __forceinline__ LineClass classify(const uint8_t *b, uint32_t len) {
+    uint32_t i = 0, e = len;
+    if (!skip_ws(b, i, e)) return {LT_NONE, false, 0};
+    const uint32_t a = i;
+    skip_token(b, i, e);
+    const uint8_t t = keyword(b, a, i);
+    if (t == LT_NONE) return {LT_NONE, false, 0};
+    uint32_t ntok = 1;
     bool bad = false;
-    if (l < L) {
-        uint64_t p, e;
-        line_span(s, n, line_start, L, l, p, e);
-        uint64_t i = p, a = 0, b = 0;
-        if (next_token(s, i, e, a, b)) t = keyword(s, a, b);
-        uint32_t ntok = 1, fan = 0;
-        if (t != LT_NONE) {
-            while (next_token(s, i, e, a, b)) {
-                ++ntok;
-                if (t == LT_L || t == LT_F) {
-                    int slashes = 0;
-                    uint64_t first_end = b;
-                    for (uint64_t k = a; k < b; ++k)
-                        if (s[k] == '/') {
-                            if (!slashes) first_end = k;
-                            ++slashes;
-                        }
-                    if (t == LT_L && slashes > 1) bad = true;
-                    if (t == LT_F && (slashes > 2 || parse_int(s, a, first_end) == 0.0)) bad = true;
-                }
-            }
-            if ((t == LT_G || t == LT_S) && ntok != 2) bad = true;
-            if (t == LT_L && ntok < 3) bad = true;
-            if (t == LT_F) {
-                if (ntok < 4) bad = true;
-                else fan = ntok - 3;
-            }
+    while (skip_ws(b, i, e)) {
+        ++ntok;
+        if (t == LT_F) {
+            bad |= parse_index(b, i, e) == 0;
+            bad |= skip_token(b, i, e) > 2;
+        } else if (t == LT_L) {
+            bad |= skip_token(b, i, e) > 1;
+        } else {
+            skip_token(b, i, e);
         }
-        type[l] = t;
-        fans[l] = fan;
     }
-    warp_min_into(bad ? l : kNone, &ctl->err_line);
-    warp_min_into(t == LT_O ? l : kNone, &ctl->first_o);
-    const bool need = t == LT_V || t == LT_VT || t == LT_VN || t == LT_L || t == LT_F;
+    if ((t == LT_G || t == LT_S) && ntok != 2) bad = true;
+    if (t == LT_L && ntok < 3) bad = true;
+    uint32_t fan = 0;
+    if (t == LT_F) {
+        if (ntok < 4) bad = true;
+        else fan = ntok - 3;
+    }
+    return {t, bad, fan};
+}
+
+// Per line: its class, and the first `o` and model-creating lines.  One block per kLineBlock
+// lines, their text staged in shared memory.
+__global__ void __launch_bounds__(kLineBlock) k_lines(const uint8_t *__restrict__ text, uint64_t n,
+                                                      const uint64_t *__restrict__ line_start, uint32_t L,
+                                                      uint8_t *__restrict__ type, uint32_t *__restrict__ fans,
+                                                      ObjCtl *__restrict__ ctl) {
+    __shared__ __align__(16) uint8_t win[kWindow];
+    const uint32_t l0 = blockIdx.x * kLineBlock, l = l0 + threadIdx.x;
+    uint64_t w0, w1;
+    stage_lines(text, n, line_start, L, l0, min((uint32_t)kLineBlock, L - l0), win, w0, w1);
+    LineClass c{LT_NONE, false, 0};
+    if (l < L) {
+        uint64_t p, q;
+        line_bytes(n, line_start, L, l, p, q);
+        if (p >= w0 && q <= w1) c = classify(win + (p - w0), (uint32_t)(q - p));
+        else c = classify(text + p, (uint32_t)(q - p));
+        type[l] = c.type;
+        fans[l] = c.fan;
+    }
+    warp_min_into(c.bad ? l : kNone, &ctl->err_line);
+    warp_min_into(c.type == LT_O ? l : kNone, &ctl->first_o);
+    const bool need = c.type == LT_V || c.type == LT_VT || c.type == LT_VN || c.type == LT_L || c.type == LT_F;
     warp_min_into(need ? l : kNone, &ctl->first_need);
 }
 
@@ -491,34 +624,62 @@ __global__ void __launch_bounds__(kT) k_scan_down(const uint8_t *__restrict__ ty
     }
 }
 
-// Model-0 vertex lines -> doubles at their rank; numbers outside the device's exact range are
-// listed for the host.
-__global__ void __launch_bounds__(kT) k_vertices(const uint8_t *__restrict__ s, uint64_t n,
-                                                 const uint64_t *__restrict__ line_start, uint32_t L,
-                                                 const uint8_t *__restrict__ type, uint32_t a, uint32_t m,
-                                                 const unsigned long long *__restrict__ pre,
-                                                 double *__restrict__ verts, HardLine *__restrict__ hard,
-                                                 ObjCtl *__restrict__ ctl) {
-    const uint32_t i = blockIdx.x * kT + threadIdx.x;
-    if (i >= m || type[a + i] != LT_V) return;
-    const uint32_t l = a + i;
-    uint64_t p, e;
-    line_span(s, n, line_start, L, l, p, e);
-    uint64_t k = p, ta = 0, tb = 0;
-    next_token(s, k, e, ta, tb);  // the keyword
-    double xyz[3] = {0.0, 0.0, 0.0};
-    bool ok = true;
-    for (int c = 0; c < 3; ++c) {
-        if (!next_token(s, k, e, ta, tb)) break;
-        ok &= parse_float(s, ta, tb, xyz[c]);
+struct VertexParse {
+    double x, y, z;
+    uint32_t end;  // where the scan stopped (the content's end when a number was left over)
+    bool ok;
+};
+
+// The coordinates of the vertex line b[0, len) (missing ones 0, as _parseVertexCoords has it).
+__device__ __forceinline__ VertexParse parse_vertex(const uint8_t *b, uint32_t len) {
+    VertexParse r{0.0, 0.0, 0.0, len, true};
+    uint32_t i = 0, e = len;
+    skip_ws(b, i, e);
+    skip_token(b, i, e);  // the keyword
+    if (skip_ws(b, i, e)) {
+        r.ok &= parse_number(b, i, e, r.x);
+        skip_token(b, i, e);
+        if (skip_ws(b, i, e)) {
+            r.ok &= parse_number(b, i, e, r.y);
+            skip_token(b, i, e);
+            if (skip_ws(b, i, e)) {
+                r.ok &= parse_number(b, i, e, r.z);
+                skip_token(b, i, e);
+            }
+        }
     }
+    r.end = e;
+    return r;
+}
+
+// Model-0 vertex lines -> doubles at their rank; numbers outside the device's exact range are
+// listed for the host.  One block per kLineBlock lines of model 0, its text staged when it holds
+// a vertex line.
+__global__ void __launch_bounds__(kLineBlock) k_vertices(const uint8_t *__restrict__ text, uint64_t n,
+                                                         const uint64_t *__restrict__ line_start, uint32_t L,
+                                                         const uint8_t *__restrict__ type, uint32_t a, uint32_t m,
+                                                         const unsigned long long *__restrict__ pre,
+                                                         double *__restrict__ verts, HardLine *__restrict__ hard,
+                                                         ObjCtl *__restrict__ ctl) {
+    __shared__ __align__(16) uint8_t win[kWindow];
+    const uint32_t i0 = blockIdx.x * kLineBlock, i = i0 + threadIdx.x;
+    const bool mine = i < m && type[a + i] == LT_V;
+    if (!__syncthreads_or(mine)) return;
+    uint64_t w0, w1;
+    stage_lines(text, n, line_start, L, a + i0, min((uint32_t)kLineBlock, m - i0), win, w0, w1);
+    if (!mine) return;
+    uint64_t p, q;
+    line_bytes(n, line_start, L, a + i, p, q);
+    VertexParse r;
+    if (p >= w0 && q <= w1) r = parse_vertex(win + (p - w0), (uint32_t)(q - p));
+    else r = parse_vertex(text + p, (uint32_t)(q - p));
     const uint32_t vi = (uint32_t)(pre[i] & 0xFFFFFFFFull);
-    verts[3ull * vi] = xyz[0];
-    verts[3ull * vi + 1] = xyz[1];
-    verts[3ull * vi + 2] = xyz[2];
-    if (!ok) {
+    verts[3ull * vi] = r.x;
+    verts[3ull * vi + 1] = r.y;
+    verts[3ull * vi + 2] = r.z;
+    if (!r.ok) {
         const uint32_t h = atomicAdd(&ctl->num_hard, 1u);
-        hard[h] = HardLine{p, e, vi, 0u, 0u, 0u};
+        hard[h] = HardLine{p, p + r.end, vi, 0u, 0u, 0u};
     }
 }
 
@@ -537,66 +698,93 @@ __device__ __forceinline__ float to_f32(double d) {
     return isnan(d) ? __int_as_float(0x7FC00000) : __double2float_rn(d);
 }
 
-// Model-0 faces -> fan triangles (y and z swapped, float32, pad 3.1415) and the bounds.
-__global__ void __launch_bounds__(kT) k_faces(const uint8_t *__restrict__ s, uint64_t n,
-                                              const uint64_t *__restrict__ line_start, uint32_t L,
-                                              const uint8_t *__restrict__ type, uint32_t a, uint32_t m,
-                                              const unsigned long long *__restrict__ pre, uint32_t nverts,
-                                              const double *__restrict__ verts, float4 *__restrict__ tri,
-                                              ObjCtl *__restrict__ ctl) {
-    const uint32_t i = blockIdx.x * kT + threadIdx.x;
-    unsigned long long mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0ull, 0ull, 0ull};
-    bool nan_seen[3] = {false, false, false};
-    if (i < m && type[a + i] == LT_F) {
-        const uint32_t l = a + i;
-        uint64_t p, e;
-        line_span(s, n, line_start, L, l, p, e);
-        const double before = (double)(uint32_t)(pre[i] & 0xFFFFFFFFull);  // model-0 vertices so far
-        unsigned long long out = pre[i] >> 32;
-        uint64_t k = p, ta = 0, tb = 0;
-        next_token(s, k, e, ta, tb);  // the keyword
-        const float pad = __double2float_rn(3.1415);
-        float4 r = make_float4(0.f, 0.f, 0.f, pad), prev = r;
-        int nv = 0;
-        bool bad = false;
-        while (next_token(s, k, e, ta, tb)) {
-            uint64_t fe = tb;
-            for (uint64_t j = ta; j < tb; ++j)
-                if (s[j] == '/') { fe = j; break; }
-            double idx = parse_int(s, ta, fe);
-            if (idx < 0.0) idx = __dadd_rn(__dadd_rn(before, 1.0), idx);
-            const double vk = __dsub_rn(idx, 1.0);
-            if (!(vk >= 0.0) || vk != floor(vk) || vk >= (double)nverts) { bad = true; break; }
-            const double *v = verts + 3ull * (unsigned long long)vk;
-            const double c[3] = {v[0], v[2], v[1]};  // x, then the file's z as y and y as z
+// Running Math.min / Math.max of one thread's vertices (ordered doubles, NaN flags).
+struct BoundsAcc {
+    unsigned long long mn[3], mx[3];
+    bool nan[3];
+    __device__ __forceinline__ void add(const double (&c)[3]) {
 #pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-                if (isnan(c[ax])) { nan_seen[ax] = true; continue; }
-                const unsigned long long o = ord64(c[ax]);
-                mn[ax] = o < mn[ax] ? o : mn[ax];
-                mx[ax] = o > mx[ax] ? o : mx[ax];
+        for (int ax = 0; ax < 3; ++ax) {
+            if (isnan(c[ax])) {
+                nan[ax] = true;
+                continue;
             }
-            const float4 cur = make_float4(to_f32(c[0]), to_f32(c[1]), to_f32(c[2]), pad);
-            if (nv == 0) {
-                r = cur;
-            } else if (nv >= 2) {
-                float4 *o = tri + 3ull * out;
-                o[0] = r;
-                o[1] = prev;
-                o[2] = cur;
-                ++out;
-            }
-            prev = cur;
-            ++nv;
+            const unsigned long long o = ord64(c[ax]);
+            mn[ax] = o < mn[ax] ? o : mn[ax];
+            mx[ax] = o > mx[ax] ? o : mx[ax];
         }
-        if (bad) atomicOr(&ctl->bad_index, 1u);
     }
-    __shared__ unsigned long long s_mn[3][kT / 32], s_mx[3][kT / 32];
-    __shared__ int s_nan[3][kT / 32];
+};
+
+// The face line b[0, len): its vertices resolved (negative indices against `before`, the
+// model's vertices so far), fanned from the first, stored from triangle `out` on; false when an
+// index names no vertex.
+__device__ __forceinline__ bool emit_face(const uint8_t *b, uint32_t len, long long before, uint32_t nverts,
+                                          const double *__restrict__ verts, float4 *__restrict__ tri,
+                                          unsigned long long out, BoundsAcc &bd) {
+    uint32_t i = 0, e = len;
+    skip_ws(b, i, e);
+    skip_token(b, i, e);  // the keyword
+    const float pad = __double2float_rn(3.1415);
+    float4 r = make_float4(0.f, 0.f, 0.f, pad), prev = r;
+    int nv = 0;
+    while (skip_ws(b, i, e)) {
+        long long v = parse_index(b, i, e);
+        skip_token(b, i, e);
+        if (v == kIdxNaN || v == kIdxHuge) return false;
+        if (v < 0) v = before + 1 + v;  // vertices.length + 1 + vertexIndex
+        const long long vk = v - 1;
+        if (vk < 0 || vk >= (long long)nverts) return false;
+        const double *vp = verts + 3ull * (unsigned long long)vk;
+        const double c[3] = {vp[0], vp[2], vp[1]};  // x, then the file's z as y and y as z
+        bd.add(c);
+        const float4 cur = make_float4(to_f32(c[0]), to_f32(c[1]), to_f32(c[2]), pad);
+        if (nv == 0) {
+            r = cur;
+        } else if (nv >= 2) {
+            float4 *o = tri + 3ull * out;
+            o[0] = r;
+            o[1] = prev;
+            o[2] = cur;
+            ++out;
+        }
+        prev = cur;
+        ++nv;
+    }
+    return true;
+}
+
+// Model-0 faces -> fan triangles (y and z swapped, float32, pad 3.1415) and the bounds.  One
+// block per kLineBlock lines of model 0, its text staged when it holds a face line.
+__global__ void __launch_bounds__(kLineBlock) k_faces(const uint8_t *__restrict__ text, uint64_t n,
+                                                      const uint64_t *__restrict__ line_start, uint32_t L,
+                                                      const uint8_t *__restrict__ type, uint32_t a, uint32_t m,
+                                                      const unsigned long long *__restrict__ pre, uint32_t nverts,
+                                                      const double *__restrict__ verts, float4 *__restrict__ tri,
+                                                      ObjCtl *__restrict__ ctl) {
+    __shared__ __align__(16) uint8_t win[kWindow];
+    const uint32_t i0 = blockIdx.x * kLineBlock, i = i0 + threadIdx.x;
+    const bool mine = i < m && type[a + i] == LT_F;
+    if (!__syncthreads_or(mine)) return;
+    uint64_t w0, w1;
+    stage_lines(text, n, line_start, L, a + i0, min((uint32_t)kLineBlock, m - i0), win, w0, w1);
+    BoundsAcc bd{{~0ull, ~0ull, ~0ull}, {0ull, 0ull, 0ull}, {false, false, false}};
+    if (mine) {
+        uint64_t p, q;
+        line_bytes(n, line_start, L, a + i, p, q);
+        const long long before = (long long)(pre[i] & 0xFFFFFFFFull);  // model-0 vertices so far
+        const unsigned long long out = pre[i] >> 32;
+        bool ok;
+        if (p >= w0 && q <= w1) ok = emit_face(win + (p - w0), (uint32_t)(q - p), before, nverts, verts, tri, out, bd);
+        else ok = emit_face(text + p, (uint32_t)(q - p), before, nverts, verts, tri, out, bd);
+        if (!ok) atomicOr(&ctl->bad_index, 1u);
+    }
+    __shared__ unsigned long long s_mn[3][kLineBlock / 32], s_mx[3][kLineBlock / 32];
+    __shared__ int s_nan[3][kLineBlock / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-        unsigned long long lo = mn[ax], hi = mx[ax];
+        unsigned long long lo = bd.mn[ax], hi = bd.mx[ax];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const unsigned long long lo2 = __shfl_xor_sync(0xFFFFFFFFu, lo, o);
@@ -604,7 +792,7 @@ __global__ void __launch_bounds__(kT) k_faces(const uint8_t *__restrict__ s, uin
             lo = lo2 < lo ? lo2 : lo;
             hi = hi2 > hi ? hi2 : hi;
         }
-        const int nan_any = __any_sync(0xFFFFFFFFu, nan_seen[ax]);
+        const int nan_any = __any_sync(0xFFFFFFFFu, bd.nan[ax]);
         if (lane == 0) { s_mn[ax][warp] = lo; s_mx[ax][warp] = hi; s_nan[ax][warp] = nan_any; }
     }
     __syncthreads();
@@ -612,7 +800,7 @@ __global__ void __launch_bounds__(kT) k_faces(const uint8_t *__restrict__ s, uin
         const int ax = threadIdx.x;
         unsigned long long lo = ~0ull, hi = 0ull;
         int nan_any = 0;
-        for (int w = 0; w < kT / 32; ++w) {
+        for (int w = 0; w < kLineBlock / 32; ++w) {
             lo = s_mn[ax][w] < lo ? s_mn[ax][w] : lo;
             hi = s_mx[ax][w] > hi ? s_mx[ax][w] : hi;
             nan_any |= s_nan[ax][w];
@@ -744,7 +932,7 @@ int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, 
     if (chunks) k_nl_write<<<chunks, kT, 0, s>>>(d_text, bytes, cnt, line_start);
     else OBJ_CUDA(cudaMemsetAsync(line_start, 0, 8, s), "cudaMemsetAsync");
     const uint32_t lb = (uint32_t)((L + (uint64_t)kT - 1) / kT);
-    k_lines<<<lb, kT, 0, s>>>(d_text, bytes, line_start, L, type, fans, ctl);
+    k_lines<<<lb, kLineBlock, 0, s>>>(d_text, bytes, line_start, L, type, fans, ctl);
     OBJ_CUDA(cudaGetLastError(), "k_lines");
     OBJ_CUDA(cudaMemcpyAsync(hc, ctl, sizeof(ObjCtl), cudaMemcpyDeviceToHost, s), "readback");
     OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
@@ -789,7 +977,7 @@ int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, 
     double *verts = reinterpret_cast<double *>(static_cast<char *>(sc.soup) + tbytes);
     HardLine *hard = reinterpret_cast<HardLine *>(static_cast<char *>(sc.soup) + tbytes + vbytes);
     if (nverts) {
-        k_vertices<<<mb, kT, 0, s>>>(d_text, bytes, line_start, L, type, m0a, m, pre, verts, hard, ctl);
+        k_vertices<<<mb, kLineBlock, 0, s>>>(d_text, bytes, line_start, L, type, m0a, m, pre, verts, hard, ctl);
         OBJ_CUDA(cudaGetLastError(), "k_vertices");
         OBJ_CUDA(cudaMemcpyAsync(&hc->num_hard, &ctl->num_hard, 4, cudaMemcpyDeviceToHost, s), "readback");
         OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
@@ -803,13 +991,15 @@ int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, 
         std::vector<HardFix> fix(nh);
         std::vector<uint8_t> buf;
         for (uint32_t h = 0; h < nh; ++h) {
-            const uint64_t len = hl[h].end - hl[h].start;
+            uint64_t len = hl[h].end - hl[h].start;
             const uint8_t *ln = reinterpret_cast<const uint8_t *>(text) + hl[h].start;
             if (!host_text) {
                 buf.resize(len);
                 if (len) OBJ_CUDA(cudaMemcpy(buf.data(), d_text + hl[h].start, len, cudaMemcpyDeviceToHost), "readback");
                 ln = buf.data();
             }
+            const void *hash = len ? std::memchr(ln, '#', len) : nullptr;  // the comment cut
+            if (hash) len = static_cast<const uint8_t *>(hash) - ln;
             uint64_t k = 0, ta = 0, tb = 0;
             next_token(ln, k, len, ta, tb);  // the keyword
             HardFix f{{0.0, 0.0, 0.0}, hl[h].vi, 0u};
@@ -825,7 +1015,7 @@ int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, 
         k_patch<<<(nh + kT - 1) / kT, kT, 0, s>>>(dfix, nh, verts);
         OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");  // `fix` is pageable host memory
     }
-    if (nfan) k_faces<<<mb, kT, 0, s>>>(d_text, bytes, line_start, L, type, m0a, m, pre, nverts, verts, tri, ctl);
+    if (nfan) k_faces<<<mb, kLineBlock, 0, s>>>(d_text, bytes, line_start, L, type, m0a, m, pre, nverts, verts, tri, ctl);
     OBJ_CUDA(cudaGetLastError(), "k_faces");
     OBJ_CUDA(cudaMemcpyAsync(hc, ctl, sizeof(ObjCtl), cudaMemcpyDeviceToHost, s), "readback");
     OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");

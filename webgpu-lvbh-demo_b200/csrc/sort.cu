@@ -294,13 +294,12 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
     if (oob) atomicOr(&ctl->err, ERR_LOOKBACK_TIMEOUT);
 }
 
-constexpr int kChunkTiles = kSortChunkTiles;
 
-// Reduce: digit counts of every tile (tile_hist[tile][digit]) and of every chunk of kChunkTiles
+// Reduce: digit counts of every tile (tile_hist[tile][digit]) and of every chunk of chunk_tiles
 // tiles (chunk_sum[chunk][digit]).  One block per chunk; each thread owns P contiguous digits.
 template <int BITS>
 __global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ keys, uint32_t n, int pass,
-                                                 uint32_t *__restrict__ tile_hist,
+                                                 uint32_t chunk_tiles, uint32_t *__restrict__ tile_hist,
                                                  uint32_t *__restrict__ chunk_sum) {
     constexpr int D = 1 << BITS, P = D / T;
     __shared__ __align__(16) uint32_t h[D];
@@ -309,8 +308,8 @@ __global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ ke
     uint32_t acc[P];
 #pragma unroll
     for (int j = 0; j < P; ++j) acc[j] = 0;
-    for (int tt = 0; tt < kChunkTiles; ++tt) {
-        const uint32_t tile = blockIdx.x * kChunkTiles + tt;
+    for (uint32_t tt = 0; tt < chunk_tiles; ++tt) {
+        const uint32_t tile = blockIdx.x * chunk_tiles + tt;
         if (tile >= tiles) break;  // uniform across the block
         for (int i = tid; i < D; i += T) h[i] = 0;
         __syncthreads();
@@ -322,8 +321,7 @@ __global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ ke
             k[i] = idx < n ? __ldcs(keys + idx) : 0xFFFFFFFFu;
         }
 #pragma unroll
-        for (int i = 0; i < IPT; ++i)
-            if (base + i * T + tid < n) atomicAdd(&h[(k[i] >> shift) & (D - 1)], 1u);
+        for (int i = 0; i < IPT; ++i) add_runs(h, (k[i] >> shift) & (D - 1), base + i * T + tid < n);
         __syncthreads();
         uint32_t c[P];
 #pragma unroll
@@ -391,7 +389,7 @@ __global__ void __launch_bounds__(T, 4) k_scatter(const uint32_t *__restrict__ k
                                                uint32_t *__restrict__ vals_out, uint32_t n,
                                                int pass, const uint32_t *__restrict__ tile_hist,
                                                const uint32_t *__restrict__ chunk_off,
-                                               Control *__restrict__ ctl) {
+                                               uint32_t chunk_tiles, Control *__restrict__ ctl) {
     constexpr int D = 1 << BITS;
     constexpr int P = D / T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -411,11 +409,11 @@ __global__ void __launch_bounds__(T, 4) k_scatter(const uint32_t *__restrict__ k
     // the digit prefixes of this tile (final values: independent loads, in flight with the
     // keys), parked in S.out until the tile's own starts are known
     {
-        const uint32_t chunk = tile / kChunkTiles;
+        const uint32_t chunk = tile / chunk_tiles;
         uint32_t pre[P];
 #pragma unroll
         for (int j = 0; j < P; ++j) pre[j] = __ldg(chunk_off + (size_t)chunk * D + tid * P + j);
-        for (uint32_t t = chunk * kChunkTiles; t < tile; ++t) {
+        for (uint32_t t = chunk * chunk_tiles; t < tile; ++t) {
 #pragma unroll
             for (int j = 0; j < P; ++j) pre[j] += __ldg(tile_hist + (size_t)t * D + tid * P + j);
         }
@@ -525,7 +523,7 @@ cudaError_t sort_init() {
     return e;
 }
 
-size_t sort_scratch_words(uint32_t n) { return ((size_t)sort_tiles(n) + 2ull * sort_chunks(n)) * kDigits; }
+size_t sort_scratch_words(uint32_t n) { return ((size_t)sort_tiles(n) + 2ull * sort_chunks_bound(n)) * kDigits; }
 
 void launch_sort_pass(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
                       uint32_t *vals_out, uint32_t n, int pass, bool counted, Control *ctl,
@@ -535,11 +533,12 @@ void launch_sort_pass(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t
     uint32_t *tile_hist = scratch;
     uint32_t *chunk_sum = sort_chunk_sums(scratch, n);
     uint32_t *chunk_off = chunk_sum + (size_t)chunks * kDigits;
-    if (!counted) k_tile_hist<kDigitBits><<<chunks, T, 0, s>>>(keys_in, n, pass, tile_hist, chunk_sum);
+    const uint32_t ct = sort_chunk_tiles(n);
+    if (!counted) k_tile_hist<kDigitBits><<<chunks, T, 0, s>>>(keys_in, n, pass, ct, tile_hist, chunk_sum);
     k_chunk_scan<kDigitBits><<<kDigits / 32, kScanThreads, 0, s>>>(chunk_sum, chunks,
                                                                    ctl->hist + pass * kDigits, chunk_off);
     k_scatter<kDigitBits><<<tiles, T, sizeof(SortSmem<kDigitBits>), s>>>(
-        keys_in, vals_in, keys_out, vals_out, n, pass, tile_hist, chunk_off, ctl);
+        keys_in, vals_in, keys_out, vals_out, n, pass, tile_hist, chunk_off, ct, ctl);
 }
 
 void launch_onesweep32(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
