@@ -24,9 +24,10 @@ Prints one JSON line (rank 0).  Fields beyond the base contract:
   trace         closest-hit traversal of 4,194,304 rays through the built 2M-triangle sphere
   obj           OBJ ingest: the sphere's 80 MB OBJ text -> soup + bounds on the GPU, and end to
                 end through parse + build from pinned host text, beside the oracle's parse
+  pt            path-trace bounces: 1920 x 1080 pixels, one bounce each per step, on the sphere
 Under torchrun (N > 1) each rank builds its own replica (the build has no shardable exchange).
 
-    python bench.py --workload batch | served | trace | obj     one part alone
+    python bench.py --workload batch | served | trace | obj | pt     one part alone
 """
 from __future__ import annotations
 
@@ -350,6 +351,10 @@ def run_ours(args, world, rank, local):
         torch.cuda.empty_cache()
     if not args.no_obj:
         obj = run_obj(args, world, rank, local)
+        torch.cuda.empty_cache()
+    pt = None
+    if not args.no_pt:
+        pt = run_pt(args, world, rank, local)
     if rank != 0:
         return
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -360,7 +365,8 @@ def run_ours(args, world, rank, local):
                        "l2": "input soup 805 MB > 126 MB L2; no flush", "graph": True},
             "gpu_launches": LAUNCHES_PER_BUILD * args.steps,
             "roofline": roofline, "stage_ms": stage_ms, "cpu_baseline": cpu, "e2e": e2e_line,
-            "clocks": clock_summary, "batched": batched, "served": served, "trace": trace, "obj": obj}
+            "clocks": clock_summary, "batched": batched, "served": served, "trace": trace, "obj": obj,
+            "pt": pt}
     print(json.dumps(line), flush=True)
 
 
@@ -635,6 +641,65 @@ def run_obj(args, world, rank, local):
     return out
 
 
+def run_pt(args, world, rank, local):
+    """Path-trace bounces (sample(), pathtracer.js:360-392 -> ptStep :655-713): the built
+    2,097,152-triangle displaced sphere under the reference's camera (1.5 x the model's extent
+    away, looking at its centre), a 1920 x 1080 image, one lvbh_pt_sample per step (every
+    pixel's path one bounce on; four rgba32f state planes ping-ponged in HBM), CUDA events
+    around each call; the oracle's bounce of the same frame on all host cores as the CPU
+    baseline."""
+    import numpy as np
+    import torch
+
+    import lvbh
+    from lvbh import scenes
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    tri = scenes.sphere_mesh(1024, seed=1)
+    builder = lvbh.BVHBuilder(local)
+    res = builder.build_soup(torch.from_numpy(tri).to(dev))
+    w, h = args.pt_width, args.pt_height
+    pos, lat = lvbh.camera([float(x) for x in res.bounds])
+    bufs = [torch.zeros((4, h, w, 4), dtype=torch.float32, device=dev) for _ in range(2)]
+    stream = torch.cuda.current_stream(dev)
+    k = [0]
+
+    def step():
+        i = k[0]
+        builder.pt_sample(res, None if i == 0 else bufs[i % 2], bufs[(i + 1) % 2], w, h, pos, lat, reset=i == 0)
+        k[0] += 1
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = max_over_ranks(statistics.median(times), world)
+    st = bufs[k[0] % 2].cpu().numpy()
+    out = {"workload": "sphere_mesh_2M_pt_1080p", "width": w, "height": h, "samples_run": k[0],
+           "ms_per_bounce": ms, "mpix_bounces_per_s": world * w * h / (ms * 1e-3) / 1e6,
+           "state_bytes_per_bounce": 128 * w * h,
+           "state_gbs": world * 128 * w * h / (ms * 1e-3) / 1e9,
+           "mean_samples_per_pixel": float(st[2][..., 3].mean())}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        ref = res.to_numpy()
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.pt_step(ref["nodes"], ref["tris"], None, w, h, pos, lat, True)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": w * h / dt / 1e6, "unit": "Mpixel-bounces/s", "cores": cores,
+                               "kind": "port", "sample": f"the first bounce of the {w} x {h} frame"}
+    builder.close()
+    return out
+
+
 def percentiles(x):
     import numpy as np
     a = np.asarray(x, dtype=np.float64)
@@ -788,6 +853,9 @@ def main():
     ap.add_argument("--serve-pool", type=int, default=4)
     ap.add_argument("--rays", type=int, default=1 << 22)
     ap.add_argument("--obj-quads", type=int, default=1024)  # OBJ workload: sphere grid side
+    ap.add_argument("--pt-width", type=int, default=1920)
+    ap.add_argument("--pt-height", type=int, default=1080)
+    ap.add_argument("--no-pt", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -801,6 +869,10 @@ def main():
                 print(json.dumps(out), flush=True)
         elif args.workload == "trace":
             out = run_trace(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(out), flush=True)
+        elif args.workload == "pt":
+            out = run_pt(args, world, rank, local)
             if rank == 0:
                 print(json.dumps(out), flush=True)
         elif args.workload == "obj":

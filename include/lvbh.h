@@ -307,6 +307,30 @@ LVBH_API int  lvbh_trace(lvbh_ctx *ctx, const void *nodes, const void *tris, uin
                 const float *rays, uint32_t num_rays, int32_t *hit_prim, float *hit_t,
                 uint32_t *max_stack, void *stream);
 
+/* ---- consumer: one path-trace bounce per pixel -------------------------------------
+ * Replaces sample() (scripts/pathtracer/pathtracer.js:360-392): the compute shader main /
+ * ptStep (:630-713) advances every pixel's path by one bounce - camera ray for a new path,
+ * closest hit through the tree (:495-628), Lambertian bounce with Russian roulette after three
+ * bounces, radiance 8 x throughput on a miss - over four rgba32f state images kept as device
+ * buffers (no textures, no swapchain): planes o (origin, seed), d (direction, bounce count),
+ * t (accumulated radiance, sample count), b (throughput, 1), each width x height float4, pixel
+ * (x, y) at y * width + x.  state_in is read unless frame->rst is non-zero (the reset that
+ * starts every path over); state_out receives the next state (ping-pong the two, as the
+ * reference does).  The shader's implementation-defined functions are fixed: normalize(v) =
+ * v / sqrt(dot(v, v)), sin / cos by a Cody-Waite reduction and Taylor polynomials (2 ulp),
+ * pow(.3, 2.2) and sin(fov / 2) the nearest floats, aspect = (float)(width / height).
+ * nodes / tris: a built tree (lvbh_result), device memory.  Returns LVBH_OK, LVBH_EINVAL or
+ * LVBH_ECUDA; the call returns once the bounce has finished. */
+typedef struct lvbh_pt_frame {
+    float pos[3];  /* camera position (the uniform buffer's pos) */
+    float rst;     /* non-zero: every path starts over (the uniform buffer's rst) */
+    float lat[3];  /* look-at point */
+    float pad;
+} lvbh_pt_frame;
+LVBH_API int  lvbh_pt_sample(lvbh_ctx *ctx, const void *nodes, const void *tris, uint32_t num_tris,
+                             const float *state_in, float *state_out, uint32_t width, uint32_t height,
+                             const lvbh_pt_frame *frame, void *stream);
+
 /* ---- producer: OBJ text -> TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS ------------------------
  * Replaces parseObj(file) (scripts/obj/parse-obj.js:3-88) and the OBJFile parser it calls
  * (scripts/obj/obj-file-parser.js:19-193), the step main.js:72-73 runs before build().  The

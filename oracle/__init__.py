@@ -35,7 +35,7 @@ def build_lib() -> str:
 def lib():
     global _lib
     if _lib is None:
-        srcs = [os.path.join(_HERE, f) for f in ("lvbh_oracle.cpp", "obj_oracle.cpp")]
+        srcs = [os.path.join(_HERE, f) for f in ("lvbh_oracle.cpp", "obj_oracle.cpp", "pt_oracle.cpp")]
         if not os.path.exists(_LIB_PATH) or any(
                 os.path.exists(f) and os.path.getmtime(f) > os.path.getmtime(_LIB_PATH) for f in srcs):
             build_lib()
@@ -56,6 +56,8 @@ def lib():
         L.oracle_parse_obj.argtypes = [ctypes.c_char_p, ctypes.c_uint64, vp, ctypes.c_uint64,
                                        ctypes.POINTER(ctypes.c_uint64), vp, ctypes.POINTER(ctypes.c_int64)]
         L.oracle_parse_obj.restype = ctypes.c_int
+        L.oracle_pt_step.argtypes = [_u32p, _f32p, u32, vp, _f32p, ctypes.POINTER(PtFrame)]
+        L.oracle_pt_sincos.argtypes = [_f32p, u32, _f32p, _f32p]
         _lib = L
     return _lib
 
@@ -185,3 +187,45 @@ def parse_obj(text):
                                 ctypes.byref(line))
     assert rc == 0
     return tri, b
+
+
+class PtFrame(ctypes.Structure):
+    """The bounce's per-frame inputs (OraclePtFrame in pt_oracle.cpp)."""
+    _fields_ = [("pos", ctypes.c_float * 3), ("rst", ctypes.c_float), ("lat", ctypes.c_float * 3),
+                ("pad", ctypes.c_float), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("aspect", ctypes.c_float), ("sinfov", ctypes.c_float), ("powc", ctypes.c_float),
+                ("pad2", ctypes.c_float)]
+
+
+def pt_constants(width: int, height: int):
+    """The constants the reference's shader bakes in: aspect = w / h, sin(.5 * fov * Pi / 180)
+    with its argument in float, pow(.3, 2.2), each rounded to float."""
+    import math
+    f = np.float32
+    half_fov = f(f(f(0.5) * f(60.0)) * f(math.pi)) / f(180.0)
+    return (f(width / height), f(math.sin(float(half_fov))), f(math.pow(float(f(0.3)), float(f(2.2)))))
+
+
+def pt_step(nodes, tris, state, width: int, height: int, pos, lat, rst: bool) -> np.ndarray:
+    """One sample() of the reference's path tracer (scripts/pathtracer/pathtracer.js:360-392,
+    630-772) over a built tree: state (4, height, width, 4) float32 planes o, d, t, b -> the next
+    state.  state may be None when rst."""
+    nodes = np.ascontiguousarray(nodes).view(np.uint32).reshape(-1)
+    tris = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1)
+    n = tris.size // 12
+    out = np.empty((4, height, width, 4), dtype=np.float32)
+    aspect, sinfov, powc = pt_constants(width, height)
+    fr = PtFrame((ctypes.c_float * 3)(*pos), 1.0 if rst else 0.0, (ctypes.c_float * 3)(*lat), 0.0,
+                 width, height, aspect, sinfov, powc, 0.0)
+    sin = None if state is None else np.ascontiguousarray(state, dtype=np.float32)
+    lib().oracle_pt_step(nodes, tris, n, _ptr(sin), out, ctypes.byref(fr))
+    return out
+
+
+def pt_sincos(theta):
+    theta = np.ascontiguousarray(theta, dtype=np.float32)
+    s = np.empty_like(theta)
+    c = np.empty_like(theta)
+    lib().oracle_pt_sincos(theta, theta.size, s, c)
+    return s, c
+

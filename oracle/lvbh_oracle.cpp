@@ -421,61 +421,71 @@ static float aabb_intersect(V3 lo, V3 hi, V3 o, V3 d) {
     return (t1 >= t0) ? ((t1 < 0.0f) ? -1e30f : t0) : -1e30f;
 }
 
+// One ray: o, d as given to intersect_bvh (d is nudged away from zero here, :501).  Returns the
+// hit leaf's sorted position (-1 = miss) with its distance in *dist (-1 = miss) and the deepest
+// stack in *deepest.
+int32_t oracle_trace_one(const uint32_t *nodes, const float *tris, uint32_t n, const float *o_in,
+                         const float *d_in, float *dist_out, uint32_t *deepest_out) {
+    auto u2f = [](uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; };
+    V3 o = {o_in[0], o_in[1], o_in[2]};
+    V3 d = {d_in[0], d_in[1], d_in[2]};
+    // d += vec3f(abs(d) < vec3f(.00001)) * vec3f(.00001)   (:501)
+    d.x = d.x + (std::fabs(d.x) < 1e-5f ? 1.0f : 0.0f) * 1e-5f;
+    d.y = d.y + (std::fabs(d.y) < 1e-5f ? 1.0f : 0.0f) * 1e-5f;
+    d.z = d.z + (std::fabs(d.z) < 1e-5f ? 1.0f : 0.0f) * 1e-5f;
+    float dist = 1e30f;
+    int32_t prim = -1;
+    int32_t stack[64];
+    int32_t sp = 0, node_idx = 0;
+    uint32_t deepest = 0;
+    if (n == 0) sp = -1;
+    while (sp >= 0) {
+        if (node_idx < 0) {
+            const int32_t leaf = -(node_idx + 1);
+            float t = tri_intersect(o, d, tris + 12 * (size_t)leaf);
+            if (t > 0.0f && t < dist) { dist = fmin_w(t, dist); prim = leaf; }
+            sp -= 1;
+            node_idx = sp >= 0 ? stack[sp] : 0;
+        } else {
+            const uint32_t *nd = nodes + 16 * (size_t)node_idx;
+            V3 lmin = {u2f(nd[0]), u2f(nd[1]), u2f(nd[2])}, lmax = {u2f(nd[4]), u2f(nd[5]), u2f(nd[6])};
+            V3 rmin = {u2f(nd[8]), u2f(nd[9]), u2f(nd[10])}, rmax = {u2f(nd[12]), u2f(nd[13]), u2f(nd[14])};
+            int32_t lc = (int32_t)nd[3], rc = (int32_t)nd[11];
+            float ld = aabb_intersect(lmin, lmax, o, d);
+            float rd = aabb_intersect(rmin, rmax, o, d);
+            bool lv = ld != -1e30f && ld < dist;
+            bool rv = rd != -1e30f && rd < dist;
+            if (lv && rv) {
+                int32_t c, f;
+                if (ld < rd) { c = lc; f = rc; } else { c = rc; f = lc; }
+                if (sp < 64) stack[sp] = f;
+                sp += 1;
+                if ((uint32_t)sp > deepest) deepest = (uint32_t)sp;
+                if (sp > 64) { sp = -1; break; }   // deeper than this restatement holds
+                node_idx = c;
+            } else if (lv) {
+                node_idx = lc;
+            } else if (rv) {
+                node_idx = rc;
+            } else {
+                sp -= 1;
+                node_idx = sp >= 0 ? stack[sp] : 0;
+            }
+        }
+    }
+    *dist_out = dist == 1e30f ? -1.0f : dist;
+    if (deepest_out) *deepest_out = deepest;
+    return dist == 1e30f ? -1 : prim;
+}
+
 void oracle_trace(const uint32_t *nodes, const float *tris, uint32_t n, const float *rays,
                   uint32_t num_rays, int32_t *hit_prim, float *hit_t, uint32_t *max_stack,
                   int threads) {
-    auto u2f = [](uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; };
 #pragma omp parallel for schedule(dynamic, 1024) num_threads(num_threads(threads))
     for (int64_t r = 0; r < (int64_t)num_rays; ++r) {
         const float *ry = rays + 8 * r;
-        V3 o = {ry[0], ry[1], ry[2]};
-        V3 d = {ry[4], ry[5], ry[6]};
-        // d += vec3f(abs(d) < vec3f(.00001)) * vec3f(.00001)   (:501)
-        d.x = d.x + (std::fabs(d.x) < 1e-5f ? 1.0f : 0.0f) * 1e-5f;
-        d.y = d.y + (std::fabs(d.y) < 1e-5f ? 1.0f : 0.0f) * 1e-5f;
-        d.z = d.z + (std::fabs(d.z) < 1e-5f ? 1.0f : 0.0f) * 1e-5f;
-        float dist = 1e30f;
-        int32_t prim = -1;
-        int32_t stack[64];
-        int32_t sp = 0, node_idx = 0;
         uint32_t deepest = 0;
-        if (n == 0) sp = -1;
-        while (sp >= 0) {
-            if (node_idx < 0) {
-                const int32_t leaf = -(node_idx + 1);
-                float t = tri_intersect(o, d, tris + 12 * (size_t)leaf);
-                if (t > 0.0f && t < dist) { dist = fmin_w(t, dist); prim = leaf; }
-                sp -= 1;
-                node_idx = sp >= 0 ? stack[sp] : 0;
-            } else {
-                const uint32_t *nd = nodes + 16 * (size_t)node_idx;
-                V3 lmin = {u2f(nd[0]), u2f(nd[1]), u2f(nd[2])}, lmax = {u2f(nd[4]), u2f(nd[5]), u2f(nd[6])};
-                V3 rmin = {u2f(nd[8]), u2f(nd[9]), u2f(nd[10])}, rmax = {u2f(nd[12]), u2f(nd[13]), u2f(nd[14])};
-                int32_t lc = (int32_t)nd[3], rc = (int32_t)nd[11];
-                float ld = aabb_intersect(lmin, lmax, o, d);
-                float rd = aabb_intersect(rmin, rmax, o, d);
-                bool lv = ld != -1e30f && ld < dist;
-                bool rv = rd != -1e30f && rd < dist;
-                if (lv && rv) {
-                    int32_t c, f;
-                    if (ld < rd) { c = lc; f = rc; } else { c = rc; f = lc; }
-                    if (sp < 64) stack[sp] = f;
-                    sp += 1;
-                    if ((uint32_t)sp > deepest) deepest = (uint32_t)sp;
-                    if (sp > 64) { sp = -1; break; }   // deeper than this restatement holds
-                    node_idx = c;
-                } else if (lv) {
-                    node_idx = lc;
-                } else if (rv) {
-                    node_idx = rc;
-                } else {
-                    sp -= 1;
-                    node_idx = sp >= 0 ? stack[sp] : 0;
-                }
-            }
-        }
-        hit_prim[r] = dist == 1e30f ? -1 : prim;
-        hit_t[r] = dist == 1e30f ? -1.0f : dist;
+        hit_prim[r] = oracle_trace_one(nodes, tris, n, ry, ry + 4, hit_t + r, &deepest);
         if (max_stack) max_stack[r] = deepest;
     }
 }

@@ -40,6 +40,10 @@ int main(void) {
         uint32_t n = 0;
         double b6[6];
         uint64_t line = 7;
+        lvbh_pt_frame fr;
+        memset(&fr, 0, sizeof fr);
+        printf("sizeof_pt_frame %zu\n", sizeof(lvbh_pt_frame));
+        printf("pt_null_ctx %d\n", lvbh_pt_sample(NULL, NULL, NULL, 0, NULL, NULL, 1, 1, &fr, NULL));
         printf("parse_obj_null_ctx %d\n", lvbh_parse_obj(NULL, "v 0 0 0\n", 8, LVBH_INPUT_HOST, &tri, &n, b6, &line, NULL));
     }
     {

@@ -898,6 +898,41 @@ int lvbh_trace(lvbh_ctx *ctx, const void *nodes, const void *tris, uint32_t num_
     return LVBH_OK;
 }
 
+int lvbh_pt_sample(lvbh_ctx *ctx, const void *nodes, const void *tris, uint32_t num_tris,
+                   const float *state_in, float *state_out, uint32_t width, uint32_t height,
+                   const lvbh_pt_frame *frame, void *stream) {
+    if (!ctx) return LVBH_EINVAL;
+    if (!frame) return fail(ctx, LVBH_EINVAL, "frame is NULL");
+    const uint64_t pixels = (uint64_t)width * height;
+    if (pixels >= (1ull << 31)) return fail(ctx, LVBH_EINVAL, "image too large");
+    if (pixels && (!state_out || (frame->rst == 0.0f && !state_in))) return fail(ctx, LVBH_EINVAL, "NULL state buffer");
+    if (num_tris && (!nodes || !tris)) return fail(ctx, LVBH_EINVAL, "NULL tree buffer");
+    if (num_tris > LVBH_MAX_TRIS) return fail(ctx, LVBH_EINVAL, "num_tris exceeds LVBH_MAX_TRIS");
+    if (!pixels) return LVBH_OK;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!ctx->trace_counter) LVBH_CUDA(ctx, cudaMalloc(&ctx->trace_counter, sizeof(uint32_t)));
+    PtFrame f{};
+    for (int a = 0; a < 3; ++a) { f.pos[a] = frame->pos[a]; f.lat[a] = frame->lat[a]; }
+    f.rst = frame->rst;
+    f.width = width;
+    f.height = height;
+    f.sw_x = (float)width;
+    f.sw_y = (float)height;
+    // the constants the shader bakes in (pathtracer.js:477-485, :716): aspect = w / h,
+    // sinfov = sin(.5 * fov * Pi / 180.f) with the argument in float, pow(.3f, 2.2)
+    f.aspect = (float)((double)width / (double)height);
+    const float half_fov = ((0.5f * 60.0f) * (float)3.14159265358979323846) / 180.0f;
+    f.sinfov = (float)std::sin((double)half_fov);
+    f.powc = (float)std::pow((double)0.3f, (double)2.2f);
+    launch_pt_step(static_cast<const float4 *>(nodes), static_cast<const float4 *>(tris), num_tris,
+                   reinterpret_cast<const float4 *>(state_in), reinterpret_cast<float4 *>(state_out), f,
+                   ctx->trace_counter, s);
+    LVBH_CUDA(ctx, cudaGetLastError());
+    LVBH_CUDA(ctx, cudaStreamSynchronize(s));
+    return LVBH_OK;
+}
+
 int lvbh_parse_obj(lvbh_ctx *ctx, const char *text, uint64_t bytes, uint32_t flags,
                    const float **tri_out, uint32_t *num_tris, double *bounds6, uint64_t *err_line,
                    void *stream) {

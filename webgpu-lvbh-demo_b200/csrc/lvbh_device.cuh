@@ -121,6 +121,15 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // of equal bins over consecutive lanes: the run's first lane adds its length.  Input in
 // spatially coherent order (a mesh's triangles, keys grouped by the previous sort digit) gives
 // long runs, which plain per-lane atomics would serialise on one bin.  All 32 lanes call it.
+// True when the warp's bins d form at most 8 runs over consecutive lanes (warp-uniform): the
+// case add_runs pays for; scattered bins are cheaper with one atomic per lane.
+__device__ __forceinline__ bool runs_few(uint32_t d, bool valid) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t dv = valid ? d : 0xFFFFFFFFu;
+    const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, dv, 1);
+    return __popc(__ballot_sync(0xFFFFFFFFu, lane == 0 || dv != up)) <= 8;
+}
+
 __device__ __forceinline__ void add_runs(uint32_t *h, uint32_t d, bool valid) {
     const int lane = threadIdx.x & 31;
     const uint32_t dv = valid ? d : 0xFFFFFFFFu;  // invalid lanes form runs of their own

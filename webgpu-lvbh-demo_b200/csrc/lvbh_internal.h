@@ -173,6 +173,17 @@ void launch_trace(const float4 *nodes, const float4 *tris, uint32_t n, const flo
                   uint32_t num_rays, int32_t *hit_prim, float *hit_t, uint32_t *max_stack,
                   uint32_t *counter, cudaStream_t s);
 
+// Path-trace bounce (trace.cu): the uniform buffer (pos, rst, lat) and the constants the
+// reference's shader bakes in (image size, aspect, sin(fov / 2), pow(.3, 2.2)).
+struct PtFrame {
+    float pos[3], rst, lat[3];
+    uint32_t width, height;
+    float sw_x, sw_y, aspect, sinfov, powc;
+};
+// One bounce of every pixel: state planes o, d, t, b of width x height float4 each.
+void launch_pt_step(const float4 *nodes, const float4 *tris, uint32_t n, const float4 *state_in,
+                    float4 *state_out, const PtFrame &f, uint32_t *counter, cudaStream_t s);
+
 // OBJ ingest (obj.cu): device memory of one parse, grown on demand and held by the context.
 struct ObjScratch {
     void *text = nullptr;  // staged host text, newline counts, control block

@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
         if (tile >= tiles) break;  // uniform across the block
         for (int i = threadIdx.x; i < kDigits; i += kThreads) th[i] = 0;
         __syncthreads();
+        bool coherent = false;
         for (uint32_t c = warp; c < (uint32_t)kSortTile / 32; c += kWarps) {
             const uint32_t t0 = tile * (uint32_t)kSortTile + 32u * c;
             if (t0 >= n) break;
@@ -139,9 +140,18 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
                 key = morton3(qx, qy, qz);
                 keys[t] = key;
             }
+            // coherent input (a mesh in its file order) shares the top digit over long runs;
+            // the warp tests its first chunk of each tile and keeps the answer for the tile
+            if (c == (uint32_t)warp) coherent = runs_few(key >> (kDigitBits * (kSortPasses - 1)), valid);
+            if (coherent) {
 #pragma unroll
-            for (int p = 0; p < kSortPasses; ++p) add_runs(hist[p], (key >> (kDigitBits * p)) & (kDigits - 1), valid);
-            add_runs(th, key & (kDigits - 1), valid);
+                for (int p = 0; p < kSortPasses; ++p) add_runs(hist[p], (key >> (kDigitBits * p)) & (kDigits - 1), valid);
+                add_runs(th, key & (kDigits - 1), valid);
+            } else if (valid) {
+#pragma unroll
+                for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (kDigitBits * p)) & (kDigits - 1)], 1u);
+                atomicAdd(&th[key & (kDigits - 1)], 1u);
+            }
         }
         __syncthreads();
         uint32_t *row = tile_hist + (size_t)tile * kDigits + threadIdx.x * P;
@@ -246,7 +256,7 @@ __global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restr
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const float4 *src = tri + 3ull * first;
     const uint32_t nv = 3u * cnt;
-    bool bad = false;
+    bool bad = false, coherent = false;
     for (uint32_t c = warp; c < (cnt + 31) / 32; c += kWarps) {
         const uint32_t base = 96u * c;
 #pragma unroll
@@ -269,8 +279,14 @@ __global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restr
             key = morton3(qx, qy, qz);
             keys[first + t] = key;
         }
+        if (c == (uint32_t)warp) coherent = runs_few(key >> (BITS * (NP - 1)), valid);
+        if (coherent) {
 #pragma unroll
-        for (int p = 0; p < NP; ++p) add_runs(hist[p], (key >> (BITS * p)) & (D - 1), valid);
+            for (int p = 0; p < NP; ++p) add_runs(hist[p], (key >> (BITS * p)) & (D - 1), valid);
+        } else if (valid) {
+#pragma unroll
+            for (int p = 0; p < NP; ++p) atomicAdd(&hist[p][(key >> (BITS * p)) & (D - 1)], 1u);
+        }
     }
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
     __syncthreads();

@@ -320,8 +320,16 @@ __global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ ke
             const uint32_t idx = base + i * T + tid;
             k[i] = idx < n ? __ldcs(keys + idx) : 0xFFFFFFFFu;
         }
+        // keys grouped by the previous digit repeat this one over long runs when the input was
+        // spatially coherent; the warp tests its first 32 keys and keeps the answer for the tile
+        const bool coherent = runs_few((k[0] >> shift) & (D - 1), base + tid < n);
 #pragma unroll
-        for (int i = 0; i < IPT; ++i) add_runs(h, (k[i] >> shift) & (D - 1), base + i * T + tid < n);
+        for (int i = 0; i < IPT; ++i) {
+            const uint32_t d = (k[i] >> shift) & (D - 1);
+            const bool valid = base + i * T + tid < n;
+            if (coherent) add_runs(h, d, valid);
+            else if (valid) atomicAdd(&h[d], 1u);
+        }
         __syncthreads();
         uint32_t c[P];
 #pragma unroll

@@ -68,7 +68,7 @@ struct RayState {
 
 __device__ __forceinline__ void ray_init(RayState &st, const float4 *__restrict__ rays, uint32_t r,
                                          uint32_t n) {
-    const float4 ro = __ldg(rays + 2ull * r), rd = __ldg(rays + 2ull * r + 1);
+    const float4 ro = rays[2ull * r], rd = rays[2ull * r + 1];
     st.o = {ro.x, ro.y, ro.z};
     F3 d = {rd.x, rd.y, rd.z};
     // d += vec3f(abs(d) < vec3f(.00001)) * vec3f(.00001)   (:501)
@@ -175,6 +175,213 @@ __global__ void __launch_bounds__(128) k_trace(const float4 *__restrict__ nodes,
     }
 }
 
+// ---- path-trace bounce (sample(), pathtracer.js:360-392 -> main / ptStep, :630-713) ----------
+// The WGSL leaves sin, cos, pow and normalize to the implementation; these definitions fix
+// them: normalize(v) = v / sqrt(dot(v, v)) (IEEE square root and divisions), sin / cos by
+// Cody-Waite reduction over pi/2 (three-part float split, k * C1 and k * C2 exact) and Taylor
+// polynomials to degree 11 / 10, pow(.3, 2.2) a host constant.  Every operation is an
+// explicitly rounded intrinsic, so a CPU restatement in the same order gives the same bits.
+
+__device__ __forceinline__ F3 add3(F3 a, F3 b) { return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)}; }
+__device__ __forceinline__ F3 mul3(F3 a, float s) { return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)}; }
+__device__ __forceinline__ F3 normalize3(F3 v) {
+    const float len = __fsqrt_rn(dot3(v, v));
+    return {__fdiv_rn(v.x, len), __fdiv_rn(v.y, len), __fdiv_rn(v.z, len)};
+}
+__device__ __forceinline__ F3 to_world(F3 vx, F3 vy, F3 vz, F3 w) {
+    return add3(add3(mul3(vx, w.x), mul3(vy, w.y)), mul3(vz, w.z));
+}
+__device__ __forceinline__ F3 ortho3(F3 v) {
+    if (fabsf(v.x) > fabsf(v.y)) return {-v.y, v.x, 0.0f};
+    return {0.0f, -v.z, v.y};
+}
+
+__device__ __forceinline__ void pt_sincos(float theta, float &s_out, float &c_out) {
+    const float kTwoOverPi = 0x1.45f306p-1f;
+    const float C1 = 0x1.92p+0f, C2 = 0x1.fb544p-12f, C3 = 0x1.0b4612p-34f;
+    const int k = __float2int_rn(__fmul_rn(theta, kTwoOverPi));
+    const float kf = __int2float_rn(k);
+    const float r = __fsub_rn(__fsub_rn(__fsub_rn(theta, __fmul_rn(kf, C1)), __fmul_rn(kf, C2)), __fmul_rn(kf, C3));
+    const float r2 = __fmul_rn(r, r);
+    float ps = __fadd_rn(0x1.71de3ap-19f, __fmul_rn(r2, -0x1.ae6456p-26f));
+    ps = __fadd_rn(-0x1.a01a02p-13f, __fmul_rn(r2, ps));
+    ps = __fadd_rn(0x1.111112p-7f, __fmul_rn(r2, ps));
+    ps = __fadd_rn(-0x1.555556p-3f, __fmul_rn(r2, ps));
+    const float s = __fadd_rn(r, __fmul_rn(__fmul_rn(r, r2), ps));
+    float pc = __fadd_rn(0x1.a01a02p-16f, __fmul_rn(r2, -0x1.27e4fcp-22f));
+    pc = __fadd_rn(-0x1.6c16c2p-10f, __fmul_rn(r2, pc));
+    pc = __fadd_rn(0x1.555556p-5f, __fmul_rn(r2, pc));
+    pc = __fadd_rn(-0x1p-1f, __fmul_rn(r2, pc));
+    const float c = __fadd_rn(1.0f, __fmul_rn(r2, pc));
+    switch (k & 3) {
+        case 0: s_out = s; c_out = c; break;
+        case 1: s_out = c; c_out = -s; break;
+        case 2: s_out = -s; c_out = -c; break;
+        default: s_out = -c; c_out = s; break;
+    }
+}
+
+// baseHash (:752-756).
+__device__ __forceinline__ uint32_t base_hash(uint32_t px, uint32_t py) {
+    const uint32_t p2x = 1103515245u * ((px >> 1) ^ py);
+    const uint32_t p2y = 1103515245u * ((py >> 1) ^ px);
+    const uint32_t h32 = 1103515245u * (p2x ^ (p2y >> 3));
+    return h32 ^ (h32 >> 16);
+}
+
+// rand2 (:757-761).
+__device__ __forceinline__ void rand2(float seed, float &rx, float &ry) {
+    const uint32_t n = base_hash(__float_as_uint(__fadd_rn(seed, 1.0f)), __float_as_uint(__fadd_rn(seed, 2.0f)));
+    rx = __fdiv_rn(__uint2float_rn(n & 0x7fffffffu), 2147483648.0f);
+    ry = __fdiv_rn(__uint2float_rn((n * 48271u) & 0x7fffffffu), 2147483648.0f);
+}
+
+// One pixel's path between bounces (the four state images' texels).
+struct PixelPath {
+    F3 o, d, b;
+    float4 t;
+    float seed, bounces;
+    uint32_t px;
+};
+
+// ptStep up to the traversal (:656-674): a new path draws its camera ray.
+__device__ __forceinline__ void pt_begin(PixelPath &pp, const float4 *__restrict__ in, size_t plane, uint32_t px,
+                                         const PtFrame &f) {
+    pp.px = px;
+    const uint32_t cx = px % f.width, cy = px / f.width;
+    float4 o4 = make_float4(0.f, 0.f, 0.f, 0.f), d4 = o4, t4 = o4, b4 = o4;
+    if (f.rst == 0.0f) {
+        o4 = __ldcs(in + px);
+        d4 = __ldcs(in + plane + px);
+        t4 = __ldcs(in + 2 * plane + px);
+        b4 = __ldcs(in + 3 * plane + px);
+    }
+    pp.o = {o4.x, o4.y, o4.z};
+    pp.d = {d4.x, d4.y, d4.z};
+    pp.b = {b4.x, b4.y, b4.z};
+    pp.t = t4;
+    pp.seed = o4.w;
+    pp.bounces = d4.w;
+    const bool new_path = pp.b.x == 0.0f && pp.b.y == 0.0f && pp.b.z == 0.0f;
+    if (new_path && t4.w == 0.0f)
+        pp.seed = __fadd_rn(__fdiv_rn(__uint2float_rn(base_hash(cx, cy)), 4294967296.0f), 0.008f);
+    if (new_path) {
+        float rx, ry;
+        rand2(pp.seed, rx, ry);
+        float sx = __fdiv_rn(__fadd_rn(__uint2float_rn(cx), rx), f.sw_x);
+        float sy = __fdiv_rn(__fadd_rn(__uint2float_rn(cy), ry), f.sw_y);
+        sx = __fsub_rn(__fmul_rn(sx, 2.0f), 1.0f);
+        sy = -__fsub_rn(__fmul_rn(sy, 2.0f), 1.0f);
+        const F3 local = {__fmul_rn(__fmul_rn(f.aspect, sx), f.sinfov), 1.0f, __fmul_rn(sy, f.sinfov)};
+        const F3 pos = {f.pos[0], f.pos[1], f.pos[2]}, lat = {f.lat[0], f.lat[1], f.lat[2]};
+        const F3 forward = normalize3(sub3(lat, pos));
+        const F3 right = normalize3(F3{forward.y, -forward.x, 0.0f});
+        const F3 up = cross3(right, forward);
+        pp.o = pos;
+        pp.d = to_world(right, forward, up, normalize3(local));
+        pp.seed = __fadd_rn(pp.seed, 2.0f);
+        pp.b = {1.0f, 1.0f, 1.0f};
+    }
+}
+
+// ptStep after the traversal (:675-712) and the texel stores.
+__device__ __forceinline__ void pt_end(PixelPath &pp, const RayState &st, const float4 *__restrict__ tris,
+                                       float4 *__restrict__ out, size_t plane, const PtFrame &f) {
+    const float eps = 0.0001f, two_pi = 0x1.921fb6p+2f;
+    F3 b = pp.b;
+    float4 t = pp.t;
+    float seed = pp.seed, bounces = pp.bounces;
+    F3 o = pp.o, d = pp.d;
+    if (st.dist != 1e30f) {
+        const float4 *tr = tris + 3ull * st.prim;
+        const float4 a = __ldg(tr), bb = __ldg(tr + 1), c = __ldg(tr + 2);
+        const F3 v0 = {a.x, a.y, a.z}, v1 = {bb.x, bb.y, bb.z}, v2 = {c.x, c.y, c.z};
+        F3 norm = normalize3(cross3(sub3(v1, v0), sub3(v2, v0)));
+        if (!(dot3(st.d, F3{-norm.x, -norm.y, -norm.z}) > 0.0f)) norm = {-norm.x, -norm.y, -norm.z};
+        const F3 o1 = normalize3(ortho3(norm));
+        const F3 o2 = normalize3(cross3(o1, norm));
+        o = add3(o, mul3(d, st.dist));
+        float r2x, r2y;
+        rand2(seed, r2x, r2y);
+        const float rr = __fsqrt_rn(r2x > 0.0f ? r2x : 0.0f);
+        float sn, cs;
+        pt_sincos(__fmul_rn(two_pi, r2y), sn, cs);
+        const float dx = __fmul_rn(rr, cs), dy = __fmul_rn(rr, sn);
+        const float zz = __fsub_rn(__fsub_rn(1.0f, __fmul_rn(dx, dx)), __fmul_rn(dy, dy));
+        const F3 wi = {dx, dy, __fsqrt_rn(zz > 0.0f ? zz : 0.0f)};
+        seed = __fadd_rn(seed, 2.0f);
+        b = mul3(b, f.powc);
+        o = add3(o, mul3(mul3(norm, 1.01f), eps));
+        d = to_world(o1, o2, norm, wi);
+        if (bounces > 3.0f) {
+            const float q1 = __fsub_rn(1.0f, b.y), q = 0.05f > q1 ? 0.05f : q1;
+            float ux, uy;
+            rand2(seed, ux, uy);
+            if (ux < q) {
+                b = {0.0f, 0.0f, 0.0f};
+            } else {
+                const float keep = __fsub_rn(1.0f, q);
+                b = {__fdiv_rn(b.x, keep), __fdiv_rn(b.y, keep), __fdiv_rn(b.z, keep)};
+            }
+            seed = __fadd_rn(seed, 2.0f);
+        }
+        if (b.x == 0.0f && b.y == 0.0f && b.z == 0.0f) {
+            t = make_float4(__fadd_rn(t.x, 0.0f), __fadd_rn(t.y, 0.0f), __fadd_rn(t.z, 0.0f), __fadd_rn(t.w, 1.0f));
+            bounces = -1.0f;
+        }
+    } else {
+        t = make_float4(__fadd_rn(t.x, __fmul_rn(b.x, 8.0f)), __fadd_rn(t.y, __fmul_rn(b.y, 8.0f)),
+                        __fadd_rn(t.z, __fmul_rn(b.z, 8.0f)), __fadd_rn(t.w, 1.0f));
+        bounces = -1.0f;
+        b = {0.0f, 0.0f, 0.0f};
+    }
+    const uint32_t px = pp.px;
+    __stcs(out + px, make_float4(o.x, o.y, o.z, seed));
+    __stcs(out + plane + px, make_float4(d.x, d.y, d.z, __fadd_rn(bounces, 1.0f)));
+    __stcs(out + 2 * plane + px, t);
+    __stcs(out + 3 * plane + px, make_float4(b.x, b.y, b.z, 1.0f));
+}
+
+// One bounce of every pixel: persistent warps fetch pixels from *counter as lanes finish (the
+// traversal's dynamic fetch), each pixel's walk exactly the reference's.
+__global__ void __launch_bounds__(128) k_pt_step(const float4 *__restrict__ nodes, const float4 *__restrict__ tris,
+                                                 uint32_t n, const float4 *__restrict__ in, float4 *__restrict__ out,
+                                                 PtFrame f, uint32_t *__restrict__ counter) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+    const uint32_t num = f.width * f.height;
+    const size_t plane = num;
+    int32_t stack[kStack];
+    RayState st;
+    PixelPath pp;
+    bool have = false, exhausted = false;
+    for (;;) {
+        const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !have);
+        if (!exhausted && __popc(idle) >= 8) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(counter, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base + __popc(idle) >= num) exhausted = true;
+            if (!have) {
+                const uint32_t my = base + __popc(idle & lt);
+                if (my < num) {
+                    pt_begin(pp, in, plane, my, f);
+                    const float4 ray[2] = {make_float4(pp.o.x, pp.o.y, pp.o.z, 0.f),
+                                           make_float4(pp.d.x, pp.d.y, pp.d.z, 0.f)};
+                    ray_init(st, ray, 0, n);
+                    have = true;
+                }
+            }
+        } else if (exhausted && idle == 0xFFFFFFFFu) {
+            break;
+        }
+        if (have && !ray_step(st, stack, nodes, tris, n)) {
+            pt_end(pp, st, tris, out, plane, f);
+            have = false;
+        }
+    }
+}
+
 }  // namespace
 
 void launch_trace(const float4 *nodes, const float4 *tris, uint32_t n, const float4 *rays,
@@ -191,6 +398,21 @@ void launch_trace(const float4 *nodes, const float4 *tris, uint32_t n, const flo
     cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     k_trace<<<want < cap ? want : cap, 128, 0, s>>>(nodes, tris, n, rays, num_rays, hit_prim, hit_t,
                                                     max_stack, counter);
+}
+
+void launch_pt_step(const float4 *nodes, const float4 *tris, uint32_t n, const float4 *state_in,
+                    float4 *state_out, const PtFrame &f, uint32_t *counter, cudaStream_t s) {
+    const uint32_t num = f.width * f.height;
+    if (num == 0) return;
+    static int per_sm = 0;
+    if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pt_step, 128, 0) != cudaSuccess ||
+                    per_sm < 1)) {
+        cudaGetLastError();
+        per_sm = 4;
+    }
+    const uint32_t want = (num + 127) / 128, cap = (uint32_t)(sm_count() * per_sm);
+    cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+    k_pt_step<<<want < cap ? want : cap, 128, 0, s>>>(nodes, tris, n, state_in, state_out, f, counter);
 }
 
 }  // namespace lvbh

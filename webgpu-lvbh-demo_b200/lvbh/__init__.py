@@ -341,6 +341,25 @@ class BVHBuilder:
         return prim, t, st
 
 
+    def pt_sample(self, res: BuildResult, state_in, state_out, width: int, height: int, pos, lat,
+                  reset: bool = False, stream=None):
+        """One sample() of the reference's path tracer (pathtracer.js:360-392): every pixel's
+        path advances one bounce through the built tree.  state_in / state_out: (4, height,
+        width, 4) float32 CUDA tensors, planes o, d, t, b (state_in unread when reset)."""
+        for st in (state_in, state_out):
+            if st is not None and (tuple(st.shape) != (4, height, width, 4) or not st.is_contiguous()):
+                raise ValueError("state must be a contiguous (4, height, width, 4) float32 tensor")
+        fr = _native.PtFrame((ctypes.c_float * 3)(*[float(x) for x in pos]), 1.0 if reset else 0.0,
+                             (ctypes.c_float * 3)(*[float(x) for x in lat]), 0.0)
+        n = res.tris.shape[0]
+        rc = _native.lib.lvbh_pt_sample(self._ctx, ctypes.c_void_p(res.nodes.data_ptr() if n else 0),
+                                        ctypes.c_void_p(res.tris.data_ptr() if n else 0), n,
+                                        ctypes.c_void_p(state_in.data_ptr() if state_in is not None else 0),
+                                        ctypes.c_void_p(state_out.data_ptr()), width, height, ctypes.byref(fr),
+                                        _stream_ptr(stream, self.device))
+        _native.check(self._ctx, rc)
+        return state_out
+
     def parse_obj(self, text, stream=None) -> dict:
         """parseObj(file) (scripts/obj/parse-obj.js:3-88) on the GPU.
 
@@ -415,3 +434,16 @@ def trace(builder: BVHBuilder, res: BuildResult, rays):
 def parseObj(builder: BVHBuilder, file) -> dict:  # noqa: N802
     """parseObj(file) (scripts/obj/parse-obj.js:3-88) on the builder's GPU."""
     return builder.parse_obj(file)
+
+
+def camera(bounds, rot: float = 0.0):
+    """The path tracer's camera for a model (initPathTracer, pathtracer.js:5-23, rotateView
+    :418-426): look at the box centre from 1.5 x its largest extent away, rotated by `rot` about
+    z.  bounds: {"min", "max"} or 6 numbers.  Returns (pos, lat) as float lists."""
+    import math
+    b = list(bounds["min"]) + list(bounds["max"]) if isinstance(bounds, dict) else [float(x) for x in bounds]
+    dist = 1.5 * max(max(b[3] - b[0], b[4] - b[1]), b[5] - b[2])
+    lat = [(b[0] + b[3]) * .5, (b[1] + b[4]) * .5, (b[2] + b[5]) * .5]
+    pos = [lat[0] + math.cos(rot) * dist, lat[1] + math.sin(rot) * dist, lat[2]]
+    return pos, lat
+

@@ -33,6 +33,12 @@ class LvbhError(RuntimeError):
         self.code = code
 
 
+class PtFrame(ctypes.Structure):
+    """lvbh_pt_frame: the path tracer's uniform buffer (pos, rst, lat)."""
+    _fields_ = [("pos", ctypes.c_float * 3), ("rst", ctypes.c_float), ("lat", ctypes.c_float * 3),
+                ("pad", ctypes.c_float)]
+
+
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("reserve_tris", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint64 * 4)]
@@ -126,6 +132,8 @@ def _load():
     L.lvbh_server_last_error.argtypes = [vp]
     L.lvbh_trace.restype = i32
     L.lvbh_trace.argtypes = [vp, vp, vp, u32, vp, u32, vp, vp, vp, vp]
+    L.lvbh_pt_sample.restype = i32
+    L.lvbh_pt_sample.argtypes = [vp, vp, vp, u32, vp, vp, u32, u32, ctypes.POINTER(PtFrame), vp]
     L.lvbh_parse_obj.restype = i32
     L.lvbh_parse_obj.argtypes = [vp, vp, ctypes.c_uint64, u32, ctypes.POINTER(vp), ctypes.POINTER(u32),
                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64), vp]
