@@ -25,9 +25,11 @@ Prints one JSON line (rank 0).  Fields beyond the base contract:
   obj           OBJ ingest: the sphere's 80 MB OBJ text -> soup + bounds on the GPU, and end to
                 end through parse + build from pinned host text, beside the oracle's parse
   pt            path-trace bounces: 1920 x 1080 pixels, one bounce each per step, on the sphere
+  mesh          the indexed leaf format (no 48-byte triangle copies) beside the soup build of
+                the same indexed mesh, and traversal through both layouts
 Under torchrun (N > 1) each rank builds its own replica (the build has no shardable exchange).
 
-    python bench.py --workload batch | served | trace | obj | pt     one part alone
+    python bench.py --workload batch | served | trace | obj | pt | mesh     one part alone
 """
 from __future__ import annotations
 
@@ -352,9 +354,12 @@ def run_ours(args, world, rank, local):
     if not args.no_obj:
         obj = run_obj(args, world, rank, local)
         torch.cuda.empty_cache()
-    pt = None
+    pt = mesh = None
     if not args.no_pt:
         pt = run_pt(args, world, rank, local)
+        torch.cuda.empty_cache()
+    if not args.no_mesh:
+        mesh = run_mesh(args, world, rank, local)
     if rank != 0:
         return
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -366,7 +371,7 @@ def run_ours(args, world, rank, local):
             "gpu_launches": LAUNCHES_PER_BUILD * args.steps,
             "roofline": roofline, "stage_ms": stage_ms, "cpu_baseline": cpu, "e2e": e2e_line,
             "clocks": clock_summary, "batched": batched, "served": served, "trace": trace, "obj": obj,
-            "pt": pt}
+            "pt": pt, "mesh": mesh}
     print(json.dumps(line), flush=True)
 
 
@@ -700,6 +705,64 @@ def run_pt(args, world, rank, local):
     return out
 
 
+def run_mesh(args, world, rank, local):
+    """The indexed leaf format on the 2,097,152-triangle displaced sphere as an indexed mesh
+    (1,050,625 vertex rows of 16 B, 2,097,152 index triples): lvbh_build_mesh (no 48-byte
+    triangle is gathered or written; the leaves are index triples) beside lvbh_build_indexed
+    (gather to the soup, soup build with the rearranged soup out) on the same mesh, identical
+    trees; then closest-hit traversal of args.rays rays through both layouts."""
+    import numpy as np
+    import torch
+
+    import lvbh
+    from lvbh import empty_outputs, scenes
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    xyz, idx = scenes.sphere_mesh(1024, seed=1, indexed=True)
+    n = idx.shape[0]
+    v4 = np.zeros((xyz.shape[0], 4), np.float32)
+    v4[:, :3] = xyz
+    dv4 = torch.from_numpy(v4).to(dev)
+    dxyz = torch.from_numpy(np.ascontiguousarray(xyz)).to(dev)
+    didx = torch.from_numpy(idx.astype(np.uint32).view(np.int32)).to(dev)
+    builder = lvbh.BVHBuilder(local, reserve_tris=n)
+    stream = torch.cuda.current_stream(dev)
+    om, os_ = empty_outputs(n, dev, mesh=True), empty_outputs(n, dev)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        times = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return max_over_ranks(statistics.median(times), world)
+
+    ms_mesh = timed(lambda: builder.build_mesh(dv4, didx, outputs=om, stream=stream))
+    ms_soup = timed(lambda: builder.build_indexed(dxyz, didx, outputs=os_, stream=stream))
+    rm = builder.build_mesh(dv4, didx, outputs=om, stream=stream)
+    rs = builder.build_indexed(dxyz, didx, outputs=os_, stream=stream)
+    same = all(torch.equal(om[k], os_[k]) for k in ("nodes", "parents", "leaf_index", "morton"))
+    rays = torch.from_numpy(scenes.sphere_rays(args.rays, seed=11)).to(dev)
+    tm = timed(lambda: builder.trace_mesh(rm, dv4, rays))
+    ts = timed(lambda: builder.trace(rs, rays))
+    out = {"workload": "sphere_mesh_2M_indexed", "num_tris": n, "num_verts": int(v4.shape[0]),
+           "build_mesh_ms": ms_mesh, "build_indexed_soup_ms": ms_soup,
+           "mesh_mprims_per_s": world * n / (ms_mesh * 1e-3) / 1e6,
+           "soup_mprims_per_s": world * n / (ms_soup * 1e-3) / 1e6,
+           "identical_trees": bool(same),
+           "leaf_bytes": {"mesh": 12 * n + 16 * int(v4.shape[0]), "soup": 48 * n},
+           "trace_mrays_per_s": {"mesh": world * args.rays / (tm * 1e-3) / 1e6,
+                                 "soup": world * args.rays / (ts * 1e-3) / 1e6}}
+    builder.close()
+    return out
+
+
 def percentiles(x):
     import numpy as np
     a = np.asarray(x, dtype=np.float64)
@@ -856,6 +919,7 @@ def main():
     ap.add_argument("--pt-width", type=int, default=1920)
     ap.add_argument("--pt-height", type=int, default=1080)
     ap.add_argument("--no-pt", action="store_true")
+    ap.add_argument("--no-mesh", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -869,6 +933,10 @@ def main():
                 print(json.dumps(out), flush=True)
         elif args.workload == "trace":
             out = run_trace(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(out), flush=True)
+        elif args.workload == "mesh":
+            out = run_mesh(args, world, rank, local)
             if rank == 0:
                 print(json.dumps(out), flush=True)
         elif args.workload == "pt":

@@ -140,6 +140,22 @@ LVBH_API int  lvbh_build_indexed(lvbh_ctx *ctx, const float *xyz, uint32_t num_v
                         const uint32_t *idx3, uint32_t num_tris, const float *model_bounds,
                         uint32_t flags, lvbh_result *out, void *stream);
 
+/* Indexed leaf format: the same tree from an indexed mesh without any 48-byte triangle copy.
+ * No counterpart in the reference, whose rearrange pass (scripts/bvh/kernels/rearrange.js:
+ * 162-169) copies every triangle into O_TRIANGLE_BUFFER; here a leaf refers to its vertices.
+ *   verts4     num_verts rows of 16 B {x, y, z, pad} (16-byte aligned when device memory)
+ *   idx3       num_tris uint32 triples into verts4
+ * nodes, parents, leaf_index and morton equal those of lvbh_build_soup over the triangles the
+ * mesh spells out (bounds: min / max over the vertices the triangles use).  out->tris receives,
+ * per sorted leaf, the triangle's three vertex indices (12 B per triangle, i.e. idx3 of
+ * leaf_index) instead of its 48-byte rows: leaf -(i+1) of a node has the vertices
+ * verts4[tris[3i]], verts4[tris[3i+1]], verts4[tris[3i+2]].  With LVBH_OUT_CALLER, out->tris
+ * must hold 12 N bytes (4-byte aligned).  An index >= num_verts fails the build with
+ * LVBH_EINVAL. */
+LVBH_API int  lvbh_build_mesh(lvbh_ctx *ctx, const float *verts4, uint32_t num_verts,
+                        const uint32_t *idx3, uint32_t num_tris, const float *model_bounds,
+                        uint32_t flags, lvbh_result *out, void *stream);
+
 /* Batched build: num_segs independent meshes laid end to end in one triangle soup, built in
  * one stream-ordered launch sequence (replayed as a cached CUDA graph) instead of one
  * build(TRI_ARRAY, NUM_TRIS, MODEL_BOUNDS) per mesh (scripts/bvh/build-bvh.js:12-66 called
@@ -306,6 +322,13 @@ LVBH_API int  lvbh_sort_pairs_noalloc(const uint32_t *keys_in, uint32_t num_keys
 LVBH_API int  lvbh_trace(lvbh_ctx *ctx, const void *nodes, const void *tris, uint32_t num_tris,
                 const float *rays, uint32_t num_rays, int32_t *hit_prim, float *hit_t,
                 uint32_t *max_stack, void *stream);
+
+/* lvbh_trace over the indexed leaf format (lvbh_build_mesh): leaf i's vertices are
+ * verts4[leaf_idx3[3i..3i+2]] (16-byte rows, device memory); results equal lvbh_trace's over
+ * the same triangles as a soup.  Indices >= num_verts read row 0. */
+LVBH_API int  lvbh_trace_mesh(lvbh_ctx *ctx, const void *nodes, const uint32_t *leaf_idx3,
+                const float *verts4, uint32_t num_verts, uint32_t num_tris, const float *rays,
+                uint32_t num_rays, int32_t *hit_prim, float *hit_t, uint32_t *max_stack, void *stream);
 
 /* ---- consumer: one path-trace bounce per pixel -------------------------------------
  * Replaces sample() (scripts/pathtracer/pathtracer.js:360-392): the compute shader main /

@@ -43,6 +43,8 @@ int main(void) {
         lvbh_pt_frame fr;
         memset(&fr, 0, sizeof fr);
         printf("sizeof_pt_frame %zu\n", sizeof(lvbh_pt_frame));
+        printf("mesh_null_ctx %d\n", lvbh_build_mesh(NULL, NULL, 0, NULL, 0, NULL, 0, &r, NULL));
+        printf("trace_mesh_null_ctx %d\n", lvbh_trace_mesh(NULL, NULL, NULL, NULL, 0, 0, NULL, 0, NULL, NULL, NULL, NULL));
         printf("pt_null_ctx %d\n", lvbh_pt_sample(NULL, NULL, NULL, 0, NULL, NULL, 1, 1, &fr, NULL));
         printf("parse_obj_null_ctx %d\n", lvbh_parse_obj(NULL, "v 0 0 0\n", 8, LVBH_INPUT_HOST, &tri, &n, b6, &line, NULL));
     }

@@ -60,7 +60,8 @@ def test_c_header_layout_and_host_errors(tmp_path):
     for k in ("build_null_ctx", "indexed_null_ctx", "sync_null", "release_null", "create_null",
               "stage_null", "trace_null", "copy_null", "batched_null_ctx", "server_create_null",
               "submit_null", "poll_null", "wait_null", "release_req_null", "stats_null",
-              "set_tunables_null", "get_tunables_null", "parse_obj_null_ctx", "pt_null_ctx"):
+              "set_tunables_null", "get_tunables_null", "parse_obj_null_ctx", "pt_null_ctx", "mesh_null_ctx",
+              "trace_mesh_null_ctx"):
         assert int(kv[k]) == nat.EINVAL, k
     assert kv["server_error_null"] == "no server"
     assert kv["last_error_null"] == "no context"

@@ -55,6 +55,8 @@ size_t arena_bytes(uint32_t cap) {
 
 struct GraphKey {
     const void *tri = nullptr;
+    const void *verts = nullptr, *idx3 = nullptr;  // mesh input (the indexed leaf format)
+    uint32_t nverts = 0;
     uint32_t n = 0;
     HostBounds hb{};
     void *outs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -286,22 +288,42 @@ int ensure_stage(lvbh_ctx *ctx, size_t bytes) {
 }
 
 // The build proper: every launch on `s`, nothing synchronous.
+// A mesh input of the indexed leaf format: 16-byte vertex rows and index triples (device).
+struct MeshIn {
+    const float4 *verts;
+    uint32_t nverts;
+    const uint32_t *idx3;
+};
+
 void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
-                   const lvbh_result *out, cudaStream_t s, bool profile) {
+                   const lvbh_result *out, cudaStream_t s, bool profile, const MeshIn *mesh = nullptr) {
     if (profile) cudaEventRecord(ctx->ev[1], s);
     cudaMemsetAsync(reinterpret_cast<char *>(ctx->ctl) + offsetof(Control, err), 0,
                     sizeof(Control) - offsetof(Control, err), s);
-    if (!hb.use) launch_bounds(tri, n, ctx->ctl, s);
+    if (!hb.use) {
+        if (mesh) launch_bounds_mesh(mesh->verts, mesh->nverts, mesh->idx3, n, ctx->ctl, s);
+        else launch_bounds(tri, n, ctx->ctl, s);
+    }
     if (profile) cudaEventRecord(ctx->ev[2], s);
     // unsorted keys go to keys_a, so that the three passes ping-pong keys_a -> result ->
     // scratch -> result
     uint32_t *keys_a = ctx->keys_a;
-    launch_morton(tri, n, hb, ctx->ctl, keys_a, ctx->epoch, ctx->lookback, s);
+    if (mesh) launch_morton_mesh(mesh->verts, mesh->nverts, mesh->idx3, n, hb, ctx->ctl, keys_a, ctx->epoch,
+                                 ctx->lookback, s);
+    else launch_morton(tri, n, hb, ctx->ctl, keys_a, ctx->epoch, ctx->lookback, s);
     if (profile) cudaEventRecord(ctx->ev[3], s);
     launch_sort_pass(keys_a, nullptr, out->morton, out->leaf_index, n, 0, true, ctx->ctl, ctx->lookback, s);
     launch_sort_pass(out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, n, 1, false, ctx->ctl, ctx->lookback, s);
     launch_sort_pass(ctx->keys_b, ctx->vals_b, out->morton, out->leaf_index, n, 2, false, ctx->ctl, ctx->lookback, s);
     if (profile) cudaEventRecord(ctx->ev[4], s);
+    if (mesh) {
+        uint32_t *sidx = static_cast<uint32_t *>(out->tris);
+        launch_leaf_idx(mesh->idx3, out->leaf_index, n, sidx, s);
+        launch_emit_mesh(mesh->verts, mesh->nverts, sidx, out->morton, n, static_cast<float4 *>(out->nodes),
+                         out->parents, ctx->items, ctx->counts, ctx->arrive, ctx->pend, ctx->pend_d, ctx->epoch,
+                         ctx->ctl, s, profile ? ctx->ev + 5 : nullptr);
+        return;
+    }
     launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
                 static_cast<float4 *>(out->nodes), out->parents, ctx->items, ctx->counts,
                 ctx->arrive, ctx->pend, ctx->pend_d, ctx->epoch, ctx->ctl, s,
@@ -382,10 +404,15 @@ int launch_batch_graph(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bo
 }
 
 int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
-                 const lvbh_result *out, cudaStream_t s) {
+                 const lvbh_result *out, cudaStream_t s, const MeshIn *mesh) {
     GraphKey key;
     std::memset(static_cast<void *>(&key), 0, sizeof key);  // padding takes part in the compare
     key.tri = tri;
+    if (mesh) {
+        key.verts = mesh->verts;
+        key.idx3 = mesh->idx3;
+        key.nverts = mesh->nverts;
+    }
     key.n = n;
     key.hb = hb;
     key.outs[0] = out->nodes; key.outs[1] = out->tris; key.outs[2] = out->parents;
@@ -393,7 +420,7 @@ int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds 
     if (!ctx->gexec || !(key == ctx->gkey)) {
         if (!ctx->cap_stream) LVBH_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
         LVBH_CUDA(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_build(ctx, tri, n, hb, out, ctx->cap_stream, false);
+        enqueue_build(ctx, tri, n, hb, out, ctx->cap_stream, false, mesh);
         cudaGraph_t g = nullptr;
         LVBH_CUDA(ctx, cudaStreamEndCapture(ctx->cap_stream, &g));
         bool updated = false;
@@ -416,14 +443,14 @@ int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds 
     return LVBH_OK;
 }
 
-int alloc_outputs(lvbh_ctx *ctx, uint32_t n, lvbh_result *out) {
+int alloc_outputs(lvbh_ctx *ctx, uint32_t n, lvbh_result *out, size_t tri_row = 48) {
     out->nodes = out->tris = nullptr;
     out->parents = nullptr;
     out->leaf_index = out->morton = nullptr;
     out->owned = 0;
     if (n == 0) return LVBH_OK;
     void *p[5] = {};
-    const size_t sz[5] = {64ull * n, 48ull * n, 8ull * n, 4ull * n, 4ull * n};
+    const size_t sz[5] = {64ull * n, tri_row * n, 8ull * n, 4ull * n, 4ull * n};
     for (int i = 0; i < 5; ++i) {
         cudaError_t e = cudaMalloc(&p[i], sz[i]);
         if (e != cudaSuccess) {
@@ -441,7 +468,8 @@ int alloc_outputs(lvbh_ctx *ctx, uint32_t n, lvbh_result *out) {
 }
 
 int build_common(lvbh_ctx *ctx, const float4 *tri_dev, uint32_t n, const float *model_bounds,
-                 uint32_t flags, lvbh_result *out, cudaStream_t s, bool profile_upload) {
+                 uint32_t flags, lvbh_result *out, cudaStream_t s, bool profile_upload,
+                 const MeshIn *mesh = nullptr) {
     HostBounds hb{};
     if (model_bounds) {
         std::memcpy(hb.v, model_bounds, sizeof hb.v);
@@ -457,11 +485,11 @@ int build_common(lvbh_ctx *ctx, const float4 *tri_dev, uint32_t n, const float *
     int rc = LVBH_OK;
     if (profile && !profile_upload) cudaEventRecord(ctx->ev[0], s);
     if (profile || (flags & LVBH_NO_GRAPH)) {
-        enqueue_build(ctx, tri_dev, n, hb, out, s, profile);
+        enqueue_build(ctx, tri_dev, n, hb, out, s, profile, mesh);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
     } else {
-        rc = launch_graph(ctx, tri_dev, n, hb, out, s);
+        rc = launch_graph(ctx, tri_dev, n, hb, out, s, mesh);
         if (rc) return rc;
     }
     ctx->ev_valid = profile;
@@ -485,19 +513,21 @@ float ord_word_to_float(uint32_t o) {
     return f;
 }
 
-int check_out(lvbh_ctx *ctx, uint32_t n, uint32_t flags, lvbh_result *out) {
+int check_out(lvbh_ctx *ctx, uint32_t n, uint32_t flags, lvbh_result *out, size_t tri_row = 48) {
     if (!out) return fail(ctx, LVBH_EINVAL, "out is NULL");
     if (flags & LVBH_OUT_CALLER) {
         if (n && (!out->nodes || !out->tris || !out->parents || !out->leaf_index || !out->morton))
             return fail(ctx, LVBH_EINVAL, "LVBH_OUT_CALLER with a NULL result buffer");
-        if (n && (((uintptr_t)out->nodes | (uintptr_t)out->tris) & 15u))
+        if (n && (((uintptr_t)out->nodes | (tri_row == 48 ? (uintptr_t)out->tris : 0)) & 15u))
             return fail(ctx, LVBH_EINVAL, "result nodes/tris must be 16-byte aligned");
+        if (n && ((uintptr_t)out->tris & 3u))
+            return fail(ctx, LVBH_EINVAL, "result tris must be 4-byte aligned");
         if (n && (((uintptr_t)out->parents | (uintptr_t)out->leaf_index | (uintptr_t)out->morton) & 3u))
             return fail(ctx, LVBH_EINVAL, "result parents/leaf_index/morton must be 4-byte aligned");
         out->owned = 0;
         return LVBH_OK;
     }
-    return alloc_outputs(ctx, n, out);
+    return alloc_outputs(ctx, n, out, tri_row);
 }
 
 }  // namespace
@@ -641,6 +671,56 @@ int lvbh_build_indexed(lvbh_ctx *ctx, const float *xyz, uint32_t num_verts, cons
                           &ctx->ctl->aux_err, s);
     return build_common(ctx, reinterpret_cast<const float4 *>(st), num_tris, model_bounds, flags,
                         out, s, profile_upload);
+}
+
+int lvbh_build_mesh(lvbh_ctx *ctx, const float *verts4, uint32_t num_verts, const uint32_t *idx3,
+                    uint32_t num_tris, const float *model_bounds, uint32_t flags, lvbh_result *out,
+                    void *stream) {
+    if (!ctx) return LVBH_EINVAL;
+    if (!out) return fail(ctx, LVBH_EINVAL, "out is NULL");
+    if (num_tris > LVBH_MAX_TRIS) return fail(ctx, LVBH_EINVAL, "num_tris exceeds LVBH_MAX_TRIS");
+    if (num_tris && (!verts4 || !idx3 || !num_verts)) return fail(ctx, LVBH_EINVAL, "NULL vertex or index buffer");
+    const bool host = (flags & LVBH_INPUT_HOST) != 0;
+    if (num_tris && !host && ((reinterpret_cast<uintptr_t>(verts4) & 15u) || (reinterpret_cast<uintptr_t>(idx3) & 3u)))
+        return fail(ctx, LVBH_EINVAL, "device vertex rows must be 16-byte aligned, indices 4-byte aligned");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (int rc = check_out(ctx, num_tris, flags, out, 12)) return rc;
+    out->num_tris = out->num_nodes = num_tris;
+    std::memset(out->bounds, 0, sizeof out->bounds);
+    if (!num_tris) return build_common(ctx, nullptr, 0, model_bounds, flags, out, s, false);
+    if (int rc = ensure_arena(ctx, num_tris)) return rc;
+    LVBH_CUDA(ctx, cudaMemsetAsync(&ctx->ctl->aux_err, 0, sizeof(uint32_t), s));
+    bool profile_upload = false;
+    if (host) {
+        const size_t vb = align_up(16ull * num_verts), ib = align_up(12ull * num_tris);
+        if (int rc = ensure_stage(ctx, vb + ib)) return rc;
+        if (flags & LVBH_PROFILE) { cudaEventRecord(ctx->ev[0], s); profile_upload = true; }
+        char *st = static_cast<char *>(ctx->stage);
+        LVBH_CUDA(ctx, cudaMemcpyAsync(st, verts4, 16ull * num_verts, cudaMemcpyHostToDevice, s));
+        LVBH_CUDA(ctx, cudaMemcpyAsync(st + vb, idx3, 12ull * num_tris, cudaMemcpyHostToDevice, s));
+        verts4 = reinterpret_cast<const float *>(st);
+        idx3 = reinterpret_cast<const uint32_t *>(st + vb);
+    }
+    const MeshIn mesh{reinterpret_cast<const float4 *>(verts4), num_verts, idx3};
+    return build_common(ctx, nullptr, num_tris, model_bounds, flags, out, s, profile_upload, &mesh);
+}
+
+int lvbh_trace_mesh(lvbh_ctx *ctx, const void *nodes, const uint32_t *leaf_idx3, const float *verts4,
+                    uint32_t num_verts, uint32_t num_tris, const float *rays, uint32_t num_rays,
+                    int32_t *hit_prim, float *hit_t, uint32_t *max_stack, void *stream) {
+    if (!ctx) return LVBH_EINVAL;
+    if (num_rays && (!rays || !hit_prim || !hit_t)) return fail(ctx, LVBH_EINVAL, "NULL ray buffer");
+    if (num_tris && (!nodes || !leaf_idx3 || !verts4 || !num_verts)) return fail(ctx, LVBH_EINVAL, "NULL tree buffer");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!ctx->trace_counter) LVBH_CUDA(ctx, cudaMalloc(&ctx->trace_counter, sizeof(uint32_t)));
+    launch_trace_mesh(static_cast<const float4 *>(nodes), reinterpret_cast<const float4 *>(verts4), num_verts,
+                      leaf_idx3, num_tris, reinterpret_cast<const float4 *>(rays), num_rays, hit_prim, hit_t,
+                      max_stack, ctx->trace_counter, s);
+    LVBH_CUDA(ctx, cudaGetLastError());
+    LVBH_CUDA(ctx, cudaStreamSynchronize(s));
+    return LVBH_OK;
 }
 
 int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *seg_offsets,

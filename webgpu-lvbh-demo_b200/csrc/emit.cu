@@ -97,6 +97,24 @@ struct ManySegs {
 
 // K3b shared memory.  A climbing item is two float4: box min + link (node index, or
 // -(leaf + 1)), box max + its packed local range and end separators (TreeGeo::pack).
+// Where the tree pass gets its leaves.  SoupLeaves: leaf t of a block is triangle perm[b0 + t]
+// of the 48-byte soup, copied to the output soup.  MeshLeaves (the indexed leaf format): leaf t
+// is the sorted triangle b0 + t, whose three vertex indices are already in sorted order
+// (sidx, written by the leaf-index pass) and whose vertices are 16-byte rows of a vertex
+// buffer; nothing is copied.
+struct SoupLeaves {
+    static constexpr bool kMesh = false;
+    const float4 *tri;
+    const uint32_t *perm;
+    float4 *otri;
+};
+struct MeshLeaves {
+    static constexpr bool kMesh = true;
+    const float4 *verts;
+    const uint32_t *sidx;
+    uint32_t nverts;
+};
+
 template <int EB>
 struct ClimbSmem {
     float4 tri[2][EB][3];   // the gathered triangles of this block and the next (cp.async)
@@ -117,12 +135,10 @@ struct ClimbSmem {
 // above).  Leaf t of a block gathers triangle perm[b0 + t]: its index is loaded two blocks
 // ahead, its three 16-byte rows are copied into shared memory one block ahead (cp.async, no
 // registers held meanwhile), then written to the output soup and reduced to the leaf box.
-template <int LOG, class Segs>
+template <int LOG, class Segs, class Leaves = SoupLeaves>
 __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_tree_climb(Segs segs,
                                                     const uint32_t *__restrict__ keys_all,
-                                                    const float4 *__restrict__ tri_all,
-                                                    const uint32_t *__restrict__ perm_all,
-                                                    float4 *__restrict__ otri_all,
+                                                    Leaves lv,
                                                     float4 *nodes_all, int32_t *parents_all,
                                                     OpenItem *out_items, uint32_t *out_counts,
                                                     Control *ctl) {
@@ -134,11 +150,20 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
     const int nblk = segs.blocks();
     const uint32_t lt = lanemask_lt();
 
-    // two blocks ahead: this thread's permutation entry
-    uint32_t pa = 0;
+    // two blocks ahead: this thread's permutation entry (its three vertex indices for a mesh)
+    uint32_t pa = 0, pb = 0, pc = 0;
     auto fetch_perm = [&](int blk) {
         const Span sp = segs.span(blk);
-        if (sp.b0 + t < sp.n) pa = __ldg(perm_all + sp.start + sp.b0 + t);
+        if (sp.b0 + t < sp.n) {
+            if constexpr (Leaves::kMesh) {
+                const uint32_t *r = lv.sidx + 3ull * (sp.start + sp.b0 + t);
+                pa = __ldg(r);
+                pb = __ldg(r + 1);
+                pc = __ldg(r + 2);
+            } else {
+                pa = __ldg(lv.perm + sp.start + sp.b0 + t);
+            }
+        }
     };
     // one block ahead: its span, this thread's key and triangle (into S.tri[buf]), edge keys
     Span nsp{0, 0, 0};
@@ -150,12 +175,20 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         const int b0 = nsp.b0, n = nsp.n, k = b0 + t;
         if (k < n) {
             nk = __ldg(keys + k);
-            uint32_t ti = pa;
-            if (ti >= (uint32_t)n) { bad_perm = true; ti = 0; }
-            const float4 *src = tri_all + 3ull * (nsp.start + ti);
-            cp_async16(&S.tri[buf][t][0], src);
-            cp_async16(&S.tri[buf][t][1], src + 1);
-            cp_async16(&S.tri[buf][t][2], src + 2);
+            if constexpr (Leaves::kMesh) {
+                // an index past the vertex buffer was reported by the Morton pass; read row 0
+                const uint32_t nv = lv.nverts;
+                cp_async16(&S.tri[buf][t][0], lv.verts + (pa < nv ? pa : 0u));
+                cp_async16(&S.tri[buf][t][1], lv.verts + (pb < nv ? pb : 0u));
+                cp_async16(&S.tri[buf][t][2], lv.verts + (pc < nv ? pc : 0u));
+            } else {
+                uint32_t ti = pa;
+                if (ti >= (uint32_t)n) { bad_perm = true; ti = 0; }
+                const float4 *src = lv.tri + 3ull * (nsp.start + ti);
+                cp_async16(&S.tri[buf][t][0], src);
+                cp_async16(&S.tri[buf][t][1], src + 1);
+                cp_async16(&S.tri[buf][t][2], src + 2);
+            }
         }
         cp_async_commit();
         if (t == 0) nk_lo = b0 > 0 ? __ldg(keys + b0 - 1) : 0u;
@@ -191,10 +224,12 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         float4 leaf_hi0 = make_float4(0.f, 0.f, 0.f, 0.f);
         if (active) {
             const float4 a = S.tri[buf][t][0], b = S.tri[buf][t][1], c = S.tri[buf][t][2];
-            float4 *dst = otri_all + 3ull * (sp.start + k);
-            st_stream(dst, a);
-            st_stream(dst + 1, b);
-            st_stream(dst + 2, c);
+            if constexpr (!Leaves::kMesh) {
+                float4 *dst = lv.otri + 3ull * (sp.start + k);
+                st_stream(dst, a);
+                st_stream(dst + 1, b);
+                st_stream(dst + 2, c);
+            }
             float nx = fminf(a.x, fminf(b.x, c.x)), ny = fminf(a.y, fminf(b.y, c.y)), nz = fminf(a.z, fminf(b.z, c.z));
             float xx = fmaxf(a.x, fmaxf(b.x, c.x)), xy = fmaxf(a.y, fmaxf(b.y, c.y)), xz = fmaxf(a.z, fmaxf(b.z, c.z));
             nx = nx == 0.0f ? -1e-8f : nx; ny = ny == 0.0f ? -1e-8f : ny; nz = nz == 0.0f ? -1e-8f : nz;
@@ -445,9 +480,8 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
 template <int LOG>
 inline size_t leaves_smem_bytes() { return sizeof(ClimbSmem<TreeGeo<LOG>::EB>); }
 
-template <int LOG, class Segs>
-void launch_emit_impl(Segs segs, int groups, const float4 *tri, const uint32_t *perm,
-                      const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
+template <int LOG, class Segs, class Leaves>
+void launch_emit_impl(Segs segs, int groups, Leaves lv, const uint32_t *keys, float4 *nodes, int32_t *parents,
                       OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
                       uint8_t *pend_d, const uint32_t *epoch, Control *ctl, bool top,
                       cudaStream_t s, cudaEvent_t *ev, int ctas_per_sm) {
@@ -455,8 +489,8 @@ void launch_emit_impl(Segs segs, int groups, const float4 *tri, const uint32_t *
     const int per_sm = ctas_per_sm > 0 && ctas_per_sm < TreeGeo<LOG>::kCtasPerSm ? ctas_per_sm
                                                                                 : TreeGeo<LOG>::kCtasPerSm;
     const int grid = min(groups, sm_count() * per_sm);
-    k_tree_climb<LOG, Segs><<<grid, TreeGeo<LOG>::EB, leaves_smem_bytes<LOG>(), s>>>(
-        segs, keys, tri, perm, otri, nodes, parents, items, counts, ctl);
+    k_tree_climb<LOG, Segs, Leaves><<<grid, TreeGeo<LOG>::EB, leaves_smem_bytes<LOG>(), s>>>(
+        segs, keys, lv, nodes, parents, items, counts, ctl);
     if (ev) cudaEventRecord(ev[1], s);
     if (top)
         k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, counts, nodes,
@@ -481,6 +515,7 @@ cudaError_t emit_init() {
     cudaError_t e = prefer_shared(k_tree_climb<8, OneSeg<8>>, leaves_smem_bytes<8>());
     if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, ManySegs<8>>, leaves_smem_bytes<8>());
     if (e == cudaSuccess) e = prefer_shared(k_tree_climb<7, ManySegs<7>>, leaves_smem_bytes<7>());
+    if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, OneSeg<8>, MeshLeaves>, leaves_smem_bytes<8>());
     return e;
 }
 
@@ -490,9 +525,20 @@ void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, 
                  const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev) {
     if (n == 0) return;
     const int groups = (int)emit_groups(n, kLogEmitBlock);
-    launch_emit_impl<kLogEmitBlock>(OneSeg<kLogEmitBlock>{(int)n}, groups, tri, perm, keys, otri,
+    launch_emit_impl<kLogEmitBlock>(OneSeg<kLogEmitBlock>{(int)n}, groups, SoupLeaves{tri, perm, otri}, keys,
                                     nodes, parents, items, counts, arrive, pend, pend_d, epoch,
                                     ctl, groups > 1, s, ev, 0);
+}
+
+void launch_emit_mesh(const float4 *verts, uint32_t num_verts, const uint32_t *sidx, const uint32_t *keys,
+                      uint32_t n, float4 *nodes, int32_t *parents, OpenItem *items, uint32_t *counts,
+                      uint32_t *arrive, float4 *pend, uint8_t *pend_d, const uint32_t *epoch, Control *ctl,
+                      cudaStream_t s, cudaEvent_t *ev) {
+    if (n == 0) return;
+    const int groups = (int)emit_groups(n, kLogEmitBlock);
+    launch_emit_impl<kLogEmitBlock>(OneSeg<kLogEmitBlock>{(int)n}, groups, MeshLeaves{verts, sidx, num_verts},
+                                    keys, nodes, parents, items, counts, arrive, pend, pend_d, epoch, ctl,
+                                    groups > 1, s, ev, 0);
 }
 
 void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
@@ -502,13 +548,13 @@ void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *p
                        cudaEvent_t *ev) {
     if (bp.blocks == 0) return;
     if (bp.log_block == 7)
-        launch_emit_impl<7>(ManySegs<7>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks, tri,
-                            perm, keys, otri, nodes, parents, items, counts, arrive, pend, pend_d,
-                            epoch, ctl, true, s, ev, bp.tree_ctas_per_sm);
+        launch_emit_impl<7>(ManySegs<7>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks,
+                            SoupLeaves{tri, perm, otri}, keys, nodes, parents, items, counts, arrive, pend,
+                            pend_d, epoch, ctl, true, s, ev, bp.tree_ctas_per_sm);
     else
-        launch_emit_impl<8>(ManySegs<8>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks, tri,
-                            perm, keys, otri, nodes, parents, items, counts, arrive, pend, pend_d,
-                            epoch, ctl, true, s, ev, bp.tree_ctas_per_sm);
+        launch_emit_impl<8>(ManySegs<8>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks,
+                            SoupLeaves{tri, perm, otri}, keys, nodes, parents, items, counts, arrive, pend,
+                            pend_d, epoch, ctl, true, s, ev, bp.tree_ctas_per_sm);
 }
 
 }  // namespace lvbh

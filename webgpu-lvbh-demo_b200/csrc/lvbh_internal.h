@@ -173,6 +173,23 @@ void launch_trace(const float4 *nodes, const float4 *tris, uint32_t n, const flo
                   uint32_t num_rays, int32_t *hit_prim, float *hit_t, uint32_t *max_stack,
                   uint32_t *counter, cudaStream_t s);
 
+// The indexed leaf format (a mesh of 16-byte vertex rows + index triples): K1a over the
+// vertices the triangles use, K1b gathering each triangle's rows, the sorted index triples
+// (sidx[i] = idx3[perm[i]]), and K3 reading leaves through sidx.
+void launch_bounds_mesh(const float4 *verts, uint32_t nverts, const uint32_t *idx3, uint32_t n, Control *ctl,
+                        cudaStream_t s);
+void launch_morton_mesh(const float4 *verts, uint32_t nverts, const uint32_t *idx3, uint32_t n, HostBounds hb,
+                        Control *ctl, uint32_t *keys, uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s);
+void launch_leaf_idx(const uint32_t *idx3, const uint32_t *perm, uint32_t n, uint32_t *sidx, cudaStream_t s);
+void launch_emit_mesh(const float4 *verts, uint32_t num_verts, const uint32_t *sidx, const uint32_t *keys,
+                      uint32_t n, float4 *nodes, int32_t *parents, OpenItem *items, uint32_t *counts,
+                      uint32_t *arrive, float4 *pend, uint8_t *pend_d, const uint32_t *epoch, Control *ctl,
+                      cudaStream_t s, cudaEvent_t *ev);
+// K5 over the indexed leaf format: leaf i's vertices are verts[sidx[3i..3i+2]].
+void launch_trace_mesh(const float4 *nodes, const float4 *verts, uint32_t num_verts, const uint32_t *sidx, uint32_t n,
+                       const float4 *rays, uint32_t num_rays, int32_t *hit_prim, float *hit_t,
+                       uint32_t *max_stack, uint32_t *counter, cudaStream_t s);
+
 // Path-trace bounce (trace.cu): the uniform buffer (pos, rst, lat) and the constants the
 // reference's shader bakes in (image size, aspect, sin(fov / 2), pow(.3, 2.2)).
 struct PtFrame {

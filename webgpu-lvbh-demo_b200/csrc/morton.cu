@@ -74,12 +74,17 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const float4 *__restrict__ 
 // memory so that each lane owns a triangle); the digit counts of all three sort passes
 // accumulate over the block, and the counts of the first pass's digit per tile and per chunk
 // go straight to the sort's scratch, so the first sort pass starts from them.
+// MESH: the triangles are index triples into a buffer of 16-byte vertex rows (the indexed leaf
+// format's input); each lane gathers its triangle's three rows, an index past the buffer reads
+// row 0 and sets ERR_BAD_INDEX.
+template <bool MESH>
 __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ tri, uint32_t n,
                                                      HostBounds hb, Control *__restrict__ ctl,
                                                      uint32_t *__restrict__ keys,
                                                      uint32_t *__restrict__ epoch, uint32_t chunk_tiles,
                                                      uint32_t *__restrict__ tile_hist,
-                                                     uint32_t *__restrict__ chunk_sum) {
+                                                     uint32_t *__restrict__ chunk_sum,
+                                                     const uint32_t *__restrict__ idx3, uint32_t nverts) {
     constexpr int P = kDigits / kThreads;  // digits per thread in the per-tile counts
     __shared__ float4 stage[kWarps][96];
     __shared__ uint32_t hist[kSortPasses][kDigits];
@@ -108,7 +113,7 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
     uint32_t acc[P];
 #pragma unroll
     for (int j = 0; j < P; ++j) acc[j] = 0;
-    bool bad = false;
+    bool bad = false, bad_index = false;
     for (uint32_t tt = 0; tt < chunk_tiles; ++tt) {
         const uint32_t tile = blockIdx.x * chunk_tiles + tt;
         if (tile >= tiles) break;  // uniform across the block
@@ -118,18 +123,38 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
         for (uint32_t c = warp; c < (uint32_t)kSortTile / 32; c += kWarps) {
             const uint32_t t0 = tile * (uint32_t)kSortTile + 32u * c;
             if (t0 >= n) break;
-            const uint64_t base = 3ull * t0;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                const uint64_t e = base + 32 * r + lane;
-                stage[warp][32 * r + lane] = e < nv ? ld_stream(tri + e) : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-            __syncwarp();
-            const float4 v0 = stage[warp][3 * lane], v1 = stage[warp][3 * lane + 1],
-                         v2 = stage[warp][3 * lane + 2];
-            __syncwarp();
             const uint32_t t = t0 + lane;
             const bool valid = t < n;
+            float4 v0, v1, v2;
+            if constexpr (MESH) {
+                uint32_t i0 = 0, i1 = 0, i2 = 0;
+                if (valid) {
+                    i0 = __ldcs(idx3 + 3ull * t);
+                    i1 = __ldcs(idx3 + 3ull * t + 1);
+                    i2 = __ldcs(idx3 + 3ull * t + 2);
+                    if (i0 >= nverts || i1 >= nverts || i2 >= nverts) {
+                        bad_index = true;
+                        i0 = i0 < nverts ? i0 : 0u;
+                        i1 = i1 < nverts ? i1 : 0u;
+                        i2 = i2 < nverts ? i2 : 0u;
+                    }
+                }
+                v0 = __ldg(tri + i0);
+                v1 = __ldg(tri + i1);
+                v2 = __ldg(tri + i2);
+            } else {
+                const uint64_t base = 3ull * t0;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const uint64_t e = base + 32 * r + lane;
+                    stage[warp][32 * r + lane] = e < nv ? ld_stream(tri + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                __syncwarp();
+                v0 = stage[warp][3 * lane];
+                v1 = stage[warp][3 * lane + 1];
+                v2 = stage[warp][3 * lane + 2];
+                __syncwarp();
+            }
             uint32_t key = 0;
             if (valid) {
                 bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
@@ -167,11 +192,60 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
 #pragma unroll
     for (int j = 0; j < P; ++j) crow[j] = acc[j];
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
+    if (__any_sync(0xFFFFFFFFu, bad_index) && lane == 0) atomicOr(&ctl->err, ERR_BAD_INDEX);
     __syncthreads();
     for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) {
         const uint32_t c = (&hist[0][0])[i];
         if (c) atomicAdd(ctl->hist + i, c);
     }
+}
+
+// K1a for a mesh: min / max over the vertices the triangles use (the rows of unused vertices
+// take no part, as in the soup), three gathers of 16-byte rows per triangle.  Indices past the
+// buffer are skipped (K1b reports them).
+__global__ void __launch_bounds__(kThreads) k_bounds_mesh(const float4 *__restrict__ verts, uint32_t nverts,
+                                                          const uint32_t *__restrict__ idx3, uint32_t n,
+                                                          Control *__restrict__ ctl) {
+    float mn[3] = {INFINITY, INFINITY, INFINITY};
+    float mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const uint32_t stride = gridDim.x * kThreads;
+    for (uint64_t e = (uint64_t)blockIdx.x * kThreads + threadIdx.x; e < 3ull * n; e += stride) {
+        const uint32_t vi = __ldcs(idx3 + e);
+        if (vi >= nverts) continue;
+        const float4 p = __ldg(verts + vi);
+        mn[0] = fminf(mn[0], p.x); mx[0] = fmaxf(mx[0], p.x);
+        mn[1] = fminf(mn[1], p.y); mx[1] = fmaxf(mx[1], p.y);
+        mn[2] = fminf(mn[2], p.z); mx[2] = fmaxf(mx[2], p.z);
+    }
+    warp_minmax(mn, mx);
+    __shared__ float s[kWarps][6];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { s[warp][a] = mn[a]; s[warp][3 + a] = mx[a]; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int a = threadIdx.x;
+        float r = s[0][a];
+        for (int w = 1; w < kWarps; ++w) r = a < 3 ? fminf(r, s[w][a]) : fmaxf(r, s[w][a]);
+        if (a < 3) atomicMax(&ctl->bounds_ord[a], ~ord_lo(r));
+        else atomicMax(&ctl->bounds_ord[a], ord_lo(r));
+    }
+}
+
+// The indexed leaf format's triangle rows: the three vertex indices of each sorted triangle.
+__global__ void __launch_bounds__(256) k_leaf_idx(const uint32_t *__restrict__ idx3, const uint32_t *__restrict__ perm,
+                                                  uint32_t n, uint32_t *__restrict__ sidx) {
+    const uint32_t i = blockIdx.x * 256u + threadIdx.x;
+    if (i >= n) return;
+    uint32_t ti = __ldcs(perm + i);
+    ti = ti < n ? ti : 0u;  // a permutation entry is below n
+    const uint32_t *src = idx3 + 3ull * ti;
+    const uint32_t a = __ldg(src), b = __ldg(src + 1), c = __ldg(src + 2);
+    sidx[3ull * i] = a;
+    sidx[3ull * i + 1] = b;
+    sidx[3ull * i + 2] = c;
 }
 
 // Batched K1a: one block per sort tile (at most kSortTile triangles of one segment); the
@@ -340,8 +414,29 @@ void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s) 
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl, uint32_t *keys,
                    uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
     if (n == 0) return;
-    k_morton<<<sort_chunks(n), kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch, sort_chunk_tiles(n), sort_scratch,
-                                                 sort_chunk_sums(sort_scratch, n));
+    k_morton<false><<<sort_chunks(n), kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch, sort_chunk_tiles(n),
+                                                        sort_scratch, sort_chunk_sums(sort_scratch, n), nullptr, 0u);
+}
+
+void launch_bounds_mesh(const float4 *verts, uint32_t nverts, const uint32_t *idx3, uint32_t n, Control *ctl,
+                        cudaStream_t s) {
+    uint64_t blocks = (3ull * n + kThreads * 4 - 1) / (kThreads * 4);
+    const uint64_t cap = (uint64_t)sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    k_bounds_mesh<<<(unsigned)blocks, kThreads, 0, s>>>(verts, nverts, idx3, n, ctl);
+}
+
+void launch_morton_mesh(const float4 *verts, uint32_t nverts, const uint32_t *idx3, uint32_t n, HostBounds hb,
+                        Control *ctl, uint32_t *keys, uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
+    if (n == 0) return;
+    k_morton<true><<<sort_chunks(n), kThreads, 0, s>>>(verts, n, hb, ctl, keys, epoch, sort_chunk_tiles(n),
+                                                       sort_scratch, sort_chunk_sums(sort_scratch, n), idx3, nverts);
+}
+
+void launch_leaf_idx(const uint32_t *idx3, const uint32_t *perm, uint32_t n, uint32_t *sidx, cudaStream_t s) {
+    if (n == 0) return;
+    k_leaf_idx<<<(n + 255) / 256, 256, 0, s>>>(idx3, perm, n, sidx);
 }
 
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,

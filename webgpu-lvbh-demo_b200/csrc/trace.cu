@@ -30,8 +30,35 @@ __device__ __forceinline__ F3 cross3(F3 a, F3 b) {
             __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
 }
 
-__device__ float tri_intersect(F3 o, F3 d, const float4 *t) {
-    const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+// Where a leaf's three vertices come from: the 48-byte sorted soup, or the indexed leaf format
+// (three vertex indices per sorted leaf into 16-byte vertex rows; an index past the buffer
+// reads row 0).
+struct SoupTris {
+    const float4 *tris;
+    __device__ __forceinline__ void get(int leaf, float4 &a, float4 &b, float4 &c) const {
+        const float4 *t = tris + 3ull * leaf;
+        a = __ldg(t);
+        b = __ldg(t + 1);
+        c = __ldg(t + 2);
+    }
+};
+struct MeshTris {
+    const float4 *verts;
+    const uint32_t *sidx;
+    uint32_t nverts;
+    __device__ __forceinline__ void get(int leaf, float4 &a, float4 &b, float4 &c) const {
+        const uint32_t *r = sidx + 3ull * leaf;
+        const uint32_t i0 = __ldg(r), i1 = __ldg(r + 1), i2 = __ldg(r + 2);
+        a = __ldg(verts + (i0 < nverts ? i0 : 0u));
+        b = __ldg(verts + (i1 < nverts ? i1 : 0u));
+        c = __ldg(verts + (i2 < nverts ? i2 : 0u));
+    }
+};
+
+template <class Tris>
+__device__ float tri_intersect(F3 o, F3 d, const Tris &tr, int leaf) {
+    float4 a, b, c;
+    tr.get(leaf, a, b, c);
     const F3 v0 = {a.x, a.y, a.z}, v1 = {b.x, b.y, b.z}, v2 = {c.x, c.y, c.z};
     const F3 v0v1 = sub3(v1, v0), v0v2 = sub3(v2, v0);
     const F3 pvec = cross3(d, v0v2);
@@ -89,8 +116,9 @@ __device__ __forceinline__ void ray_init(RayState &st, const float4 *__restrict_
 // One node visit of the reference's loop (pathtracer.js:505-581): a leaf is tested, an internal
 // node's children are tested and the nearer valid one is taken with the farther pushed.
 // Returns false once the ray's stack is empty.
+template <class Tris>
 __device__ __forceinline__ bool ray_step(RayState &st, int32_t *stack, const float4 *__restrict__ nodes,
-                                         const float4 *__restrict__ tris, uint32_t n) {
+                                         const Tris &tris, uint32_t n) {
     if (st.sp < 0) return false;
     const int node_idx = st.node_idx;
     if ((node_idx < 0 ? (uint32_t)(-(node_idx + 1)) >= n : (uint32_t)node_idx >= n) ||
@@ -101,7 +129,7 @@ __device__ __forceinline__ bool ray_step(RayState &st, int32_t *stack, const flo
     }
     if (node_idx < 0) {
         const int leaf = -(node_idx + 1);
-        const float t = tri_intersect(st.o, st.d, tris + 3ull * leaf);
+        const float t = tri_intersect(st.o, st.d, tris, leaf);
         if (t > 0.0f && t < st.dist) { st.dist = wmin(t, st.dist); st.prim = leaf; }
         st.sp -= 1;
         st.node_idx = st.sp >= 0 ? stack[st.sp] : 0;
@@ -135,8 +163,8 @@ __device__ __forceinline__ bool ray_step(RayState &st, int32_t *stack, const flo
 // Persistent traversal: each lane takes a new ray as soon as its current one is done (a warp
 // refills its idle lanes from a global counter once a quarter of them are idle), so a warp is
 // not held by its slowest ray.  Each ray's own walk is exactly the reference's.
-__global__ void __launch_bounds__(128) k_trace(const float4 *__restrict__ nodes,
-                                               const float4 *__restrict__ tris, uint32_t n,
+template <class Tris>
+__global__ void __launch_bounds__(128) k_trace(const float4 *__restrict__ nodes, Tris tris, uint32_t n,
                                                const float4 *__restrict__ rays, uint32_t num_rays,
                                                int32_t *__restrict__ hit_prim,
                                                float *__restrict__ hit_t,
@@ -285,7 +313,8 @@ __device__ __forceinline__ void pt_begin(PixelPath &pp, const float4 *__restrict
 }
 
 // ptStep after the traversal (:675-712) and the texel stores.
-__device__ __forceinline__ void pt_end(PixelPath &pp, const RayState &st, const float4 *__restrict__ tris,
+template <class Tris>
+__device__ __forceinline__ void pt_end(PixelPath &pp, const RayState &st, const Tris &tris,
                                        float4 *__restrict__ out, size_t plane, const PtFrame &f) {
     const float eps = 0.0001f, two_pi = 0x1.921fb6p+2f;
     F3 b = pp.b;
@@ -293,8 +322,8 @@ __device__ __forceinline__ void pt_end(PixelPath &pp, const RayState &st, const 
     float seed = pp.seed, bounces = pp.bounces;
     F3 o = pp.o, d = pp.d;
     if (st.dist != 1e30f) {
-        const float4 *tr = tris + 3ull * st.prim;
-        const float4 a = __ldg(tr), bb = __ldg(tr + 1), c = __ldg(tr + 2);
+        float4 a, bb, c;
+        tris.get(st.prim, a, bb, c);
         const F3 v0 = {a.x, a.y, a.z}, v1 = {bb.x, bb.y, bb.z}, v2 = {c.x, c.y, c.z};
         F3 norm = normalize3(cross3(sub3(v1, v0), sub3(v2, v0)));
         if (!(dot3(st.d, F3{-norm.x, -norm.y, -norm.z}) > 0.0f)) norm = {-norm.x, -norm.y, -norm.z};
@@ -344,7 +373,8 @@ __device__ __forceinline__ void pt_end(PixelPath &pp, const RayState &st, const 
 
 // One bounce of every pixel: persistent warps fetch pixels from *counter as lanes finish (the
 // traversal's dynamic fetch), each pixel's walk exactly the reference's.
-__global__ void __launch_bounds__(128) k_pt_step(const float4 *__restrict__ nodes, const float4 *__restrict__ tris,
+template <class Tris>
+__global__ void __launch_bounds__(128) k_pt_step(const float4 *__restrict__ nodes, Tris tris,
                                                  uint32_t n, const float4 *__restrict__ in, float4 *__restrict__ out,
                                                  PtFrame f, uint32_t *__restrict__ counter) {
     const int lane = threadIdx.x & 31;
@@ -389,15 +419,31 @@ void launch_trace(const float4 *nodes, const float4 *tris, uint32_t n, const flo
                   uint32_t *counter, cudaStream_t s) {
     if (num_rays == 0) return;
     static int per_sm = 0;
-    if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace, 128, 0) != cudaSuccess ||
+    if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<SoupTris>, 128, 0) != cudaSuccess ||
                     per_sm < 1)) {
         cudaGetLastError();
         per_sm = 4;
     }
     const uint32_t want = (num_rays + 127) / 128, cap = (uint32_t)(sm_count() * per_sm);
     cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
-    k_trace<<<want < cap ? want : cap, 128, 0, s>>>(nodes, tris, n, rays, num_rays, hit_prim, hit_t,
+    k_trace<<<want < cap ? want : cap, 128, 0, s>>>(nodes, SoupTris{tris}, n, rays, num_rays, hit_prim, hit_t,
                                                     max_stack, counter);
+}
+
+void launch_trace_mesh(const float4 *nodes, const float4 *verts, uint32_t num_verts, const uint32_t *sidx, uint32_t n,
+                       const float4 *rays, uint32_t num_rays, int32_t *hit_prim, float *hit_t,
+                       uint32_t *max_stack, uint32_t *counter, cudaStream_t s) {
+    if (num_rays == 0) return;
+    static int per_sm = 0;
+    if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<MeshTris>, 128, 0) != cudaSuccess ||
+                    per_sm < 1)) {
+        cudaGetLastError();
+        per_sm = 4;
+    }
+    const uint32_t want = (num_rays + 127) / 128, cap = (uint32_t)(sm_count() * per_sm);
+    cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+    k_trace<<<want < cap ? want : cap, 128, 0, s>>>(nodes, MeshTris{verts, sidx, num_verts}, n, rays, num_rays,
+                                                    hit_prim, hit_t, max_stack, counter);
 }
 
 void launch_pt_step(const float4 *nodes, const float4 *tris, uint32_t n, const float4 *state_in,
@@ -405,14 +451,14 @@ void launch_pt_step(const float4 *nodes, const float4 *tris, uint32_t n, const f
     const uint32_t num = f.width * f.height;
     if (num == 0) return;
     static int per_sm = 0;
-    if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pt_step, 128, 0) != cudaSuccess ||
+    if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pt_step<SoupTris>, 128, 0) != cudaSuccess ||
                     per_sm < 1)) {
         cudaGetLastError();
         per_sm = 4;
     }
     const uint32_t want = (num + 127) / 128, cap = (uint32_t)(sm_count() * per_sm);
     cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
-    k_pt_step<<<want < cap ? want : cap, 128, 0, s>>>(nodes, tris, n, state_in, state_out, f, counter);
+    k_pt_step<<<want < cap ? want : cap, 128, 0, s>>>(nodes, SoupTris{tris}, n, state_in, state_out, f, counter);
 }
 
 }  // namespace lvbh

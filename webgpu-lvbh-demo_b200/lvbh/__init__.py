@@ -121,10 +121,12 @@ class BatchResult(BuildResult):
                            morton=self.morton[a:b], bounds=self.seg_bounds[i].copy())
 
 
-def empty_outputs(n: int, device):
+def empty_outputs(n: int, device, mesh: bool = False):
+    """Result buffers of an n-triangle build; mesh: the indexed leaf format's tris (n, 3) uint32."""
     torch = _torch()
-    return dict(nodes=torch.empty((n, 16), dtype=torch.int32, device=device),
-                tris=torch.empty((n, 12), dtype=torch.float32, device=device),
+    tris = (torch.empty((n, 3), dtype=torch.int32, device=device) if mesh
+            else torch.empty((n, 12), dtype=torch.float32, device=device))
+    return dict(nodes=torch.empty((n, 16), dtype=torch.int32, device=device), tris=tris,
                 parents=torch.empty(2 * n, dtype=torch.int32, device=device),
                 leaf_index=torch.empty(n, dtype=torch.int32, device=device),
                 morton=torch.empty(n, dtype=torch.int32, device=device))
@@ -215,6 +217,49 @@ class BVHBuilder:
             | (PROFILE if profile else 0)
         return self._run(_native.lib.lvbh_build_indexed, (pv, nv, pi, n), n, bounds, flags,
                          outputs, stream, sync, profile, keep=(xyz, idx3))
+
+    def build_mesh(self, verts4, idx3, bounds=None, outputs=None, stream=None, sync=True,
+                   profile=False) -> BuildResult:
+        """The indexed leaf format (lvbh_build_mesh): verts4 (V, 4) float32 rows {x, y, z, pad},
+        idx3 (N, 3) uint32 - both host arrays or both CUDA tensors.  The result's tris are the
+        (N, 3) vertex indices of each sorted leaf (int32 tensor holding uint32 values)."""
+        torch = _torch()
+        host = not isinstance(verts4, torch.Tensor)
+        if host:
+            verts4 = np.ascontiguousarray(verts4, dtype=np.float32).reshape(-1, 4)
+            idx3 = np.ascontiguousarray(idx3, dtype=np.uint32).reshape(-1, 3)
+            pv, pi = verts4.ctypes.data_as(ctypes.c_void_p), idx3.ctypes.data_as(ctypes.c_void_p)
+        else:
+            verts4 = verts4.contiguous().reshape(-1, 4)
+            idx3 = idx3.contiguous().reshape(-1, 3)
+            pv, pi = ctypes.c_void_p(verts4.data_ptr()), ctypes.c_void_p(idx3.data_ptr())
+        n, nv = idx3.shape[0], verts4.shape[0]
+        flags = OUT_CALLER | (INPUT_HOST if host else 0) | (0 if sync else ASYNC) \
+            | (PROFILE if profile else 0)
+        if outputs is None:
+            outputs = empty_outputs(n, self.device, mesh=True)
+        return self._run(_native.lib.lvbh_build_mesh, (pv, nv, pi, n), n, bounds, flags,
+                         outputs, stream, sync, profile, keep=(verts4, idx3))
+
+    def trace_mesh(self, res: BuildResult, verts4, rays, stream=None):
+        """lvbh_trace over the indexed leaf format: res from build_mesh, verts4 (V, 4) float32
+        CUDA tensor.  Returns (hit_prim int32, hit_t float32, max_stack int32)."""
+        torch = _torch()
+        rays = rays.contiguous().reshape(-1, 8)
+        verts4 = verts4.contiguous().reshape(-1, 4)
+        nr = rays.shape[0]
+        prim = torch.empty(nr, dtype=torch.int32, device=self.device)
+        t = torch.empty(nr, dtype=torch.float32, device=self.device)
+        st = torch.empty(nr, dtype=torch.int32, device=self.device)
+        n = res.tris.shape[0]
+        rc = _native.lib.lvbh_trace_mesh(self._ctx, ctypes.c_void_p(res.nodes.data_ptr() if n else 0),
+                                         ctypes.c_void_p(res.tris.data_ptr() if n else 0),
+                                         ctypes.c_void_p(verts4.data_ptr() if n else 0), verts4.shape[0], n,
+                                         ctypes.c_void_p(rays.data_ptr()), nr, ctypes.c_void_p(prim.data_ptr()),
+                                         ctypes.c_void_p(t.data_ptr()), ctypes.c_void_p(st.data_ptr()),
+                                         _stream_ptr(stream, self.device))
+        _native.check(self._ctx, rc)
+        return prim, t, st
 
     def build_batched(self, tri, offsets, seg_bounds=None, outputs=None, stream=None, sync=True,
                       profile=False, graph=True, autotune=False) -> BatchResult:

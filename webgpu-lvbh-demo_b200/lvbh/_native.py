@@ -93,6 +93,10 @@ def _load():
     L.lvbh_build_soup.argtypes = [vp, vp, u32, vp, u32, ctypes.POINTER(Result), vp]
     L.lvbh_build_indexed.restype = i32
     L.lvbh_build_indexed.argtypes = [vp, vp, u32, vp, u32, vp, u32, ctypes.POINTER(Result), vp]
+    L.lvbh_build_mesh.restype = i32
+    L.lvbh_build_mesh.argtypes = [vp, vp, u32, vp, u32, vp, u32, ctypes.POINTER(Result), vp]
+    L.lvbh_trace_mesh.restype = i32
+    L.lvbh_trace_mesh.argtypes = [vp, vp, vp, vp, u32, u32, vp, u32, vp, vp, vp, vp]
     L.lvbh_build_batched.restype = i32
     L.lvbh_build_batched.argtypes = [vp, vp, vp, u32, vp, vp, u32, ctypes.POINTER(Result), vp]
     L.lvbh_set_tunables.restype = i32
