@@ -49,7 +49,7 @@ size_t control_bytes(uint32_t n) {
 size_t arena_bytes(uint32_t cap) {
     const size_t groups = emit_groups(cap);
     return 4 * align_up((size_t)cap * 4) + align_up((size_t)cap * 32) + align_up((size_t)cap) +
-           align_up(groups * kOpenCap * sizeof(OpenItem)) + align_up(groups * sizeof(uint32_t)) +
+           align_up(groups * kOpenCap * sizeof(OpenItem)) + align_up(2 * groups * sizeof(uint32_t)) +
            align_up(sizeof(uint32_t)) + control_bytes(cap);
 }
 
@@ -263,7 +263,7 @@ int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
     ctx->pend = reinterpret_cast<float4 *>(c); c += align_up((size_t)cap * 32);
     ctx->pend_d = reinterpret_cast<uint8_t *>(c); c += align_up((size_t)cap);
     ctx->items = reinterpret_cast<OpenItem *>(c); c += align_up(groups * kOpenCap * sizeof(OpenItem));
-    ctx->counts = reinterpret_cast<uint32_t *>(c); c += align_up(groups * sizeof(uint32_t));
+    ctx->counts = reinterpret_cast<uint32_t *>(c); c += align_up(2 * groups * sizeof(uint32_t));  // blocks, groups
     ctx->epoch = reinterpret_cast<uint32_t *>(c); c += align_up(sizeof(uint32_t));
     ctx->ctl = reinterpret_cast<Control *>(c);
     ctx->lookback = reinterpret_cast<uint32_t *>(c + align_up(sizeof(Control)));

@@ -34,6 +34,8 @@
 //                        most 64 deep).
 //   K3c (k_emit_top)     the nodes that straddle blocks (~3 % of them), built bottom-up from
 //                        the open items with arrival words in global memory (see below).
+#include <type_traits>
+
 #include "lvbh_device.cuh"
 #include "lvbh_internal.h"
 
@@ -399,17 +401,17 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
 // Nothing waits, so the kernel cannot hang; climbs are bounded and every index is
 // range-checked.  The epoch makes the arrival words reusable without clearing: a word left by
 // an older build never equals the current epoch.
-template <class Segs>
-__global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__restrict__ items,
+template <class Segs, int LANES = kTopLanes>
+__global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__restrict__ items, int cap,
                                                   const uint32_t *__restrict__ counts,
                                                   float4 *nodes_all, int32_t *parents_all,
                                                   uint32_t *arrive_all, float4 *pend_all,
                                                   uint8_t *pend_d_all,
                                                   const uint32_t *__restrict__ epoch_p,
                                                   Control *ctl) {
-    const int gw = (blockIdx.x * 256 + threadIdx.x) / kTopLanes, lane = threadIdx.x % kTopLanes;
+    const int gw = (blockIdx.x * 256 + threadIdx.x) / LANES, lane = threadIdx.x % LANES;
     if (gw >= segs.blocks()) return;
-    const int cnt = (int)min(counts[gw], (uint32_t)kOpenCap);
+    const int cnt = (int)min(counts[gw], (uint32_t)cap);
     if (lane >= cnt) return;
     const uint32_t epoch = *epoch_p;
     const Span sp = segs.span(gw);
@@ -419,8 +421,8 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
     uint32_t *arrive = arrive_all + sp.start;
     float4 *pend = pend_all + 2ull * sp.start;
     uint8_t *pend_d = pend_d_all + sp.start;
-    for (int q = lane; q < cnt; q += kTopLanes) {
-        const OpenItem it = items[(size_t)gw * kOpenCap + q];
+    for (int q = lane; q < cnt; q += LANES) {
+        const OpenItem it = items[(size_t)gw * cap + q];
         int l = it.xl, r = it.xr, ref = __float_as_int(it.lo.w);
         float nx = it.lo.x, ny = it.lo.y, nz = it.lo.z, xx = it.hi.x, xy = it.hi.y, xz = it.hi.z;
         int dl = it.pad0, dr = __float_as_int(it.hi.w);
@@ -477,6 +479,169 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
     }
 }
 
+// K3c, first level (plain builds): one block per group of kGroupBlocks consecutive K3b blocks
+// climbs the group's open items through every split both of whose sides lie in the group, in
+// shared memory - the same park / merge handshake as K3b, splits found through a hash table,
+// rounds separated by block barriers - and writes those records and parent links.  What is
+// left (items whose next split leaves the group, children parked at a split whose sibling
+// never came) replaces the group's items, packed from its first block's slot on, for the
+// global pass (k_emit_top over groups), which so sees about 1 / kGroupBlocks of the items.
+// A group with more than kGroupCap items packs them all for the global pass unchanged.
+constexpr int kGroupBlocks = 16;
+constexpr int kGroupCap = 256;
+constexpr int kGroupHash = 512;   // slots (power of two); distinct splits <= 2 x items
+constexpr int kGroupThreads = 128;
+constexpr int kGroupLanes = 64;   // threads per group in the global pass
+
+struct GroupSmem {
+    OpenItem it[kGroupCap];
+    int act[2][kGroupCap];
+    int out[kGroupCap];
+    int hkey[kGroupHash];
+    uint32_t hmask[kGroupHash];
+    int hidx[kGroupHash][2];
+    int bstart[kGroupBlocks + 1];
+    int cnt[2];
+    int nout;
+};
+
+template <int LOG>
+__global__ void __launch_bounds__(kGroupThreads) k_top_group(int n, OpenItem *items, const uint32_t *__restrict__ counts,
+                                                   uint32_t *__restrict__ group_counts, float4 *nodes,
+                                                   int32_t *parents, Control *ctl) {
+    constexpr int EB = 1 << LOG;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GroupSmem &S = *reinterpret_cast<GroupSmem *>(smem_raw);
+    const int t = threadIdx.x;
+    const int nblk = (n + EB - 1) / EB;
+    const int g = blockIdx.x, blk0 = g * kGroupBlocks, blk1 = min(nblk, blk0 + kGroupBlocks);
+    const int lo_leaf = blk0 * EB, hi_leaf = min(n, blk1 * EB);
+    OpenItem *gitems = items + (size_t)blk0 * kOpenCap;
+    if (t < 32) {  // the blocks' item counts and their exclusive prefix (one warp)
+        const int c = (t < kGroupBlocks && blk0 + t < blk1) ? (int)min(counts[blk0 + t], (uint32_t)kOpenCap) : 0;
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (t >= o) incl += y;
+        }
+        if (t <= kGroupBlocks) S.bstart[t] = incl - c;
+        if (t == 31) {
+            S.cnt[0] = min(incl, kGroupCap);
+            S.cnt[1] = 0;
+            S.nout = 0;
+        }
+    }
+    for (int h = t; h < kGroupHash; h += kGroupThreads) {
+        S.hkey[h] = -1;
+        S.hmask[h] = 0u;
+    }
+    __syncthreads();
+    const int total = S.bstart[kGroupBlocks];  // blocks past blk1 count zero
+    if (total > kGroupCap) {
+        // pack every item for the global pass, block by block through shared memory (the
+        // packed slots lie at or below the ones they come from)
+        for (int b = blk0; b < blk1; ++b) {
+            const int c = S.bstart[b - blk0 + 1] - S.bstart[b - blk0];
+            for (int k = t; k < c; k += kGroupThreads) S.it[k] = items[(size_t)b * kOpenCap + k];
+            __syncthreads();
+            for (int k = t; k < c; k += kGroupThreads) gitems[S.bstart[b - blk0] + k] = S.it[k];
+            __syncthreads();
+        }
+        if (t == 0) group_counts[g] = (uint32_t)min(total, kGroupBlocks * kOpenCap);
+        return;
+    }
+    for (int b = blk0; b < blk1; ++b) {
+        const int c = S.bstart[b - blk0 + 1] - S.bstart[b - blk0];
+        for (int k = t; k < c; k += kGroupThreads) {
+            const int at = S.bstart[b - blk0] + k;
+            S.it[at] = items[(size_t)b * kOpenCap + k];
+            S.act[0][at] = at;
+        }
+    }
+    auto push_out = [&](int i) {
+        const int at = atomicAdd(&S.nout, 1);
+        S.out[at] = i;  // at most one entry per item: < kGroupCap
+    };
+    int cur = 0;
+    for (int round = 0; round < 4 * EB; ++round) {
+        __syncthreads();
+        const int count = S.cnt[cur];
+        if (count == 0) break;
+        for (int a = t; a < count; a += kGroupThreads) {
+            const int i = S.act[cur][a];
+            const OpenItem it = S.it[i];
+            const int l = it.xl, r = it.xr, dl = it.pad0, dr = __float_as_int(it.hi.w);
+            const bool is_left = dr > dl;
+            const int s = is_left ? r : l - 1;
+            if (s < lo_leaf || s + 1 >= hi_leaf || s < 0 || s >= n - 1) {
+                push_out(i);
+                continue;
+            }
+            uint32_t h = ((uint32_t)s * 2654435761u) & (kGroupHash - 1);
+            for (int probe = 0; probe < kGroupHash; ++probe) {
+                const int prev = atomicCAS(&S.hkey[h], -1, s);
+                if (prev == -1 || prev == s) break;
+                h = (h + 1) & (kGroupHash - 1);
+            }
+            const int side = is_left ? 0 : 1;
+            S.hidx[h][side] = i;
+            if (atom_or_acq_rel_cta(&S.hmask[h], 1u << side) == 0u) continue;  // first parks
+            const int j = S.hidx[h][side ^ 1];
+            const OpenItem sb = S.it[j];
+            const int L = is_left ? l : sb.xl, R = is_left ? sb.xr : r;
+            const int ndl = is_left ? dl : sb.pad0, ndr = is_left ? __float_as_int(sb.hi.w) : dr;
+            const bool root = L == 0 && R == n - 1;
+            const int P = root ? 0 : (ndr > ndl ? R : L);
+            const OpenItem &lc = is_left ? it : sb;
+            const OpenItem &rc = is_left ? sb : it;
+            float4 *rec = nodes + 4ull * P;
+            rec[0] = lc.lo;
+            rec[1] = make_float4(lc.hi.x, lc.hi.y, lc.hi.z, __int_as_float(2));
+            rec[2] = rc.lo;
+            rec[3] = make_float4(rc.hi.x, rc.hi.y, rc.hi.z, __int_as_float(0));
+            const int lref = __float_as_int(lc.lo.w), rref = __float_as_int(rc.lo.w);
+            parents[lref >= 0 ? lref : n - (lref + 1)] = P;
+            parents[rref >= 0 ? rref : n - (rref + 1)] = P;
+            if (root) continue;
+            OpenItem pa;
+            pa.lo = make_float4(fminf(it.lo.x, sb.lo.x), fminf(it.lo.y, sb.lo.y), fminf(it.lo.z, sb.lo.z),
+                                __int_as_float(P));
+            pa.hi = make_float4(fmaxf(it.hi.x, sb.hi.x), fmaxf(it.hi.y, sb.hi.y), fmaxf(it.hi.z, sb.hi.z),
+                                __int_as_float(ndr));
+            pa.xl = L;
+            pa.xr = R;
+            pa.pad0 = ndl;
+            pa.pad1 = 0;
+            S.it[i] = pa;
+            const int at = atomicAdd(&S.cnt[cur ^ 1], 1);
+            S.act[cur ^ 1][at] = i;
+        }
+        __syncthreads();
+        if (t == 0) S.cnt[cur] = 0;
+        cur ^= 1;
+    }
+    __syncthreads();
+    // a child parked at a split whose sibling never came: its parent leaves the group
+    for (int h = t; h < kGroupHash; h += kGroupThreads) {
+        const uint32_t mk = S.hmask[h];
+        if (mk == 1u || mk == 2u) push_out(S.hidx[h][mk == 1u ? 0 : 1]);
+    }
+    __syncthreads();
+    const int nout = S.nout;
+    for (int k = t; k < nout; k += kGroupThreads) gitems[k] = S.it[S.out[k]];
+    if (t == 0) group_counts[g] = (uint32_t)nout;
+}
+
+// The global pass over groups: group g's items from its first block's slot on.
+template <int LOG>
+struct GroupSegs {
+    int n;
+    __device__ __forceinline__ int blocks() const { return ((n + (1 << LOG) - 1) >> LOG) / kGroupBlocks +
+                                                           ((((n + (1 << LOG) - 1) >> LOG) % kGroupBlocks) != 0); }
+    __device__ __forceinline__ Span span(int g) const { return Span{0, n, g * kGroupBlocks * (1 << LOG)}; }
+};
+
 template <int LOG>
 inline size_t leaves_smem_bytes() { return sizeof(ClimbSmem<TreeGeo<LOG>::EB>); }
 
@@ -492,10 +657,22 @@ void launch_emit_impl(Segs segs, int groups, Leaves lv, const uint32_t *keys, fl
     k_tree_climb<LOG, Segs, Leaves><<<grid, TreeGeo<LOG>::EB, leaves_smem_bytes<LOG>(), s>>>(
         segs, keys, lv, nodes, parents, items, counts, ctl);
     if (ev) cudaEventRecord(ev[1], s);
-    if (top)
-        k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, counts, nodes,
-                                                                     parents, arrive, pend, pend_d,
-                                                                     epoch, ctl);
+    if (top) {
+        if constexpr (std::is_same<Segs, OneSeg<LOG>>::value) {
+            const int ngroups = (groups + kGroupBlocks - 1) / kGroupBlocks;
+            uint32_t *gcounts = counts + groups;  // the counts buffer holds 2 x groups words
+            k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(segs.n, items, counts, gcounts, nodes,
+                                                                   parents, ctl);
+            // a group leaves a few dozen items: one lane each
+            k_emit_top<GroupSegs<LOG>, kGroupLanes><<<(ngroups * kGroupLanes + 255) / 256, 256, 0, s>>>(
+                GroupSegs<LOG>{segs.n}, items, kGroupBlocks * kOpenCap, gcounts, nodes, parents, arrive, pend,
+                pend_d, epoch, ctl);
+        } else {
+            k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, kOpenCap, counts, nodes,
+                                                                         parents, arrive, pend, pend_d,
+                                                                         epoch, ctl);
+        }
+    }
     if (ev) cudaEventRecord(ev[2], s);
 }
 
@@ -516,6 +693,9 @@ cudaError_t emit_init() {
     if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, ManySegs<8>>, leaves_smem_bytes<8>());
     if (e == cudaSuccess) e = prefer_shared(k_tree_climb<7, ManySegs<7>>, leaves_smem_bytes<7>());
     if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, OneSeg<8>, MeshLeaves>, leaves_smem_bytes<8>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_top_group<kLogEmitBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(GroupSmem));
     return e;
 }
 
