@@ -58,6 +58,8 @@ struct ObjCtl {
     uint32_t bad_index;   // a model-0 face names no vertex
     uint32_t num_hard;    // vertex lines left to the host parser
     uint32_t newlines;
+    uint32_t m0a, m0b;    // model 0's lines [m0a, m0b)
+    uint32_t no_model;    // the text defines no model (output.models[0] is undefined)
     uint32_t pad;
     unsigned long long totals;  // model-0 vertices (low 32 bits) and triangles (high 32 bits)
     unsigned long long bmin[3], bmax[3];  // ordered doubles (ord64)
@@ -575,11 +577,31 @@ __global__ void __launch_bounds__(kLineBlock) k_lines(const uint8_t *__restrict_
     warp_min_into(need ? l : kNone, &ctl->first_need);
 }
 
-// The first `o` line after line fo.
+// The first `o` line after the first one.
 __global__ void __launch_bounds__(kT) k_second_o(const uint8_t *__restrict__ type, uint32_t L,
-                                                 uint32_t fo, ObjCtl *__restrict__ ctl) {
+                                                 ObjCtl *__restrict__ ctl) {
+    const uint32_t fo = ctl->first_o;
+    if (fo == kNone) return;
     const uint32_t l = blockIdx.x * kT + threadIdx.x;
     warp_min_into(l < L && l > fo && type[l] == LT_O ? l : kNone, &ctl->second_o);
+}
+
+// Model 0's lines: the default model when a model-creating statement precedes the first `o`
+// (_currentModel, obj-file-parser.js:82-91), else the model that `o` opens, up to the next `o`.
+__global__ void k_model_range(uint32_t L, ObjCtl *__restrict__ ctl) {
+    const uint32_t fo = ctl->first_o, fn = ctl->first_need, so = ctl->second_o;
+    uint32_t a = 0, b = 0, none = 0;
+    if (fn != kNone && (fo == kNone || fn < fo)) {
+        b = fo == kNone ? L : fo;
+    } else if (fo != kNone) {
+        a = fo;
+        b = so == kNone ? L : so;
+    } else {
+        none = 1;
+    }
+    ctl->m0a = a;
+    ctl->m0b = b;
+    ctl->no_model = none;
 }
 
 // Packed count of a model-0 line: one vertex (low 32 bits) or a face's triangles (high).
@@ -589,37 +611,41 @@ __device__ __forceinline__ unsigned long long line_count(const uint8_t *type, co
     return t == LT_V ? 1ull : t == LT_F ? (unsigned long long)fans[l] << 32 : 0ull;
 }
 
-// Tile sums of the packed counts of lines [a, a + m).
+// Tile sums of the packed counts of the L lines (zero outside model 0's [m0a, m0b)).
 __global__ void __launch_bounds__(kT) k_scan_up(const uint8_t *__restrict__ type,
-                                                const uint32_t *__restrict__ fans, uint32_t a,
-                                                uint32_t m, unsigned long long *__restrict__ sums) {
+                                                const uint32_t *__restrict__ fans, uint32_t L,
+                                                const ObjCtl *__restrict__ ctl,
+                                                unsigned long long *__restrict__ sums) {
     __shared__ unsigned long long s_warp[kT / 32];
+    const uint32_t a = ctl->m0a, b = ctl->m0b;
     const uint64_t base = (uint64_t)blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     unsigned long long t = 0;
     for (int k = 0; k < kScanItems; ++k)
-        if (base + k < m) t += line_count(type, fans, a + (uint32_t)(base + k));
+        if (base + k >= a && base + k < b) t += line_count(type, fans, (uint32_t)(base + k));
     unsigned long long all;
     block_scan<unsigned long long>(t, s_warp, &all);
     if (threadIdx.x == 0) sums[blockIdx.x] = all;
 }
 
-// pre[i]: exclusive prefix of the packed counts for line a + i.
+// pre[l]: exclusive prefix of the packed counts at line l.
 __global__ void __launch_bounds__(kT) k_scan_down(const uint8_t *__restrict__ type,
-                                                  const uint32_t *__restrict__ fans, uint32_t a,
-                                                  uint32_t m, const unsigned long long *__restrict__ sums,
+                                                  const uint32_t *__restrict__ fans, uint32_t L,
+                                                  const ObjCtl *__restrict__ ctl,
+                                                  const unsigned long long *__restrict__ sums,
                                                   unsigned long long *__restrict__ pre) {
     __shared__ unsigned long long s_warp[kT / 32];
+    const uint32_t a = ctl->m0a, b = ctl->m0b;
     const uint64_t base = (uint64_t)blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     unsigned long long x[kScanItems], t = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        x[k] = base + k < m ? line_count(type, fans, a + (uint32_t)(base + k)) : 0ull;
+        x[k] = (base + k >= a && base + k < b) ? line_count(type, fans, (uint32_t)(base + k)) : 0ull;
         t += x[k];
     }
     unsigned long long run = sums[blockIdx.x] + block_scan<unsigned long long>(t, s_warp, nullptr);
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < m) pre[base + k] = run;
+        if (base + k < L) pre[base + k] = run;
         run += x[k];
     }
 }
@@ -673,7 +699,7 @@ __global__ void __launch_bounds__(kLineBlock) k_vertices(const uint8_t *__restri
     VertexParse r;
     if (p >= w0 && q <= w1) r = parse_vertex(win + (p - w0), (uint32_t)(q - p));
     else r = parse_vertex(text + p, (uint32_t)(q - p));
-    const uint32_t vi = (uint32_t)(pre[i] & 0xFFFFFFFFull);
+    const uint32_t vi = (uint32_t)(pre[a + i] & 0xFFFFFFFFull);
     verts[3ull * vi] = r.x;
     verts[3ull * vi + 1] = r.y;
     verts[3ull * vi + 2] = r.z;
@@ -772,8 +798,8 @@ __global__ void __launch_bounds__(kLineBlock) k_faces(const uint8_t *__restrict_
     if (mine) {
         uint64_t p, q;
         line_bytes(n, line_start, L, a + i, p, q);
-        const long long before = (long long)(pre[i] & 0xFFFFFFFFull);  // model-0 vertices so far
-        const unsigned long long out = pre[i] >> 32;
+        const long long before = (long long)(pre[a + i] & 0xFFFFFFFFull);  // model-0 vertices so far
+        const unsigned long long out = pre[a + i] >> 32;
         bool ok;
         if (p >= w0 && q <= w1) ok = emit_face(win + (p - w0), (uint32_t)(q - p), before, nverts, verts, tri, out, bd);
         else ok = emit_face(text + p, (uint32_t)(q - p), before, nverts, verts, tri, out, bd);
@@ -812,6 +838,24 @@ __global__ void __launch_bounds__(kLineBlock) k_faces(const uint8_t *__restrict_
             atomicOr(&ctl->nan_max[ax], 1u);
         }
     }
+}
+
+// The floor (parse-obj.js:62-76): two triangles at z_min + .01, 10000 out in x and y, after the
+// model's triangles; z_min = Math.min from 1e30 over the faces' vertices (NaN absorbs).
+__global__ void k_floor(const ObjCtl *__restrict__ ctl, float4 *__restrict__ tri_floor) {
+    const int v = threadIdx.x;  // 6 vertices
+    if (v >= 6) return;
+    double zmin = 1e30;
+    if (ctl->nan_min[2]) {
+        zmin = NAN;
+    } else if (ctl->bmin[2] != ~0ull) {
+        const unsigned long long o = ctl->bmin[2];
+        const double d = __longlong_as_double((long long)((o >> 63) ? (o & 0x7FFFFFFFFFFFFFFFull) : ~o));
+        zmin = d < 1e30 ? d : 1e30;
+    }
+    const float h = to_f32(__dadd_rn(zmin, .01)), f = 10000.0f, pad = __double2float_rn(3.1415);
+    const float xs[6] = {-f, f, -f, f, f, -f}, ys[6] = {-f, -f, f, -f, f, f};
+    tri_floor[v] = make_float4(xs[v], ys[v], h, pad);
 }
 
 // parseFloat of a whitespace-free token on the host, for the numbers the device leaves to it:
@@ -883,9 +927,8 @@ int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, 
         return LVBH_EPARSE;
     };
     *err_line = 0;
-    if (!sc.host) OBJ_CUDA(cudaMallocHost(&sc.host, sizeof(ObjCtl) + 256), "cudaMallocHost");
+    if (!sc.host) OBJ_CUDA(cudaMallocHost(&sc.host, sizeof(ObjCtl)), "cudaMallocHost");
     ObjCtl *hc = static_cast<ObjCtl *>(sc.host);
-    float *floor_tri = reinterpret_cast<float *>(static_cast<char *>(sc.host) + 256);
     // text (staged when it is host memory or not 16-byte aligned), control block, newline
     // counts per chunk
     const uint32_t chunks = (uint32_t)((bytes + kChunk - 1) / kChunk);
@@ -932,39 +975,24 @@ int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, 
     if (chunks) k_nl_write<<<chunks, kT, 0, s>>>(d_text, bytes, cnt, line_start);
     else OBJ_CUDA(cudaMemsetAsync(line_start, 0, 8, s), "cudaMemsetAsync");
     const uint32_t lb = (uint32_t)((L + (uint64_t)kT - 1) / kT);
+    const uint32_t tiles = (uint32_t)((L + (uint64_t)kScanTile - 1) / kScanTile);
+    // lines, model 0 and the vertex / triangle prefixes in one stream-ordered run (the first
+    // `o`, the model range and the scan read what the kernels before them left in ctl)
     k_lines<<<lb, kLineBlock, 0, s>>>(d_text, bytes, line_start, L, type, fans, ctl);
+    k_second_o<<<lb, kT, 0, s>>>(type, L, ctl);
+    k_model_range<<<1, 1, 0, s>>>(L, ctl);
+    k_scan_up<<<tiles, kT, 0, s>>>(type, fans, L, ctl, sums);
+    k_scan_small<unsigned long long><<<1, 1024, 0, s>>>(sums, tiles, &ctl->totals);
+    k_scan_down<<<tiles, kT, 0, s>>>(type, fans, L, ctl, sums, pre);
     OBJ_CUDA(cudaGetLastError(), "k_lines");
     OBJ_CUDA(cudaMemcpyAsync(hc, ctl, sizeof(ObjCtl), cudaMemcpyDeviceToHost, s), "readback");
     OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     if (hc->err_line != kNone)
         return reject(hc->err_line + 1ull, "line " + std::to_string(hc->err_line + 1ull) +
                                                 ": a statement the OBJ parser rejects");
-    // model 0: the default model when a model-creating statement precedes the first `o`, else
-    // the model that `o` opens (up to the next `o`)
-    const uint32_t fo = hc->first_o, fn = hc->first_need;
-    uint32_t m0a, m0b;
-    if (fn != kNone && (fo == kNone || fn < fo)) {
-        m0a = 0;
-        m0b = fo == kNone ? L : fo;
-    } else if (fo != kNone) {
-        k_second_o<<<lb, kT, 0, s>>>(type, L, fo, ctl);
-        OBJ_CUDA(cudaGetLastError(), "k_second_o");
-        OBJ_CUDA(cudaMemcpyAsync(&hc->second_o, &ctl->second_o, 4, cudaMemcpyDeviceToHost, s), "readback");
-        OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-        m0a = fo;
-        m0b = hc->second_o == kNone ? L : hc->second_o;
-    } else {
-        return reject(0, "the OBJ text defines no model");
-    }
-    const uint32_t m = m0b - m0a;
-    const uint32_t tiles = (uint32_t)((m + (uint64_t)kScanTile - 1) / kScanTile);
-    const uint32_t mb = (uint32_t)((m + (uint64_t)kT - 1) / kT);
-    k_scan_up<<<tiles, kT, 0, s>>>(type, fans, m0a, m, sums);
-    k_scan_small<unsigned long long><<<1, 1024, 0, s>>>(sums, tiles, &ctl->totals);
-    k_scan_down<<<tiles, kT, 0, s>>>(type, fans, m0a, m, sums, pre);
-    OBJ_CUDA(cudaGetLastError(), "k_scan");
-    OBJ_CUDA(cudaMemcpyAsync(&hc->totals, &ctl->totals, 8, cudaMemcpyDeviceToHost, s), "readback");
-    OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (hc->no_model) return reject(0, "the OBJ text defines no model");
+    const uint32_t m0a = hc->m0a, m = hc->m0b - hc->m0a;
+    const uint32_t mb = (uint32_t)((m + (uint64_t)kLineBlock - 1) / kLineBlock);
     const uint32_t nverts = (uint32_t)(hc->totals & 0xFFFFFFFFull);
     const uint64_t nfan = hc->totals >> 32;
     if (nfan + 2 > LVBH_MAX_TRIS) return reject(0, "the OBJ text makes more than LVBH_MAX_TRIS triangles");
@@ -976,13 +1004,19 @@ int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, 
     float4 *tri = static_cast<float4 *>(sc.soup);
     double *verts = reinterpret_cast<double *>(static_cast<char *>(sc.soup) + tbytes);
     HardLine *hard = reinterpret_cast<HardLine *>(static_cast<char *>(sc.soup) + tbytes + vbytes);
-    if (nverts) {
+    // vertices, faces and the floor, then one read-back; numbers the device left to the host
+    // (rare) are patched in and the faces and floor run again
+    auto faces_and_floor = [&]() {
+        if (nfan && mb)
+            k_faces<<<mb, kLineBlock, 0, s>>>(d_text, bytes, line_start, L, type, m0a, m, pre, nverts, verts, tri, ctl);
+        k_floor<<<1, 32, 0, s>>>(ctl, tri + 3ull * nfan);
+    };
+    if (nverts && mb)
         k_vertices<<<mb, kLineBlock, 0, s>>>(d_text, bytes, line_start, L, type, m0a, m, pre, verts, hard, ctl);
-        OBJ_CUDA(cudaGetLastError(), "k_vertices");
-        OBJ_CUDA(cudaMemcpyAsync(&hc->num_hard, &ctl->num_hard, 4, cudaMemcpyDeviceToHost, s), "readback");
-        OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-    }
-    // numbers outside the device's exact range: the host parses their lines
+    faces_and_floor();
+    OBJ_CUDA(cudaGetLastError(), "k_faces");
+    OBJ_CUDA(cudaMemcpyAsync(hc, ctl, sizeof(ObjCtl), cudaMemcpyDeviceToHost, s), "readback");
+    OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     const uint32_t nh = nverts ? hc->num_hard : 0;
     if (nh) {
         std::vector<HardLine> hl(nh);
@@ -1013,12 +1047,19 @@ int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, 
         OBJ_CUDA(cudaMemcpyAsync(dfix, fix.data(), nh * sizeof(HardFix), cudaMemcpyHostToDevice, s),
                  "cudaMemcpyAsync(fix)");
         k_patch<<<(nh + kT - 1) / kT, kT, 0, s>>>(dfix, nh, verts);
-        OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");  // `fix` is pageable host memory
+        // the bounds and the index check start over
+        for (int a = 0; a < 3; ++a) {
+            hc->bmin[a] = ~0ull;
+            hc->bmax[a] = 0ull;
+            hc->nan_min[a] = hc->nan_max[a] = 0u;
+        }
+        hc->bad_index = 0u;
+        OBJ_CUDA(cudaMemcpyAsync(ctl, hc, sizeof(ObjCtl), cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(ctl)");
+        faces_and_floor();
+        OBJ_CUDA(cudaGetLastError(), "k_faces");
+        OBJ_CUDA(cudaMemcpyAsync(hc, ctl, sizeof(ObjCtl), cudaMemcpyDeviceToHost, s), "readback");
+        OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");  // also: `fix` is pageable
     }
-    if (nfan) k_faces<<<mb, kLineBlock, 0, s>>>(d_text, bytes, line_start, L, type, m0a, m, pre, nverts, verts, tri, ctl);
-    OBJ_CUDA(cudaGetLastError(), "k_faces");
-    OBJ_CUDA(cudaMemcpyAsync(hc, ctl, sizeof(ObjCtl), cudaMemcpyDeviceToHost, s), "readback");
-    OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     if (hc->bad_index) return reject(0, "a face of model 0 names a vertex the model does not have");
     // bounds: Math.min / Math.max from 1e30 / -1e30 over the faces' vertices
     for (int a = 0; a < 3; ++a) {
@@ -1027,15 +1068,6 @@ int obj_parse(ObjScratch &sc, const char *text, uint64_t bytes, bool host_text, 
         bounds6[a] = hc->nan_min[a] ? NAN : (lo < 1e30 ? lo : 1e30);
         bounds6[3 + a] = hc->nan_max[a] ? NAN : (hi > -1e30 ? hi : -1e30);
     }
-    // the floor: two triangles at z_min + .01, 10000 out in x and y (parse-obj.js:62-76)
-    const double fh = bounds6[2] + .01;
-    const float pad = (float)3.1415, h = (float)fh, f = 10000.f;
-    const float ft[24] = {-f, -f, h, pad, f, -f, h, pad, -f, f, h, pad,
-                          f,  -f, h, pad, f, f,  h, pad, -f, f, h, pad};
-    std::memcpy(floor_tri, ft, sizeof ft);
-    OBJ_CUDA(cudaMemcpyAsync(tri + 3ull * nfan, floor_tri, sizeof ft, cudaMemcpyHostToDevice, s),
-             "cudaMemcpyAsync(floor)");
-    OBJ_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     *tri_out = reinterpret_cast<const float *>(tri);
     *num_tris = ntri;
 #undef OBJ_CUDA
