@@ -59,8 +59,9 @@ UNIT = "Mprims/s"
 # straddling-node pass completes part of the same tree and has no bytes of its own.
 MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "gather": 0, "tree": 192, "top": 0}
 KERNELS = {"bounds": ("k_bounds", 1), "morton": ("k_morton", 1), "sort": ("k_scatter", 3),
-           "gather": (None, 0), "tree": ("k_tree_climb", 1), "top": ("k_emit_top", 1)}
-# bounds, morton, 3 sort passes x (tile histograms, chunk scan, scatter), tree, top
+           "gather": (None, 0), "tree": ("k_tree_climb", 1), "top": ("k_emit_top", 2)}
+# bounds, morton (+ the first pass's tile histograms), 3 sort passes x (chunk scan, scatter) and
+# 2 tile-histogram passes, tree, straddling pass in two levels (group, global)
 LAUNCHES_PER_BUILD = 13
 MODEL_TOTAL = sum(MODEL_BYTES.values())  # 340 B per triangle
 
