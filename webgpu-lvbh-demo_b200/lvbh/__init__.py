@@ -157,7 +157,10 @@ class BVHBuilder:
 
     def close(self):
         if getattr(self, "_ctx", None):
-            _native.lib.lvbh_destroy(self._ctx)
+            # at interpreter exit the module's globals may already be gone
+            lib = getattr(_native, "lib", None) if _native is not None else None
+            if lib is not None:
+                lib.lvbh_destroy(self._ctx)
             self._ctx = None
 
     def __del__(self):

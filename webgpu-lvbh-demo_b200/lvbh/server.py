@@ -53,7 +53,10 @@ class Server:
 
     def close(self):
         if getattr(self, "_h", None):
-            _native.lib.lvbh_server_destroy(self._h)
+            # at interpreter exit the module's globals may already be gone
+            lib = getattr(_native, "lib", None) if _native is not None else None
+            if lib is not None:
+                lib.lvbh_server_destroy(self._h)
             self._h = None
             self._keep.clear()
 
