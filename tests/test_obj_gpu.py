@@ -141,3 +141,22 @@ def test_reuse_and_growth(builder):
     result is complete and right."""
     for seed, lines in ((10, 100), (11, 40000), (12, 50), (13, 80000)):
         check_same(builder, messy_obj(seed, lines=lines), "host", f"seed {seed}")
+
+
+def test_lines_longer_than_the_window(builder):
+    """Lines past a block's 24 KB shared-memory window are read from global memory by the same
+    scanners: a face of 12,000 vertices, a vertex line padded with 100 KB of whitespace and a
+    comment, and ordinary lines around them in the same blocks."""
+    rng = np.random.default_rng(3)
+    nv = 12_000
+    lines = ["o big"]
+    lines += ["v %.6f %.6f %.6f" % tuple(rng.normal(size=3)) for _ in range(nv)]
+    lines.insert(5, "v 1.5" + " " * 100_000 + "2.5\t3.5 # " + "c" * 30_000)
+    lines.append("f " + " ".join(str(i + 1) for i in range(nv)))
+    lines.append("f " + " ".join("-%d/1/1" % (k + 1) for k in range(3)))
+    lines.append("f 1 2 3 " + " " * 9000 + "4")
+    text = "\n".join(lines) + "\n"
+    for where in ("host", "device"):
+        check_same(builder, text, where, f"long lines {where}")
+    with_throw = text + "g" + " " * 50_000 + "\n"
+    check_same(builder, with_throw, "host", "long throwing line")
