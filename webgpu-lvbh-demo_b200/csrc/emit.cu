@@ -637,8 +637,10 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(int n, OpenItem *it
 template <int LOG>
 struct GroupSegs {
     int n;
-    __device__ __forceinline__ int blocks() const { return ((n + (1 << LOG) - 1) >> LOG) / kGroupBlocks +
-                                                           ((((n + (1 << LOG) - 1) >> LOG) % kGroupBlocks) != 0); }
+    __device__ __forceinline__ int blocks() const {
+        const int tree_blocks = (n + (1 << LOG) - 1) >> LOG;
+        return (tree_blocks + kGroupBlocks - 1) / kGroupBlocks;
+    }
     __device__ __forceinline__ Span span(int g) const { return Span{0, n, g * kGroupBlocks * (1 << LOG)}; }
 };
 
