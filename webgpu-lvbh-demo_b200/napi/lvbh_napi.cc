@@ -9,6 +9,7 @@
 //   const { initBVHBuild } = require('./lvbh_napi.node')
 //   const BVH = initBVHBuild(0)                            // CUDA device ordinal
 //   const { BVH_BUFFER, O_TRIANGLE_BUFFER } = await BVH.build(TRI_ARRAY, NUM_TRIS, BOUNDS)
+//   const { NUM_TRIS, TRI_ARR, BOUNDS } = await BVH.parseObj(fileText)   // parse-obj.js:3-88
 //
 // TRI_ARRAY is a JS number array or a Float32Array (12 floats per triangle); BOUNDS is
 // {min: [x, y, z], max: [x, y, z]} (parse-obj.js:80-87) or undefined (device reduction).
@@ -170,7 +171,120 @@ napi_value build(napi_env env, napi_callback_info info) {
     return promise;
 }
 
-// initBVHBuild(device) -> { build }
+// parseObj(text) on the GPU (scripts/obj/parse-obj.js:3-88): text is a string or a
+// Uint8Array / ArrayBuffer of the file's UTF-8 bytes.  Resolves {NUM_TRIS, TRI_ARR (a
+// Float32Array, 12 floats per triangle, floor included), BOUNDS: {min, max}}; rejects where the
+// reference throws (LVBH_EPARSE; the message names the line).
+struct ParseJob {
+    Builder *b = nullptr;
+    std::vector<char> text;
+    std::vector<float> tri;
+    uint32_t n = 0;
+    double bounds[6] = {};
+    int status = LVBH_OK;
+    std::string error;
+    napi_deferred deferred = nullptr;
+    napi_async_work work = nullptr;
+};
+
+void parse_execute(napi_env, void *data) {
+    auto *j = static_cast<ParseJob *>(data);
+    const float *dtri = nullptr;
+    uint64_t line = 0;
+    j->status = lvbh_parse_obj(j->b->ctx, j->text.data(), j->text.size(), LVBH_INPUT_HOST, &dtri, &j->n,
+                               j->bounds, &line, nullptr);
+    if (j->status != LVBH_OK) {
+        j->error = lvbh_last_error(j->b->ctx);
+        return;
+    }
+    j->tri.resize(12ull * j->n);
+    if (lvbh_copy_to_host(j->b->ctx, j->tri.data(), dtri, j->tri.size() * sizeof(float), nullptr)) {
+        j->status = LVBH_ECUDA;
+        j->error = lvbh_last_error(j->b->ctx);
+    }
+}
+
+void parse_complete(napi_env env, napi_status, void *data) {
+    auto *j = static_cast<ParseJob *>(data);
+    if (j->status != LVBH_OK) {
+        napi_value msg, err;
+        napi_create_string_utf8(env, j->error.c_str(), NAPI_AUTO_LENGTH, &msg);
+        napi_create_error(env, nullptr, msg, &err);
+        napi_reject_deferred(env, j->deferred, err);
+    } else {
+        napi_value out, ab, arr, num, bounds, mn, mx, v;
+        void *p = nullptr;
+        napi_create_object(env, &out);
+        napi_create_arraybuffer(env, j->tri.size() * sizeof(float), &p, &ab);
+        if (!j->tri.empty()) std::memcpy(p, j->tri.data(), j->tri.size() * sizeof(float));
+        napi_create_typedarray(env, napi_float32_array, j->tri.size(), ab, 0, &arr);
+        napi_create_uint32(env, j->n, &num);
+        napi_create_object(env, &bounds);
+        napi_create_array_with_length(env, 3, &mn);
+        napi_create_array_with_length(env, 3, &mx);
+        for (uint32_t a = 0; a < 3; ++a) {
+            napi_create_double(env, j->bounds[a], &v);
+            napi_set_element(env, mn, a, v);
+            napi_create_double(env, j->bounds[3 + a], &v);
+            napi_set_element(env, mx, a, v);
+        }
+        napi_set_named_property(env, bounds, "min", mn);
+        napi_set_named_property(env, bounds, "max", mx);
+        napi_set_named_property(env, out, "NUM_TRIS", num);
+        napi_set_named_property(env, out, "TRI_ARR", arr);
+        napi_set_named_property(env, out, "BOUNDS", bounds);
+        napi_resolve_deferred(env, j->deferred, out);
+    }
+    napi_delete_async_work(env, j->work);
+    delete j;
+}
+
+napi_value parse_obj(napi_env env, napi_callback_info info) {
+    size_t argc = 1;
+    napi_value argv[1];
+    void *data = nullptr;
+    NAPI_OK(env, napi_get_cb_info(env, info, &argc, argv, nullptr, &data));
+    auto *j = new ParseJob();
+    j->b = static_cast<Builder *>(data);
+    napi_valuetype t = napi_undefined;
+    if (argc > 0) napi_typeof(env, argv[0], &t);
+    bool is_typed = false, is_ab = false;
+    if (argc > 0) {
+        napi_is_typedarray(env, argv[0], &is_typed);
+        napi_is_arraybuffer(env, argv[0], &is_ab);
+    }
+    if (t == napi_string) {
+        size_t len = 0;
+        NAPI_OK(env, napi_get_value_string_utf8(env, argv[0], nullptr, 0, &len));
+        j->text.resize(len + 1);
+        NAPI_OK(env, napi_get_value_string_utf8(env, argv[0], j->text.data(), len + 1, &len));
+        j->text.resize(len);
+    } else if (is_typed || is_ab) {
+        void *raw = nullptr;
+        size_t len = 0;
+        if (is_typed) {
+            napi_typedarray_type type;
+            size_t count = 0;
+            NAPI_OK(env, napi_get_typedarray_info(env, argv[0], &type, &count, &raw, nullptr, nullptr));
+            len = count;  // a Uint8Array: one byte per element
+        } else {
+            NAPI_OK(env, napi_get_arraybuffer_info(env, argv[0], &raw, &len));
+        }
+        j->text.assign(static_cast<char *>(raw), static_cast<char *>(raw) + len);
+    } else {
+        delete j;
+        napi_throw_type_error(env, nullptr, "parseObj expects a string or the file's bytes");
+        return nullptr;
+    }
+    napi_value promise, name;
+    NAPI_OK(env, napi_create_promise(env, &j->deferred, &promise));
+    napi_create_string_utf8(env, "lvbh.parseObj", NAPI_AUTO_LENGTH, &name);
+    NAPI_OK(env, napi_create_async_work(env, nullptr, name, parse_execute, parse_complete, j, &j->work));
+    NAPI_OK(env, napi_queue_async_work(env, j->work));
+    return promise;
+}
+
+// initBVHBuild(device) -> { build, parseObj }
 napi_value init_bvh_build(napi_env env, napi_callback_info info) {
     size_t argc = 1;
     napi_value argv[1];
@@ -190,6 +304,8 @@ napi_value init_bvh_build(napi_env env, napi_callback_info info) {
     NAPI_OK(env, napi_create_object(env, &obj));
     NAPI_OK(env, napi_create_function(env, "build", NAPI_AUTO_LENGTH, build, b, &fn));
     NAPI_OK(env, napi_set_named_property(env, obj, "build", fn));
+    NAPI_OK(env, napi_create_function(env, "parseObj", NAPI_AUTO_LENGTH, parse_obj, b, &fn));
+    NAPI_OK(env, napi_set_named_property(env, obj, "parseObj", fn));
     NAPI_OK(env, napi_wrap(env, obj, b, finalize_builder, nullptr, nullptr));
     return obj;
 }
