@@ -271,3 +271,18 @@ def check_tree_properties(tri, got):
         bmax = np.where(bmax == 0, np.float32(1e-8), bmax)
         np.testing.assert_array_equal(f[idx[lm], side:side + 3], bmin)
         np.testing.assert_array_equal(f[idx[lm], side + 4:side + 7], bmax)
+
+
+def test_shrinking_builds_on_one_context(builder):
+    """Builds of shrinking sizes on one context: scratch laid out for an earlier, larger build
+    (open-item lists, level counters of the straddling pass) must not leak into a later one."""
+    from lvbh import scenes
+    for n in (1 << 20, 300_001, 131_072, 70_001, 5000):
+        tri = scenes.clustered_soup(n, seed=n % 97)
+        _, got = build_np(builder, tri)
+        assert_same(got, oracle_build(tri), f"n={n}")
+
+
+def oracle_build(tri):
+    import oracle
+    return oracle.build(tri, None, threads=0)
