@@ -905,6 +905,7 @@ int lvbh_sync(lvbh_ctx *ctx) {
     if (err & ERR_BAD_INDEX) return fail(ctx, LVBH_EINVAL, "vertex index out of range");
     if (err & ERR_NONFINITE) return fail(ctx, LVBH_EINVAL, "non-finite vertex coordinate in the input");
     if (err & ERR_LOOKBACK_TIMEOUT) return fail(ctx, LVBH_ETIMEOUT, "radix sort look-back wait exceeded its bound");
+    if (err & ERR_COPY_TIMEOUT) return fail(ctx, LVBH_ETIMEOUT, "leaf gather copy wait exceeded its bound");
     if (err & ERR_CLIMB) return fail(ctx, LVBH_EDEVICE, "refit climb exceeded the maximum tree depth");
     return LVBH_OK;
 }

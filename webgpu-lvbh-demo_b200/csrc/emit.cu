@@ -17,12 +17,11 @@
 // into the parent's record and climbs on.  No per-node binary search, N-1 box unions.
 //
 // Passes.
-//   K3a (k_leaf_gather)  one thread per sorted leaf k: gathers triangle perm[k] (3 x 16-byte
-//                        loads), writes it to the output soup at k, and writes its box (exact-
-//                        zero components nudged by 1e-8 as bvh-up-pass.js:209-210 does) to a
-//                        24-byte scratch record.  Random-access bound.
 //   K3b (k_tree_climb)   blocks of 256 sorted leaves in shared memory, a persistent grid that
-//                        prefetches the next block.  The climb runs in steps: the items still
+//                        prefetches the next block: leaf k's triangle perm[k] arrives by one
+//                        48-byte bulk copy, goes to the output soup at k and is reduced to its
+//                        box (exact-zero components nudged by 1e-8 as bvh-up-pass.js:209-210
+//                        does).  The random gather bounds the pass.  The climb runs in steps: the items still
 //                        climbing after a step are compacted into a queue, so warps stay full
 //                        while the number of items shrinks.  Parking and merging use an
 //                        arrival mask per split (shared-memory atomics) and parked items in
@@ -119,7 +118,7 @@ struct MeshLeaves {
 
 template <int EB>
 struct ClimbSmem {
-    float4 tri[2][EB][3];   // the gathered triangles of this block and the next (cp.async)
+    float4 tri[2][EB][3];   // the gathered triangles of this block and the next (bulk copies)
     float4 pend[2][2][EB];  // [side][min/max][split] the child parked at each split
     float4 q[2][2][EB / 2]; // [queue][min/max][item] the items of the current and the next
                             // step (a step after the first has at most EB / 2: every merge
@@ -131,12 +130,15 @@ struct ClimbSmem {
                             // (-1 = not set here)
     int cnt[3];             // item counters, rotating over the steps
     int open;               // open items emitted
+    uint64_t bar[2];        // completion of the bulk copies into tri[0] / tri[1]
 };
 
 // K3b: leaf gather, rearrange and the tree over blocks of EB sorted leaves (see the pass list
 // above).  Leaf t of a block gathers triangle perm[b0 + t]: its index is loaded two blocks
-// ahead, its three 16-byte rows are copied into shared memory one block ahead (cp.async, no
-// registers held meanwhile), then written to the output soup and reduced to the leaf box.
+// ahead, its 48-byte row is copied into shared memory one block ahead (one bulk copy per leaf
+// on the copy engine, completing on the buffer's mbarrier; no registers held meanwhile), then
+// written to the output soup and reduced to the leaf box.  A mesh leaf copies its three 16-byte
+// vertex rows the same way.
 template <int LOG, class Segs, class Leaves = SoupLeaves>
 __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_tree_climb(Segs segs,
                                                     const uint32_t *__restrict__ keys_all,
@@ -175,28 +177,31 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         nsp = segs.span(blk);
         const uint32_t *keys = keys_all + nsp.start;
         const int b0 = nsp.b0, n = nsp.n, k = b0 + t;
+        // the phase expects 48 bytes per leaf of the block; thread 0's arrival is its only one
+        if (t == 0) mbar_arrive_tx(&S.bar[buf], 48u * (uint32_t)min(EB, n - b0));
         if (k < n) {
             nk = __ldg(keys + k);
             if constexpr (Leaves::kMesh) {
                 // an index past the vertex buffer was reported by the Morton pass; read row 0
                 const uint32_t nv = lv.nverts;
-                cp_async16(&S.tri[buf][t][0], lv.verts + (pa < nv ? pa : 0u));
-                cp_async16(&S.tri[buf][t][1], lv.verts + (pb < nv ? pb : 0u));
-                cp_async16(&S.tri[buf][t][2], lv.verts + (pc < nv ? pc : 0u));
+                bulk_g2s(&S.tri[buf][t][0], lv.verts + (pa < nv ? pa : 0u), 16u, &S.bar[buf]);
+                bulk_g2s(&S.tri[buf][t][1], lv.verts + (pb < nv ? pb : 0u), 16u, &S.bar[buf]);
+                bulk_g2s(&S.tri[buf][t][2], lv.verts + (pc < nv ? pc : 0u), 16u, &S.bar[buf]);
             } else {
                 uint32_t ti = pa;
                 if (ti >= (uint32_t)n) { bad_perm = true; ti = 0; }
-                const float4 *src = lv.tri + 3ull * (nsp.start + ti);
-                cp_async16(&S.tri[buf][t][0], src);
-                cp_async16(&S.tri[buf][t][1], src + 1);
-                cp_async16(&S.tri[buf][t][2], src + 2);
+                bulk_g2s(&S.tri[buf][t][0], lv.tri + 3ull * (nsp.start + ti), 48u, &S.bar[buf]);
             }
         }
-        cp_async_commit();
         if (t == 0) nk_lo = b0 > 0 ? __ldg(keys + b0 - 1) : 0u;
         if (t == EB - 1) nk_hi = (b0 + EB < n) ? __ldg(keys + b0 + EB) : 0u;
     };
     int buf = 0;
+    uint32_t phase = 0;  // bit b: parity of the next phase of S.bar[b] (uniform over the block)
+    bool copy_timeout = false;
+    if (t < 2) mbar_init(&S.bar[t], 1);
+    mbar_init_fence();
+    __syncthreads();
     if ((int)blockIdx.x < nblk) {
         fetch_perm(blockIdx.x);
         fetch_leaf(blockIdx.x, 0);
@@ -221,7 +226,8 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         if (t == 0) S.open = 0;
         // this leaf's triangle: to the output soup, and its box (exact-zero components nudged
         // by 1e-8 as bvh-up-pass.js:209-210 does)
-        cp_async_wait_all();
+        if (!mbar_wait(&S.bar[buf], (phase >> buf) & 1u)) copy_timeout = true;
+        phase ^= 1u << buf;
         float4 leaf_lo = make_float4(0.f, 0.f, 0.f, __int_as_float(-(k + 1)));
         float4 leaf_hi0 = make_float4(0.f, 0.f, 0.f, 0.f);
         if (active) {
@@ -253,7 +259,10 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
                 parents[1] = 0;
                 out_counts[blk] = 0;
             }
-            continue;  // uniform across the block; no other thread reads what this one wrote
+            // uniform across the block; no other thread reads what this one wrote.  The barrier
+            // keeps every thread's wait on this buffer's phase ahead of its next arming.
+            __syncthreads();
+            continue;
         }
         if (k == 0) {  // the root has no parent; slot N-1 and record N-1 stay zero
             parents[0] = 0;
@@ -386,6 +395,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         }
     }
     if (bad_perm) atomicOr(&ctl->err, ERR_CLIMB);
+    if (copy_timeout) atomicOr(&ctl->err, ERR_COPY_TIMEOUT);
 }
 
 // K3c: the nodes that straddle blocks.  kTopLanes threads per block of K3b; each climbs one of

@@ -12,6 +12,7 @@ enum : uint32_t {
     ERR_LOOKBACK_TIMEOUT = 2u,  // a decoupled look-back wait exceeded its bound
     ERR_CLIMB = 4u,             // a refit climb exceeded the depth any valid tree has
     ERR_BAD_INDEX = 8u,         // an indexed-mesh vertex index is out of range
+    ERR_COPY_TIMEOUT = 16u,     // a bulk-copy wait (mbarrier) exceeded its bound
 };
 
 // Largest number of cycles a device-side wait spins before it records an error and gives up
@@ -99,13 +100,38 @@ __device__ __forceinline__ void st_relaxed_gpu(uint32_t *p, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// 16-byte asynchronous copy global -> shared (L2 only), its group commit and wait.
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+// Bulk asynchronous copies global -> shared (the TMA engine, no tensor map) completing on an
+// mbarrier in this CTA's shared memory.  A random gather of small rows runs far faster this way
+// than through per-thread 16-byte cp.async: on the B200 a gather of 16.7 M random 48-byte rows
+// into shared memory took 0.66 ms as one 48-byte bulk copy per row, 1.14 ms as three cp.async.
+// Addresses and sizes are multiples of 16 bytes.  No multicast.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// makes initialised mbarriers visible to the copy engine; a CTA barrier follows before use
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// one arrival that also raises the phase's expected byte count
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gmem_src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(smem_dst)), "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+// Waits for the completion of the mbarrier phase of the given parity, at most kSpinLimitCycles;
+// false if the bound ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    long long t0 = 0;
+    for (uint32_t it = 0;; ++it) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+        if (ok) return true;
+        if (it == 0) t0 = clock64();
+        else if (clock64() - t0 > kSpinLimitCycles) return false;
+    }
+}
 
 // Streaming (evict-first) 16-byte load and store.
 __device__ __forceinline__ float4 ld_stream(const float4 *p) { return __ldcs(p); }
