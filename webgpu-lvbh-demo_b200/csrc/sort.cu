@@ -414,17 +414,26 @@ __global__ void __launch_bounds__(T, 4) k_scatter(const uint32_t *__restrict__ k
         const uint32_t idx = wbase + i * 32 + lane;
         k[i] = idx < n ? __ldcs(keys_in + idx) : 0u;
     }
-    // the digit prefixes of this tile (final values: independent loads, in flight with the
-    // keys), parked in S.out until the tile's own starts are known
+    // the tile's values are read only when they are staged, after the ranking: start bringing
+    // them into L2 now (one 128-byte line of 32 values per lane)
+    if (vals_in && lane < IPT && wbase + lane * 32 < n)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(vals_in + wbase + lane * 32));
+    // the digit prefixes of this tile (final values: independent 16-byte loads, all in flight
+    // with the keys), parked in S.out until the tile's own starts are known
     {
-        const uint32_t chunk = tile / chunk_tiles;
-        uint32_t pre[P];
+        static_assert(P == 4, "one 16-byte load per row");
+        const uint32_t chunk = tile / chunk_tiles, t0c = chunk * chunk_tiles;
+        uint4 acc = __ldg(reinterpret_cast<const uint4 *>(chunk_off + (size_t)chunk * D + tid * P));
+        uint4 row[kSortChunkTiles - 1];
 #pragma unroll
-        for (int j = 0; j < P; ++j) pre[j] = __ldg(chunk_off + (size_t)chunk * D + tid * P + j);
-        for (uint32_t t = chunk * chunk_tiles; t < tile; ++t) {
+        for (int q = 0; q < kSortChunkTiles - 1; ++q)
+            row[q] = t0c + q < tile ? __ldg(reinterpret_cast<const uint4 *>(tile_hist + (size_t)(t0c + q) * D + tid * P))
+                                    : make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
-            for (int j = 0; j < P; ++j) pre[j] += __ldg(tile_hist + (size_t)t * D + tid * P + j);
+        for (int q = 0; q < kSortChunkTiles - 1; ++q) {
+            acc.x += row[q].x; acc.y += row[q].y; acc.z += row[q].z; acc.w += row[q].w;
         }
+        const uint32_t pre[P] = {acc.x, acc.y, acc.z, acc.w};
 #pragma unroll
         for (int j = 0; j < P; ++j) S.out[tid * P + j] = pre[j];
     }
