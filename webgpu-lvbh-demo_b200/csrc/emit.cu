@@ -21,9 +21,9 @@
 //                        prefetches the next block: leaf k's triangle perm[k] arrives by one
 //                        48-byte bulk copy, goes to the output soup at k and is reduced to its
 //                        box (exact-zero components nudged by 1e-8 as bvh-up-pass.js:209-210
-//                        does).  The random gather bounds the pass.  The climb runs in steps: the items still
-//                        climbing after a step are compacted into a queue, so warps stay full
-//                        while the number of items shrinks.  Parking and merging use an
+//                        does).  The random gather bounds the pass.  The climb runs in steps:
+//                        the items still climbing after a step are compacted into a queue, so
+//                        warps stay full while the number of items shrinks.  Parking and merging use an
 //                        arrival mask per split (shared-memory atomics) and parked items in
 //                        shared memory; records go straight to the node buffer, parent links
 //                        are staged and written coalesced.  An item whose parent split lies
