@@ -23,14 +23,14 @@
 //                        box (exact-zero components nudged by 1e-8 as bvh-up-pass.js:209-210
 //                        does).  The random gather bounds the pass.  The climb runs in steps:
 //                        the items still climbing after a step are compacted into a queue, so
-//                        warps stay full while the number of items shrinks.  Parking and merging use an
-//                        arrival mask per split (shared-memory atomics) and parked items in
-//                        shared memory; records go straight to the node buffer, parent links
-//                        are staged and written coalesced.  An item whose parent split lies
-//                        outside the block, or whose sibling never arrives (the parent
-//                        straddles the block boundary), leaves as an "open item" (at most
-//                        2 x 64 per block: they hang off the two boundary paths of a tree at
-//                        most 64 deep).
+//                        warps stay full while the number of items shrinks.  Parking and
+//                        merging use an arrival mask per split (shared-memory atomics) and
+//                        parked items in shared memory; records go straight to the node
+//                        buffer, parent links are staged and written coalesced.  An item
+//                        whose parent split lies outside the block, or whose sibling never
+//                        arrives (the parent straddles the block boundary), leaves as an
+//                        "open item" (at most 2 x 64 per block: they hang off the two boundary
+//                        paths of a tree at most 64 deep).
 //   K3c (k_emit_top)     the nodes that straddle blocks (~3 % of them), built bottom-up from
 //                        the open items with arrival words in global memory (see below).
 #include <type_traits>
@@ -137,8 +137,8 @@ struct ClimbSmem {
 // above).  Leaf t of a block gathers triangle perm[b0 + t]: its index is loaded two blocks
 // ahead, its 48-byte row is copied into shared memory one block ahead (one bulk copy per leaf
 // on the copy engine, completing on the buffer's mbarrier; no registers held meanwhile), then
-// written to the output soup and reduced to the leaf box.  A mesh leaf copies its three 16-byte
-// vertex rows the same way.
+// written to the output soup and reduced to the leaf box.  A mesh leaf's three 16-byte vertex
+// rows (mostly L2 hits) come by cp.async instead.
 template <int LOG, class Segs, class Leaves = SoupLeaves>
 __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_tree_climb(Segs segs,
                                                     const uint32_t *__restrict__ keys_all,
@@ -177,22 +177,24 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         nsp = segs.span(blk);
         const uint32_t *keys = keys_all + nsp.start;
         const int b0 = nsp.b0, n = nsp.n, k = b0 + t;
-        // the phase expects 48 bytes per leaf of the block; thread 0's arrival is its only one
-        if (t == 0) mbar_arrive_tx(&S.bar[buf], 48u * (uint32_t)min(EB, n - b0));
+        // soup: the phase expects 48 bytes per leaf of the block; thread 0's arrival is its only
+        // one.  Mesh: the vertex rows (mostly in L2) come by cp.async.
+        if (!Leaves::kMesh && t == 0) mbar_arrive_tx(&S.bar[buf], 48u * (uint32_t)min(EB, n - b0));
         if (k < n) {
             nk = __ldg(keys + k);
             if constexpr (Leaves::kMesh) {
                 // an index past the vertex buffer was reported by the Morton pass; read row 0
                 const uint32_t nv = lv.nverts;
-                bulk_g2s(&S.tri[buf][t][0], lv.verts + (pa < nv ? pa : 0u), 16u, &S.bar[buf]);
-                bulk_g2s(&S.tri[buf][t][1], lv.verts + (pb < nv ? pb : 0u), 16u, &S.bar[buf]);
-                bulk_g2s(&S.tri[buf][t][2], lv.verts + (pc < nv ? pc : 0u), 16u, &S.bar[buf]);
+                cp_async16(&S.tri[buf][t][0], lv.verts + (pa < nv ? pa : 0u));
+                cp_async16(&S.tri[buf][t][1], lv.verts + (pb < nv ? pb : 0u));
+                cp_async16(&S.tri[buf][t][2], lv.verts + (pc < nv ? pc : 0u));
             } else {
                 uint32_t ti = pa;
                 if (ti >= (uint32_t)n) { bad_perm = true; ti = 0; }
                 bulk_g2s(&S.tri[buf][t][0], lv.tri + 3ull * (nsp.start + ti), 48u, &S.bar[buf]);
             }
         }
+        if constexpr (Leaves::kMesh) cp_async_commit();
         if (t == 0) nk_lo = b0 > 0 ? __ldg(keys + b0 - 1) : 0u;
         if (t == EB - 1) nk_hi = (b0 + EB < n) ? __ldg(keys + b0 + EB) : 0u;
     };
@@ -226,8 +228,12 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         if (t == 0) S.open = 0;
         // this leaf's triangle: to the output soup, and its box (exact-zero components nudged
         // by 1e-8 as bvh-up-pass.js:209-210 does)
-        if (!mbar_wait(&S.bar[buf], (phase >> buf) & 1u)) copy_timeout = true;
-        phase ^= 1u << buf;
+        if constexpr (Leaves::kMesh) {
+            cp_async_wait_all();
+        } else {
+            if (!mbar_wait(&S.bar[buf], (phase >> buf) & 1u)) copy_timeout = true;
+            phase ^= 1u << buf;
+        }
         float4 leaf_lo = make_float4(0.f, 0.f, 0.f, __int_as_float(-(k + 1)));
         float4 leaf_hi0 = make_float4(0.f, 0.f, 0.f, 0.f);
         if (active) {

@@ -100,10 +100,19 @@ __device__ __forceinline__ void st_relaxed_gpu(uint32_t *p, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// 16-byte asynchronous copy global -> shared (L2 only), its group commit and wait.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // Bulk asynchronous copies global -> shared (the TMA engine, no tensor map) completing on an
-// mbarrier in this CTA's shared memory.  A random gather of small rows runs far faster this way
-// than through per-thread 16-byte cp.async: on the B200 a gather of 16.7 M random 48-byte rows
-// into shared memory took 0.66 ms as one 48-byte bulk copy per row, 1.14 ms as three cp.async.
+// mbarrier in this CTA's shared memory.  A random gather of rows from DRAM runs far faster this
+// way than through per-thread 16-byte cp.async: on the B200 a gather of 16.7 M random 48-byte
+// rows into shared memory took 0.66 ms as one 48-byte bulk copy per row, 1.14 ms as three
+// cp.async.  For 16-byte rows that hit L2 cp.async stays ahead (less work per copy).
 // Addresses and sizes are multiples of 16 bytes.  No multicast.
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
