@@ -498,10 +498,11 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
 // K3c, first level (plain builds): one block per group of kGroupBlocks consecutive K3b blocks
 // climbs the group's open items through every split both of whose sides lie in the group, in
 // shared memory - the same park / merge handshake as K3b, splits found through a hash table,
-// rounds separated by block barriers - and writes those records and parent links.  What is
-// left (items whose next split leaves the group, children parked at a split whose sibling
-// never came) replaces the group's items, packed from its first block's slot on, for the
-// global pass (k_emit_top over groups), which so sees about 1 / kGroupBlocks of the items.
+// each item climbing on its own thread with no barrier between levels - and writes those
+// records and parent links.  What is left (items whose next split leaves the group, children
+// parked at a split whose sibling never came) replaces the group's items, packed from its
+// first block's slot on, for the global pass (k_emit_top over groups), which so sees about
+// 1 / kGroupBlocks of the items.
 // A group with more than kGroupCap items packs them all for the global pass unchanged.
 constexpr int kGroupBlocks = 16;
 constexpr int kGroupCap = 256;
@@ -511,13 +512,12 @@ constexpr int kGroupLanes = 64;   // threads per group in the global pass
 
 struct GroupSmem {
     OpenItem it[kGroupCap];
-    int act[2][kGroupCap];
     int out[kGroupCap];
     int hkey[kGroupHash];
     uint32_t hmask[kGroupHash];
     int hidx[kGroupHash][2];
     int bstart[kGroupBlocks + 1];
-    int cnt[2];
+    int cnt[1];
     int nout;
 };
 
@@ -544,7 +544,6 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(int n, OpenItem *it
         if (t <= kGroupBlocks) S.bstart[t] = incl - c;
         if (t == 31) {
             S.cnt[0] = min(incl, kGroupCap);
-            S.cnt[1] = 0;
             S.nout = 0;
         }
     }
@@ -572,27 +571,26 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(int n, OpenItem *it
         for (int k = t; k < c; k += kGroupThreads) {
             const int at = S.bstart[b - blk0] + k;
             S.it[at] = items[(size_t)b * kOpenCap + k];
-            S.act[0][at] = at;
         }
     }
     auto push_out = [&](int i) {
         const int at = atomicAdd(&S.nout, 1);
         S.out[at] = i;  // at most one entry per item: < kGroupCap
     };
-    int cur = 0;
-    for (int round = 0; round < 4 * EB; ++round) {
-        __syncthreads();
-        const int count = S.cnt[cur];
-        if (count == 0) break;
-        for (int a = t; a < count; a += kGroupThreads) {
-            const int i = S.act[cur][a];
-            const OpenItem it = S.it[i];
+    __syncthreads();
+    // Every item climbs on its own thread, with no barrier between levels: S.it[i] holds item
+    // i's current node; at a split the first child parks (its row and index published by the
+    // release of the arrival mask), the second merges both and climbs on with the parent.
+    const int count = S.cnt[0];
+    for (int i = t; i < count; i += kGroupThreads) {
+        OpenItem it = S.it[i];
+        for (int step = 0; step < 4 * EB; ++step) {
             const int l = it.xl, r = it.xr, dl = it.pad0, dr = __float_as_int(it.hi.w);
             const bool is_left = dr > dl;
             const int s = is_left ? r : l - 1;
             if (s < lo_leaf || s + 1 >= hi_leaf || s < 0 || s >= n - 1) {
                 push_out(i);
-                continue;
+                break;
             }
             uint32_t h = ((uint32_t)s * 2654435761u) & (kGroupHash - 1);
             for (int probe = 0; probe < kGroupHash; ++probe) {
@@ -602,7 +600,7 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(int n, OpenItem *it
             }
             const int side = is_left ? 0 : 1;
             S.hidx[h][side] = i;
-            if (atom_or_acq_rel_cta(&S.hmask[h], 1u << side) == 0u) continue;  // first parks
+            if (atom_or_acq_rel_cta(&S.hmask[h], 1u << side) == 0u) break;  // first parks
             const int j = S.hidx[h][side ^ 1];
             const OpenItem sb = S.it[j];
             const int L = is_left ? l : sb.xl, R = is_left ? sb.xr : r;
@@ -619,7 +617,7 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(int n, OpenItem *it
             const int lref = __float_as_int(lc.lo.w), rref = __float_as_int(rc.lo.w);
             parents[lref >= 0 ? lref : n - (lref + 1)] = P;
             parents[rref >= 0 ? rref : n - (rref + 1)] = P;
-            if (root) continue;
+            if (root) break;
             OpenItem pa;
             pa.lo = make_float4(fminf(it.lo.x, sb.lo.x), fminf(it.lo.y, sb.lo.y), fminf(it.lo.z, sb.lo.z),
                                 __int_as_float(P));
@@ -630,12 +628,8 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(int n, OpenItem *it
             pa.pad0 = ndl;
             pa.pad1 = 0;
             S.it[i] = pa;
-            const int at = atomicAdd(&S.cnt[cur ^ 1], 1);
-            S.act[cur ^ 1][at] = i;
+            it = pa;
         }
-        __syncthreads();
-        if (t == 0) S.cnt[cur] = 0;
-        cur ^= 1;
     }
     __syncthreads();
     // a child parked at a split whose sibling never came: its parent leaves the group
