@@ -341,13 +341,23 @@ __global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restr
     const float4 *src = tri + 3ull * first;
     const uint32_t nv = 3u * cnt;
     bool bad = false, coherent = false;
-    for (uint32_t c = warp; c < (cnt + 31) / 32; c += kWarps) {
-        const uint32_t base = 96u * c;
+    const uint32_t rows_n = (cnt + 31) / 32;
+    // a warp's next row of 32 triangles is loaded while it works on this one
+    float4 q[3];
+    auto ld_row = [&](uint32_t cc) {
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
-            const uint32_t e = base + 32 * r + lane;
-            stage[warp][32 * r + lane] = e < nv ? ld_stream(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const uint32_t e = 96u * cc + 32 * r + lane;
+            q[r] = e < nv ? ld_stream(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
+    };
+    if ((uint32_t)warp < rows_n) ld_row(warp);
+    for (uint32_t c = warp; c < rows_n; c += kWarps) {
+        const float4 a0 = q[0], a1 = q[1], a2 = q[2];
+        if (c + kWarps < rows_n) ld_row(c + kWarps);
+        stage[warp][lane] = a0;
+        stage[warp][32 + lane] = a1;
+        stage[warp][64 + lane] = a2;
         __syncwarp();
         const float4 v0 = stage[warp][3 * lane], v1 = stage[warp][3 * lane + 1],
                      v2 = stage[warp][3 * lane + 2];
