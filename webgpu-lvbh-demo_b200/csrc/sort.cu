@@ -141,6 +141,9 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
         const uint32_t idx = wbase + i * 32 + lane;
         k[i] = idx < n ? __ldcs(keys_in + idx) : 0u;
     }
+    // the values are read only when they are staged: start bringing them into L2 now
+    if (vals_in && lane < IPT && wbase + lane * 32 < n)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(vals_in + wbase + lane * 32));
 
     // Stable in-warp ranking, keys visited in input order (item-major, then lane).
     uint32_t rank[IPT / 2];  // two 16-bit ranks per word
