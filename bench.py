@@ -488,8 +488,8 @@ def run_batched(args, world, rank, local, clocks=None):
             "mprims_per_s": world * n / (ms * 1e-3) / 1e6,
             "per_mesh_loop_ms": loop, "per_mesh_builds_per_s": world * count / (base_ms * 1e-3),
             "speedup_vs_per_mesh": base_ms / ms, "identical_trees": bool(identical),
-            "stage_ms": stage_ms, "kernels_per_batch": 8 if tuned["digit_bits"] == 10 else 9,
-            "graph_nodes_per_batch": 11 if tuned["digit_bits"] == 10 else 12,
+            "stage_ms": stage_ms, "kernels_per_batch": 9 if tuned["digit_bits"] == 10 else 10,
+            "graph_nodes_per_batch": 12 if tuned["digit_bits"] == 10 else 13,
             "tunables": {"chosen": {k: tuned[k] for k in ("digit_bits", "tree_block")},
                          "candidates_ms": dict(zip(["10-bit/256", "10-bit/128", "8-bit/256", "8-bit/128"],
                                                    tuned["candidates_ms"]))},

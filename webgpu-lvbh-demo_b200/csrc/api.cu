@@ -84,7 +84,7 @@ constexpr Tunables kCandidates[4] = {{kDigitBits, 8, 0}, {kDigitBits, 7, 0}, {kD
 
 struct BatchKey {
     const void *tri = nullptr;
-    uint32_t total = 0, num_segs = 0, tiles = 0, blocks = 0;
+    uint32_t total = 0, num_segs = 0, tiles = 0, blocks = 0, groups = 0;
     int use_bounds = 0, digit_bits = 0, log_block = 0, tree_ctas = 0;
     void *outs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     bool operator==(const BatchKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
@@ -124,7 +124,7 @@ struct lvbh_ctx {
     uint32_t b_segs = 0, b_tiles = 0, b_blocks = 0;  // capacity
     void *b_dev = nullptr;
     SegRow *b_rows = nullptr;
-    uint32_t *b_tile_seg = nullptr, *b_blk_seg = nullptr;
+    uint32_t *b_tile_seg = nullptr, *b_blk_seg = nullptr, *b_grp_seg = nullptr;
     uint32_t *b_zero = nullptr;  // seg_ord, seg_hist and look-back words, zeroed per build
     size_t b_zero_bytes = 0;
     uint32_t *b_ord = nullptr, *b_hist = nullptr, *b_lookback = nullptr;
@@ -199,6 +199,18 @@ void free_batch(lvbh_ctx *ctx) {
     ctx->b_segs = ctx->b_tiles = ctx->b_blocks = 0;
 }
 
+// Device bytes of the batch scratch for `segs` segments, `tiles` sort tiles and `blocks` tree
+// blocks: segment rows, tile / block / group -> segment maps, bounds, digit counts and
+// look-back words, given bounds, open items, block and group counts.
+size_t batch_bytes(uint32_t segs, uint32_t tiles, uint32_t blocks) {
+    const size_t rows = align_up((segs + 1ull) * sizeof(SegRow));
+    const size_t ord = (size_t)segs * 6 * 4, hist = (size_t)segs * kHistWords * 4;
+    const size_t lb = (size_t)kSortPasses * tiles * kDigits * 4;
+    return rows + align_up(tiles * 4ull) + 2 * align_up(blocks * 4ull) + align_up(ord + hist + lb) +
+           align_up((size_t)segs * 6 * 4) + align_up((size_t)blocks * kOpenCap * sizeof(OpenItem)) +
+           align_up(2 * blocks * 4ull);
+}
+
 // Batch scratch for up to `segs` segments, `tiles` sort tiles and `blocks` tree blocks.
 int ensure_batch(lvbh_ctx *ctx, uint32_t segs, uint32_t tiles, uint32_t blocks) {
     if (ctx->b_dev && segs <= ctx->b_segs && tiles <= ctx->b_tiles && blocks <= ctx->b_blocks)
@@ -213,8 +225,7 @@ int ensure_batch(lvbh_ctx *ctx, uint32_t segs, uint32_t tiles, uint32_t blocks) 
     const size_t lb = (size_t)kSortPasses * tiles * kDigits * 4;
     const size_t zero = align_up(ord + hist + lb);
     const size_t bnd = align_up((size_t)segs * 6 * 4);
-    const size_t dev = rows + align_up(tiles * 4ull) + align_up(blocks * 4ull) + zero + bnd +
-                       align_up((size_t)blocks * kOpenCap * sizeof(OpenItem)) + align_up(blocks * 4ull);
+    const size_t dev = batch_bytes(segs, tiles, blocks);
     void *p = nullptr;
     LVBH_CUDA(ctx, cudaMalloc(&p, dev));
     void *h = nullptr;
@@ -226,6 +237,7 @@ int ensure_batch(lvbh_ctx *ctx, uint32_t segs, uint32_t tiles, uint32_t blocks) 
     ctx->b_rows = reinterpret_cast<SegRow *>(c); c += rows;
     ctx->b_tile_seg = reinterpret_cast<uint32_t *>(c); c += align_up(tiles * 4ull);
     ctx->b_blk_seg = reinterpret_cast<uint32_t *>(c); c += align_up(blocks * 4ull);
+    ctx->b_grp_seg = reinterpret_cast<uint32_t *>(c); c += align_up(blocks * 4ull);  // groups <= blocks
     ctx->b_zero = reinterpret_cast<uint32_t *>(c);
     ctx->b_ord = ctx->b_zero;
     ctx->b_hist = ctx->b_ord + (size_t)segs * 6;
@@ -233,7 +245,7 @@ int ensure_batch(lvbh_ctx *ctx, uint32_t segs, uint32_t tiles, uint32_t blocks) 
     c += zero;
     ctx->b_bounds = reinterpret_cast<float *>(c); c += bnd;
     ctx->b_items = reinterpret_cast<OpenItem *>(c); c += align_up((size_t)blocks * kOpenCap * sizeof(OpenItem));
-    ctx->b_counts = reinterpret_cast<uint32_t *>(c);
+    ctx->b_counts = reinterpret_cast<uint32_t *>(c);  // block counts, then group counts
     char *hc = static_cast<char *>(h);
     ctx->b_host = h;
     ctx->bh_rows = reinterpret_cast<SegRow *>(hc); hc += rows;
@@ -346,7 +358,7 @@ void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool u
     const size_t lb_words = wide ? (size_t)kSortPasses * kDigits : (size_t)kSortPasses32 * kDigits32;
     const uint32_t *zero_end = ctx->b_lookback + lb_words * bp.tiles;
     cudaMemsetAsync(ctx->b_zero, 0, (zero_end - ctx->b_zero) * sizeof(uint32_t), s);
-    launch_seg_tables(ctx->b_rows, bp.num_segs, ctx->b_tile_seg, ctx->b_blk_seg, s);
+    launch_seg_tables(ctx->b_rows, bp.num_segs, ctx->b_tile_seg, ctx->b_blk_seg, ctx->b_grp_seg, s);
     launch_bounds_batch(bp, tri, use_bounds ? ctx->b_bounds : nullptr, ctx->b_ord, s);
     if (profile) cudaEventRecord(ctx->ev[2], s);
     uint32_t *keys_a = ctx->keys_a;
@@ -381,6 +393,7 @@ int launch_batch_graph(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bo
     key.num_segs = bp.num_segs;
     key.tiles = bp.tiles;
     key.blocks = bp.blocks;
+    key.groups = bp.groups;  // the straddling pass's grid
     key.use_bounds = use_bounds;
     key.digit_bits = bp.digit_bits;
     key.log_block = bp.log_block;
@@ -546,13 +559,7 @@ size_t ctx_device_bytes(const lvbh_ctx *ctx) {
     if (!ctx || !ctx->arena) return 0;
     const uint32_t segs = ctx->b_segs, tiles = ctx->b_tiles, blocks = ctx->b_blocks;
     size_t batch = 0;
-    if (ctx->b_dev) {
-        batch = align_up((segs + 1ull) * sizeof(SegRow)) + align_up(tiles * 4ull) + align_up(blocks * 4ull) +
-                align_up((size_t)segs * 6 * 4 + (size_t)segs * kHistWords * 4 +
-                         (size_t)kSortPasses * tiles * kDigits * 4) +
-                align_up((size_t)segs * 6 * 4) + align_up((size_t)blocks * kOpenCap * sizeof(OpenItem)) +
-                align_up(blocks * 4ull);
-    }
+    if (ctx->b_dev) batch = batch_bytes(segs, tiles, blocks);
     return arena_bytes(ctx->cap) + batch + ctx->stage_bytes;
 }
 
@@ -761,20 +768,22 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
     if (int rc = ensure_batch(ctx, num_segs, (uint32_t)tiles, (uint32_t)blocks128)) return rc;
     if (ctx->pending) lvbh_sync(ctx);  // the pinned mirror may still be read by the previous build
     if (seg_bounds) std::memcpy(ctx->bh_bounds, seg_bounds, num_segs * 6ull * sizeof(float));
-    // segment table for tree blocks of 2^log_block leaves: first triangle, first sort tile and
-    // first tree block per segment
+    // segment table for tree blocks of 2^log_block leaves: first triangle, first sort tile,
+    // first tree block and first straddling-pass group (16 blocks of one segment) per segment
     auto plan = [&](const Tunables &t) {
-        uint32_t tile = 0, blk = 0;
+        uint32_t tile = 0, blk = 0, grp = 0;
         for (uint32_t i = 0; i <= num_segs; ++i) {
-            ctx->bh_rows[i] = SegRow{seg_offsets[i], tile, blk, 0u};
+            ctx->bh_rows[i] = SegRow{seg_offsets[i], tile, blk, grp};
             if (i < num_segs) {
                 const uint32_t n = seg_offsets[i + 1] - seg_offsets[i];
+                const uint32_t b = (uint32_t)emit_groups(n, t.log_block);
                 tile += sort_tiles(n);
-                blk += (uint32_t)emit_groups(n, t.log_block);
+                blk += b;
+                grp += straddle_groups(b);
             }
         }
-        return BatchPlan{ctx->b_rows, ctx->b_tile_seg, ctx->b_blk_seg, num_segs, (uint32_t)tiles,
-                         blk, total, t.digit_bits, t.log_block, t.tree_ctas};
+        return BatchPlan{ctx->b_rows, ctx->b_tile_seg, ctx->b_blk_seg, ctx->b_grp_seg, num_segs,
+                         (uint32_t)tiles, blk, total, grp, t.digit_bits, t.log_block, t.tree_ctas};
     };
     LVBH_CUDA(ctx, cudaMemsetAsync(&ctx->ctl->aux_err, 0, sizeof(uint32_t), s));
     const float4 *tri = reinterpret_cast<const float4 *>(tri_array);

@@ -79,6 +79,7 @@ struct OneSeg {
     int n;
     __device__ __forceinline__ int blocks() const { return (n + EB - 1) / EB; }
     __device__ __forceinline__ Span span(int blk) const { return Span{0, n, blk * EB}; }
+    __device__ __forceinline__ size_t item_base(int blk, int cap) const { return (size_t)blk * cap; }
 };
 
 template <int LOG>
@@ -94,6 +95,7 @@ struct ManySegs {
         const int first = (int)__ldg(&rows[sg].blk);
         return Span{t0, (int)(t1 - t0), (blk - first) * EB};
     }
+    __device__ __forceinline__ size_t item_base(int blk, int cap) const { return (size_t)blk * cap; }
 };
 
 // K3b shared memory.  A climbing item is two float4: box min + link (node index, or
@@ -438,7 +440,7 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
     float4 *pend = pend_all + 2ull * sp.start;
     uint8_t *pend_d = pend_d_all + sp.start;
     for (int q = lane; q < cnt; q += LANES) {
-        const OpenItem it = items[(size_t)gw * cap + q];
+        const OpenItem it = items[segs.item_base(gw, cap) + q];
         int l = it.xl, r = it.xr, ref = __float_as_int(it.lo.w);
         float nx = it.lo.x, ny = it.lo.y, nz = it.lo.z, xx = it.hi.x, xy = it.hi.y, xz = it.hi.z;
         int dl = it.pad0, dr = __float_as_int(it.hi.w);
@@ -521,17 +523,48 @@ struct GroupSmem {
     int nout;
 };
 
+// Where group g lies: its segment (first triangle, size), its tree blocks [blk0, blk1) as
+// global block numbers and its first leaf within the segment.  A group never crosses a segment.
+struct GroupSpan {
+    size_t start;
+    int n, blk0, blk1, leaf0;
+};
 template <int LOG>
-__global__ void __launch_bounds__(kGroupThreads) k_top_group(int n, OpenItem *items, const uint32_t *__restrict__ counts,
-                                                   uint32_t *__restrict__ group_counts, float4 *nodes,
-                                                   int32_t *parents, Control *ctl) {
+struct OneSegGroups {  // plain build: blocks 16 g .. 16 g + 15 of the one segment
+    int n;
+    __device__ __forceinline__ GroupSpan group(int g) const {
+        const int nblk = (n + (1 << LOG) - 1) >> LOG, b0 = g * kGroupBlocks;
+        return GroupSpan{0, n, b0, min(nblk, b0 + kGroupBlocks), b0 << LOG};
+    }
+};
+template <int LOG>
+struct ManySegGroups {  // batched build: a segment's blocks in groups of 16, from its first group
+    const SegRow *rows;
+    const uint32_t *grp_seg;
+    __device__ __forceinline__ GroupSpan group(int g) const {
+        const uint32_t sg = __ldg(grp_seg + g);
+        const uint32_t t0 = __ldg(&rows[sg].tri), t1 = __ldg(&rows[sg + 1].tri);
+        const int first = (int)__ldg(&rows[sg].blk), end = (int)__ldg(&rows[sg + 1].blk);
+        const int b0 = first + (g - (int)__ldg(&rows[sg].grp)) * kGroupBlocks;
+        return GroupSpan{t0, (int)(t1 - t0), b0, min(end, b0 + kGroupBlocks), (b0 - first) << LOG};
+    }
+};
+
+template <int LOG, class Groups>
+__global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, OpenItem *items,
+                                                   const uint32_t *__restrict__ counts,
+                                                   uint32_t *__restrict__ group_counts, float4 *nodes_all,
+                                                   int32_t *parents_all, Control *ctl) {
     constexpr int EB = 1 << LOG;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupSmem &S = *reinterpret_cast<GroupSmem *>(smem_raw);
     const int t = threadIdx.x;
-    const int nblk = (n + EB - 1) / EB;
-    const int g = blockIdx.x, blk0 = g * kGroupBlocks, blk1 = min(nblk, blk0 + kGroupBlocks);
-    const int lo_leaf = blk0 * EB, hi_leaf = min(n, blk1 * EB);
+    const int g = blockIdx.x;
+    const GroupSpan gs = groups.group(g);
+    const int n = gs.n, blk0 = gs.blk0, blk1 = gs.blk1;
+    const int lo_leaf = gs.leaf0, hi_leaf = min(n, gs.leaf0 + (blk1 - blk0) * EB);
+    float4 *nodes = nodes_all + 4ull * gs.start;
+    int32_t *parents = parents_all + 2ull * gs.start;
     OpenItem *gitems = items + (size_t)blk0 * kOpenCap;
     if (t < 32) {  // the blocks' item counts and their exclusive prefix (one warp)
         const int c = (t < kGroupBlocks && blk0 + t < blk1) ? (int)min(counts[blk0 + t], (uint32_t)kOpenCap) : 0;
@@ -652,6 +685,18 @@ struct GroupSegs {
         return (tree_blocks + kGroupBlocks - 1) / kGroupBlocks;
     }
     __device__ __forceinline__ Span span(int g) const { return Span{0, n, g * kGroupBlocks * (1 << LOG)}; }
+    __device__ __forceinline__ size_t item_base(int g, int cap) const { return (size_t)g * cap; }
+};
+template <int LOG>
+struct ManyGroupSegs {  // the batched build's groups (ManySegGroups), counted in ngroups
+    ManySegGroups<LOG> gr;
+    int ngroups;
+    __device__ __forceinline__ int blocks() const { return ngroups; }
+    __device__ __forceinline__ Span span(int g) const {
+        const GroupSpan q = gr.group(g);
+        return Span{q.start, q.n, q.leaf0};
+    }
+    __device__ __forceinline__ size_t item_base(int g, int) const { return (size_t)gr.group(g).blk0 * kOpenCap; }
 };
 
 template <int LOG>
@@ -661,7 +706,8 @@ template <int LOG, class Segs, class Leaves>
 void launch_emit_impl(Segs segs, int groups, Leaves lv, const uint32_t *keys, float4 *nodes, int32_t *parents,
                       OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
                       uint8_t *pend_d, const uint32_t *epoch, Control *ctl, bool top,
-                      cudaStream_t s, cudaEvent_t *ev, int ctas_per_sm) {
+                      cudaStream_t s, cudaEvent_t *ev, int ctas_per_sm,
+                      const uint32_t *grp_seg = nullptr, int ngroups = 0) {
     if (ev) cudaEventRecord(ev[0], s);  // the leaf gather runs inside the tree pass
     const int per_sm = ctas_per_sm > 0 && ctas_per_sm < TreeGeo<LOG>::kCtasPerSm ? ctas_per_sm
                                                                                 : TreeGeo<LOG>::kCtasPerSm;
@@ -673,12 +719,23 @@ void launch_emit_impl(Segs segs, int groups, Leaves lv, const uint32_t *keys, fl
         if constexpr (std::is_same<Segs, OneSeg<LOG>>::value) {
             const int ngroups = (groups + kGroupBlocks - 1) / kGroupBlocks;
             uint32_t *gcounts = counts + groups;  // the counts buffer holds 2 x groups words
-            k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(segs.n, items, counts, gcounts, nodes,
-                                                                   parents, ctl);
+            k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(OneSegGroups<LOG>{segs.n}, items,
+                                                                   counts, gcounts, nodes, parents, ctl);
             // a group leaves a few dozen items: one lane each
             k_emit_top<GroupSegs<LOG>, kGroupLanes><<<(ngroups * kGroupLanes + 255) / 256, 256, 0, s>>>(
                 GroupSegs<LOG>{segs.n}, items, kGroupBlocks * kOpenCap, gcounts, nodes, parents, arrive, pend,
                 pend_d, epoch, ctl);
+        } else if (grp_seg) {
+            // batched: the same two levels over groups of 16 blocks that never cross a mesh
+            uint32_t *gcounts = counts + groups;  // the counts buffer holds 2 x blocks words
+            const ManySegGroups<LOG> gr{segs.rows, grp_seg};
+            if (ngroups > 0) {
+                k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(gr, items, counts, gcounts,
+                                                                                   nodes, parents, ctl);
+                k_emit_top<ManyGroupSegs<LOG>, kGroupLanes><<<(ngroups * kGroupLanes + 255) / 256, 256, 0, s>>>(
+                    ManyGroupSegs<LOG>{gr, ngroups}, items, kGroupBlocks * kOpenCap, gcounts, nodes, parents,
+                    arrive, pend, pend_d, epoch, ctl);
+            }
         } else {
             k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, kOpenCap, counts, nodes,
                                                                          parents, arrive, pend, pend_d,
@@ -706,7 +763,13 @@ cudaError_t emit_init() {
     if (e == cudaSuccess) e = prefer_shared(k_tree_climb<7, ManySegs<7>>, leaves_smem_bytes<7>());
     if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, OneSeg<8>, MeshLeaves>, leaves_smem_bytes<8>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_top_group<kLogEmitBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(k_top_group<kLogEmitBlock, OneSegGroups<kLogEmitBlock>>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_top_group<8, ManySegGroups<8>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(GroupSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_top_group<7, ManySegGroups<7>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(GroupSmem));
     return e;
 }
@@ -742,11 +805,11 @@ void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *p
     if (bp.log_block == 7)
         launch_emit_impl<7>(ManySegs<7>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks,
                             SoupLeaves{tri, perm, otri}, keys, nodes, parents, items, counts, arrive, pend,
-                            pend_d, epoch, ctl, true, s, ev, bp.tree_ctas_per_sm);
+                            pend_d, epoch, ctl, true, s, ev, bp.tree_ctas_per_sm, bp.grp_seg, (int)bp.groups);
     else
         launch_emit_impl<8>(ManySegs<8>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks,
                             SoupLeaves{tri, perm, otri}, keys, nodes, parents, items, counts, arrive, pend,
-                            pend_d, epoch, ctl, true, s, ev, bp.tree_ctas_per_sm);
+                            pend_d, epoch, ctl, true, s, ev, bp.tree_ctas_per_sm, bp.grp_seg, (int)bp.groups);
 }
 
 }  // namespace lvbh

@@ -89,14 +89,15 @@ struct HostBounds {
 // the totals.  Sort tiles (kSortTile keys) and tree blocks (kEmitBlock leaves) never cross a
 // segment boundary, so each tile or block works on one segment with segment-local indices.
 struct __align__(16) SegRow {
-    uint32_t tri, tile, blk, pad;
+    uint32_t tri, tile, blk, grp;  // first triangle, sort tile, tree block, straddling group
 };
 
 struct BatchPlan {
     const SegRow *rows;        // num_segs + 1 rows (device)
     const uint32_t *tile_seg;  // segment of each sort tile (device, `tiles` entries)
     const uint32_t *blk_seg;   // segment of each tree block (device, `blocks` entries)
-    uint32_t num_segs, tiles, blocks, total;
+    const uint32_t *grp_seg;   // segment of each straddling-pass group (device, `groups` entries)
+    uint32_t num_segs, tiles, blocks, total, groups;
     int digit_bits;            // sort digit width: 10 (three passes) or 8 (four passes)
     int log_block;             // tree blocks of 2^log_block leaves: 8 or 7
     int tree_ctas_per_sm;      // persistent tree grid: CTAs per SM (0 = the most that fit)
@@ -135,6 +136,8 @@ cudaError_t sort_init();  // once per device, before the first launch
 // and counts (emit_groups(n)), arrive (n words, zero or older epochs), pend (2n float4),
 // pend_d (n bytes); *epoch is this build's epoch (advanced by K1b).
 size_t emit_groups(uint32_t n, int log_eb = kLogEmitBlock);
+// Groups of the straddling pass's first level over `blocks` tree blocks of one segment.
+inline uint32_t straddle_groups(uint32_t blocks) { return (blocks + 15u) / 16u; }
 cudaError_t emit_init();  // once per device, before the first launch
 // ev (may be nullptr): three events, recorded before K3b, after K3b and after K3c.
 void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
@@ -147,7 +150,7 @@ void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, 
 // holds 6 floats per segment that replace the device reduction for every segment whose first
 // value is not NaN.  K2's look-back words: bp.tiles * 256 per pass, zeroed before the build.
 void launch_seg_tables(const SegRow *rows, uint32_t num_segs, uint32_t *tile_seg,
-                       uint32_t *blk_seg, cudaStream_t s);
+                       uint32_t *blk_seg, uint32_t *grp_seg, cudaStream_t s);
 void launch_bounds_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,
                          uint32_t *seg_ord, cudaStream_t s);
 // seg_hist: kHistWords per segment, pass-major (bp.digit_bits wide digits).
@@ -158,7 +161,8 @@ void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const u
                            uint32_t *keys_out, uint32_t *vals_out, int pass,
                            const uint32_t *seg_hist, Control *ctl, uint32_t *lookback,
                            cudaStream_t s);
-// items / counts: bp.blocks * kOpenCap / bp.blocks entries.
+// items / counts: bp.blocks * kOpenCap / 2 * bp.blocks entries (block counts, then group
+// counts of the straddling pass's first level).
 void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
                        const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
                        OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,

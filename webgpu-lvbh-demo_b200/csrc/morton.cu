@@ -394,12 +394,14 @@ __global__ void __launch_bounds__(kThreads) k_morton_batch(const float4 *__restr
 // Segment of every sort tile and tree block: one warp per segment fills its entries.
 __global__ void __launch_bounds__(256) k_seg_tables(const SegRow *__restrict__ rows, uint32_t num_segs,
                                                     uint32_t *__restrict__ tile_seg,
-                                                    uint32_t *__restrict__ blk_seg) {
+                                                    uint32_t *__restrict__ blk_seg,
+                                                    uint32_t *__restrict__ grp_seg) {
     const uint32_t sg = (blockIdx.x * 256u + threadIdx.x) / 32u, lane = threadIdx.x & 31;
     if (sg >= num_segs) return;
     const SegRow a = rows[sg], b = rows[sg + 1];
     for (uint32_t t = a.tile + lane; t < b.tile; t += 32) tile_seg[t] = sg;
     for (uint32_t t = a.blk + lane; t < b.blk; t += 32) blk_seg[t] = sg;
+    for (uint32_t t = a.grp + lane; t < b.grp; t += 32) grp_seg[t] = sg;
 }
 
 __global__ void k_gather_indexed(const float *__restrict__ xyz, uint32_t num_verts,
@@ -466,9 +468,9 @@ void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t 
 }
 
 void launch_seg_tables(const SegRow *rows, uint32_t num_segs, uint32_t *tile_seg,
-                       uint32_t *blk_seg, cudaStream_t s) {
+                       uint32_t *blk_seg, uint32_t *grp_seg, cudaStream_t s) {
     if (num_segs == 0) return;
-    k_seg_tables<<<(num_segs + 7) / 8, 256, 0, s>>>(rows, num_segs, tile_seg, blk_seg);
+    k_seg_tables<<<(num_segs + 7) / 8, 256, 0, s>>>(rows, num_segs, tile_seg, blk_seg, grp_seg);
 }
 
 void launch_bounds_batch(const BatchPlan &bp, const float4 *tri, const float *host_bounds,
