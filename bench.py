@@ -75,8 +75,33 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def load_scenes():
+    """lvbh/scenes.py (pure numpy) loaded by its path, so that the reference arm does not import
+    the lvbh package, whose __init__ loads the CUDA library."""
+    import importlib.util
+    mod = sys.modules.get("lvbh_scenes_standalone")
+    if mod is None:
+        spec = importlib.util.spec_from_file_location("lvbh_scenes_standalone",
+                                                      os.path.join(PKG, "lvbh", "scenes.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[spec.name] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def make_workload(name: str):
-    from lvbh import scenes
+    scenes = load_scenes()
     if name == "clustered16M":
         return scenes.clustered_soup(1 << 24, seed=2), "clustered_soup_16M"
     if name == "clustered4M":  # the same distribution at 2^22 triangles (profiling captures)
@@ -203,26 +228,52 @@ def cpu_baseline(tri, bounds=None):
     oracle.build(tri, bounds, threads=cores)
     dt = time.perf_counter() - t0
     return {"value": tri.shape[0] / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": f"one full build of the {tri.shape[0]:,}-triangle workload "
                       f"({dt:.2f} s wall, OpenMP over {cores} threads)"}
 
 
+def cpu_baseline_table(big=None, big_all_cores_s=None):
+    """The CPU restatement on one thread and on all host cores for the three plain-build
+    workloads (65,536 uniform, the 2,097,152-triangle sphere, the 16,777,216-triangle clustered
+    scene): one build each, Mprims/s.  `big`: the clustered soup when already generated,
+    `big_all_cores_s`: its all-core time when already measured."""
+    import oracle
+    scenes = load_scenes()
+    cores = os.cpu_count() or 1
+    rows = []
+    for wname, gen in (("uniform_soup_64K", lambda: scenes.uniform_soup(65_536, seed=0)),
+                       ("sphere_mesh_2M", lambda: scenes.sphere_mesh(1024, seed=1)),
+                       ("clustered_soup_16M", lambda: big if big is not None else scenes.clustered_soup(1 << 24, seed=2))):
+        tri = gen()
+        for threads in (1, cores):
+            if wname == "clustered_soup_16M" and threads == cores and big_all_cores_s:
+                dt = big_all_cores_s
+            else:
+                t0 = time.perf_counter()
+                oracle.build(tri, None, threads=threads)
+                dt = time.perf_counter() - t0
+            rows.append({"workload": wname, "num_tris": int(tri.shape[0]), "threads": threads,
+                         "s": round(dt, 4), "mprims_per_s": tri.shape[0] / dt / 1e6})
+    return {"cpu_model": cpu_model(), "cores": cores, "kind": "port", "rows": rows}
+
+
 def run_reference(args, world, rank):
-    """--impl reference: the CPU restatement of the reference's build, each step a bounded
-    sample (the first 2^22 triangles) of the workload, all host threads."""
+    """--impl reference: the CPU restatement of the reference's build (the oracle) on all host
+    threads, each step one full build of the workload.  The scene generator is loaded without
+    the lvbh package, so no CUDA library of this project is loaded by this arm."""
     if rank != 0:
         return
     import oracle
     tri, wname = make_workload(args.workload)
-    sample = tri[: min(tri.shape[0], 1 << 22)]
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
-        oracle.build(sample, None, threads=cores)
+        oracle.build(tri, None, threads=cores)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        oracle.build(sample, None, threads=cores)
+        oracle.build(tri, None, threads=cores)
     dt = (time.perf_counter() - t0) / args.steps
-    v = sample.shape[0] / dt / 1e6
+    v = tri.shape[0] / dt / 1e6
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32/u32", "data": "synthetic",
@@ -230,7 +281,8 @@ def run_reference(args, world, rank):
             "config": {"workload": wname, "num_tris": int(tri.shape[0]), "parallelism": "replicas",
                        "bounds": "reduced over all vertices"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"first {sample.shape[0]:,} triangles of the workload per step"},
+                             "cpu_model": cpu_model(),
+                             "sample": f"one full build of the {tri.shape[0]:,}-triangle workload per step"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference's WGSL build needs browser WebGPU (unavailable on this box); "
                     "this arm times its C++ restatement, which produces the same output"}
@@ -338,6 +390,8 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(tri)
+        if not args.no_cpu_table:
+            cpu["table"] = cpu_baseline_table(big=tri, big_all_cores_s=n / (cpu["value"] * 1e6))
 
     builder.close()
     del dtri, outs, htri
@@ -373,7 +427,35 @@ def run_ours(args, world, rank, local):
             "roofline": roofline, "stage_ms": stage_ms, "cpu_baseline": cpu, "e2e": e2e_line,
             "clocks": clock_summary, "batched": batched, "served": served, "trace": trace, "obj": obj,
             "pt": pt, "mesh": mesh}
+    line["summary"] = summarize(line)  # last, so that a tail of the output still holds it
     print(json.dumps(line), flush=True)
+
+
+def summarize(line):
+    """The headline figures of every part, compact, for the end of the JSON line."""
+    r = lambda x, d=3: None if x is None else round(float(x), d)  # noqa: E731
+    out = {"build_ms": r(line["ms_per_step"], 4), "stage_ms": {k: r(v, 4) for k, v in line["stage_ms"].items()},
+           "roofline_frac": r(line["roofline"]["frac"]),
+           "whole_build_frac": r(line["roofline"]["whole_build"]["frac_of_measured"]),
+           "e2e_mprims_per_s": r(line["e2e"]["value"], 1)}
+    b = line.get("batched")
+    if b:
+        out["batched"] = {"ms_per_batch": r(b["ms_per_batch"]), "builds_per_s": r(b["builds_per_s"], 0),
+                          "speedup_vs_per_mesh": r(b["speedup_vs_per_mesh"], 2),
+                          "identical_trees": b["identical_trees"], "num_tris": b["num_tris"]}
+    sv = line.get("served")
+    if sv:
+        out["served"] = [{"rate": x["rate"], "requests": x["requests"],
+                          "p50_p99_p999_ms": [r(x["latency_ms"][k]) for k in ("p50", "p99", "p999")],
+                          "mean_batch_reqs": r(x["mean_batch_reqs"], 2), "builds_per_s": r(x["builds_per_s"], 1),
+                          "plain_p50_p99_ms": [r(x["plain"]["latency_ms"][k]) for k in ("p50", "p99")]}
+                         for x in sv["rates"]]
+    for k, f in (("trace", "mrays_per_s"), ("pt", "mpix_bounces_per_s"), ("obj", "parse_ms")):
+        if line.get(k):
+            out[k + "_" + f] = r(line[k][f], 1 if f != "parse_ms" else 4)
+    if line.get("mesh"):
+        out["mesh_build_ms"] = r(line["mesh"]["build_mesh_ms"], 4)
+    return out
 
 
 def run_batched(args, world, rank, local, clocks=None):
@@ -906,6 +988,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="clustered16M")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-table", action="store_true")
     ap.add_argument("--batch-meshes", type=int, default=4096)
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")

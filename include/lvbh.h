@@ -203,7 +203,9 @@ LVBH_API int  lvbh_get_tunables(lvbh_ctx *ctx, lvbh_tunables *t, float *candidat
 
 /* Waits for the context's last build and returns its device-side status (LVBH_OK,
  * LVBH_EINVAL for non-finite vertices, LVBH_ETIMEOUT, LVBH_EDEVICE).  Fills out->bounds
- * of the result passed to that build when it is still reachable. */
+ * of the result passed to that build when it is still reachable.  Every build entry point
+ * first finishes the context's pending LVBH_ASYNC build this way; when that build failed, the
+ * entry point returns its status (lvbh_last_error says so) and starts no new build. */
 LVBH_API int  lvbh_sync(lvbh_ctx *ctx);
 
 /* Frees library-allocated result buffers (no-op for LVBH_OUT_CALLER results). */
@@ -299,7 +301,8 @@ LVBH_API const char *lvbh_server_last_error(const lvbh_server *srv);
  * stall (cudaMalloc / cudaFree synchronise the device), a process whose whole memory budget is
  * already reserved by its own pool, or a plugin host that owns every device allocation.
  *   keys_in   num_keys uint32 keys, device memory (not modified)
- *   keys_out  num_keys sorted keys; perm_out num_keys input indices (ties keep input order)
+ *   keys_out  num_keys sorted keys (may be keys_in itself: in place); perm_out num_keys input
+ *             indices (ties keep input order)
  *   stream    cudaStream_t or NULL; the call returns once the sort has finished
  * All other memory (ping-pong keys and values, histograms, look-back words, error word) is one
  * file-scope device array inside the library, sized for LVBH_NOALLOC_MAX_KEYS keys (about
@@ -308,7 +311,9 @@ LVBH_API const char *lvbh_server_last_error(const lvbh_server *srv);
  * array's device address (cudaGetSymbolAddress, with the device current); make it before any
  * stream capture.  Calls share the array: two calls that overlap on the GPU (unordered
  * streams, or threads) race.  Calls no cudaMalloc, cudaFree or allocating routine.
- * Returns LVBH_OK, LVBH_ERANGE, LVBH_EINVAL (NULL pointer), LVBH_ETIMEOUT or LVBH_ECUDA. */
+ * Returns LVBH_OK, LVBH_ERANGE, LVBH_EINVAL (NULL pointer), LVBH_ETIMEOUT (a look-back wait
+ * gave up), LVBH_EDEVICE (any other device-side error, e.g. a scatter target out of range when
+ * calls overlap; the outputs are then incomplete) or LVBH_ECUDA. */
 #define LVBH_NOALLOC_MAX_KEYS ((uint32_t)1 << 20)
 LVBH_API int  lvbh_sort_pairs_noalloc(const uint32_t *keys_in, uint32_t num_keys,
                                       uint32_t *keys_out, uint32_t *perm_out, void *stream);

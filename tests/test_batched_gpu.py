@@ -174,3 +174,50 @@ def test_autotune_times_candidates_and_caches(builder):
     for f in FIELDS:
         assert torch.equal(getattr(r1, f), getattr(r2, f)), f
     check_against_plain(builder, tri, offs, r2)
+
+
+def test_async_batched_then_larger_batch_keeps_first_status_and_bounds():
+    """An LVBH_ASYNC batched build followed, without lvbh_sync, by a larger batched build on the
+    same context (through the C ABI: the Python wrapper syncs in between by itself).  The second
+    call grows the batch scratch and its pinned mirror; it must first finish the pending build,
+    so that the first build's per-mesh bounds reach its bounds_out intact."""
+    import ctypes
+
+    import torch
+    import lvbh
+    import oracle
+    from lvbh import _native
+    L = _native.lib
+    b = lvbh.BVHBuilder(0)
+    try:
+        calls = []
+        for sizes, seed in (([300, 5000, 17, 4096], 61), ([900, 70_001, 3, 12_289, 40_000, 8, 4097, 256], 62)):
+            tri, offs = make_batch(sizes, seed=seed)
+            n, m = int(offs[-1]), len(sizes)
+            dtri = torch.from_numpy(tri).cuda()
+            outs = lvbh.empty_outputs(n, dtri.device)
+            r = lvbh._result_struct(outs, n)
+            offs32 = offs.astype(np.uint32)
+            bout = np.full((m, 6), np.nan, np.float32)
+            rc = L.lvbh_build_batched(b.ctx, ctypes.c_void_p(dtri.data_ptr()),
+                                      offs32.ctypes.data_as(ctypes.c_void_p), m, None,
+                                      bout.ctypes.data_as(ctypes.c_void_p),
+                                      _native.OUT_CALLER | _native.ASYNC, ctypes.byref(r), None)
+            assert rc == _native.OK, L.lvbh_last_error(b.ctx)
+            calls.append((tri, offs, bout, outs, dtri, r, offs32))
+        assert L.lvbh_sync(b.ctx) == _native.OK
+        for tri, offs, bout, outs, *_ in calls:
+            for i in range(len(offs) - 1):
+                t = tri[offs[i]:offs[i + 1]]
+                np.testing.assert_array_equal(bout[i].view(np.uint32), oracle.scene_bounds(t).view(np.uint32),
+                                              err_msg=f"mesh {i} bounds_out")
+                ref = oracle.build(t, None, threads=0)
+                a, c = int(offs[i]), int(offs[i + 1])
+                got = {"nodes": outs["nodes"][a:c].cpu().numpy().view(np.uint32),
+                       "tris": outs["tris"][a:c].cpu().numpy(),
+                       "parents": outs["parents"][2 * a:2 * c].cpu().numpy(),
+                       "leaf_index": outs["leaf_index"][a:c].cpu().numpy().view(np.uint32),
+                       "morton": outs["morton"][a:c].cpu().numpy().view(np.uint32)}
+                assert_same(got, ref, f"mesh {i}")
+    finally:
+        b.close()

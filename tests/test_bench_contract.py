@@ -48,3 +48,28 @@ def test_launches_per_build_match_the_launch_list():
     for stage, (name, launches) in bench.KERNELS.items():
         if name is not None:
             assert per_kernel[name] == (1 if stage == "top" else launches), (stage, name)
+
+
+def test_reference_arm_loads_no_project_cuda_library():
+    """bench.py --impl reference runs the oracle only: in a fresh process, after a run of the
+    arm on the 65,536-triangle workload, neither the lvbh package nor liblvbh.so is loaded,
+    and the line names the full workload it timed."""
+    import json
+    import subprocess
+    import sys
+    code = (
+        "import io, json, sys, contextlib\n"
+        "sys.path.insert(0, %r)\n"
+        "import bench\n"
+        "class A: workload, warmup, steps = 'uniform64K', 1, 1\n"
+        "buf = io.StringIO()\n"
+        "with contextlib.redirect_stdout(buf): bench.run_reference(A, 1, 0)\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'line': json.loads(buf.getvalue()), 'lvbh_loaded': 'liblvbh.so' in maps,\n"
+        "                  'lvbh_imported': 'lvbh' in sys.modules}))\n" % REPO)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, check=True)
+    r = json.loads(out.stdout.strip().splitlines()[-1])
+    assert not r["lvbh_loaded"] and not r["lvbh_imported"]
+    line = r["line"]
+    assert line["impl"] == "reference" and line["config"]["num_tris"] == 65_536
+    assert "one full build" in line["cpu_baseline"]["sample"]

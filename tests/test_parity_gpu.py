@@ -139,6 +139,45 @@ def test_nonfinite_rejected(builder):
     build_np(builder, tri)
 
 
+def test_failed_async_build_status_reaches_next_build():
+    """A failing LVBH_ASYNC build (non-finite vertex) followed by a second build without
+    lvbh_sync: the second call returns the first one's status and starts nothing; the call
+    after that builds normally."""
+    import ctypes
+
+    import torch
+    import lvbh
+    import oracle
+    from lvbh import _native, scenes
+    L = _native.lib
+    b = lvbh.BVHBuilder(0)
+    try:
+        bad = scenes.uniform_soup(5000, seed=4)
+        bad[77, 9] = np.nan
+        good = scenes.uniform_soup(7000, seed=5)
+        keep = []
+
+        def call(tri, flags):
+            t = torch.from_numpy(tri).cuda()
+            outs = lvbh.empty_outputs(tri.shape[0], t.device)
+            r = lvbh._result_struct(outs, tri.shape[0])
+            keep.append((t, outs, r))
+            return L.lvbh_build_soup(b.ctx, ctypes.c_void_p(t.data_ptr()), tri.shape[0], None,
+                                     _native.OUT_CALLER | flags, ctypes.byref(r), None), outs
+
+        rc, _ = call(bad, _native.ASYNC)
+        assert rc == _native.OK
+        rc, _ = call(good, 0)
+        assert rc == _native.EINVAL
+        assert b"earlier LVBH_ASYNC build failed" in L.lvbh_last_error(b.ctx)
+        assert L.lvbh_sync(b.ctx) == _native.OK  # nothing pending any more
+        rc, outs = call(good, 0)
+        assert rc == _native.OK
+        assert_same({k: v.cpu().numpy() for k, v in outs.items()}, oracle.build(good, None, threads=0), "after")
+    finally:
+        b.close()
+
+
 def test_indexed_bad_index_rejected(builder):
     import torch
     import lvbh

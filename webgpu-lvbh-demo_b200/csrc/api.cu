@@ -543,6 +543,16 @@ int check_out(lvbh_ctx *ctx, uint32_t n, uint32_t flags, lvbh_result *out, size_
     return alloc_outputs(ctx, n, out, tri_row);
 }
 
+// A build entry first completes the context's pending LVBH_ASYNC build, before it touches
+// any buffer that build may still use (arena, staging copy, pinned mirrors).  When the pending
+// build failed, its status is returned and no new build starts, so the status is not lost.
+int finish_pending(lvbh_ctx *ctx) {
+    if (!ctx->pending) return LVBH_OK;
+    const int rc = lvbh_sync(ctx);
+    if (rc != LVBH_OK) ctx->err = "an earlier LVBH_ASYNC build failed: " + ctx->err;
+    return rc;
+}
+
 }  // namespace
 
 namespace lvbh {
@@ -620,6 +630,7 @@ int lvbh_build_soup(lvbh_ctx *ctx, const float *tri_array, uint32_t num_tris,
     if (num_tris > LVBH_MAX_TRIS) return fail(ctx, LVBH_EINVAL, "num_tris exceeds LVBH_MAX_TRIS");
     if (num_tris && !tri_array) return fail(ctx, LVBH_EINVAL, "tri_array is NULL");
     DeviceGuard g(ctx->device);
+    if (int rc = finish_pending(ctx)) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (int rc = check_out(ctx, num_tris, flags, out)) return rc;
     out->num_tris = out->num_nodes = num_tris;
@@ -649,6 +660,7 @@ int lvbh_build_indexed(lvbh_ctx *ctx, const float *xyz, uint32_t num_verts, cons
     if (num_tris > LVBH_MAX_TRIS) return fail(ctx, LVBH_EINVAL, "num_tris exceeds LVBH_MAX_TRIS");
     if (num_tris && (!xyz || !idx3 || !num_verts)) return fail(ctx, LVBH_EINVAL, "NULL vertex or index buffer");
     DeviceGuard g(ctx->device);
+    if (int rc = finish_pending(ctx)) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (int rc = check_out(ctx, num_tris, flags, out)) return rc;
     out->num_tris = out->num_nodes = num_tris;
@@ -691,6 +703,7 @@ int lvbh_build_mesh(lvbh_ctx *ctx, const float *verts4, uint32_t num_verts, cons
     if (num_tris && !host && ((reinterpret_cast<uintptr_t>(verts4) & 15u) || (reinterpret_cast<uintptr_t>(idx3) & 3u)))
         return fail(ctx, LVBH_EINVAL, "device vertex rows must be 16-byte aligned, indices 4-byte aligned");
     DeviceGuard g(ctx->device);
+    if (int rc = finish_pending(ctx)) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (int rc = check_out(ctx, num_tris, flags, out, 12)) return rc;
     out->num_tris = out->num_nodes = num_tris;
@@ -753,6 +766,7 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
     if (total > LVBH_MAX_TRIS) return fail(ctx, LVBH_EINVAL, "total triangles exceed LVBH_MAX_TRIS");
     if (total && !tri_array) return fail(ctx, LVBH_EINVAL, "tri_array is NULL");
     DeviceGuard g(ctx->device);
+    if (int rc = finish_pending(ctx)) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (int rc = check_out(ctx, total, flags, out)) return rc;
     out->num_tris = out->num_nodes = total;
@@ -766,7 +780,6 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
     }
     if (int rc = ensure_arena(ctx, total)) return rc;
     if (int rc = ensure_batch(ctx, num_segs, (uint32_t)tiles, (uint32_t)blocks128)) return rc;
-    if (ctx->pending) lvbh_sync(ctx);  // the pinned mirror may still be read by the previous build
     if (seg_bounds) std::memcpy(ctx->bh_bounds, seg_bounds, num_segs * 6ull * sizeof(float));
     // segment table for tree blocks of 2^log_block leaves: first triangle, first sort tile,
     // first tree block and first straddling-pass group (16 blocks of one segment) per segment
@@ -916,6 +929,8 @@ int lvbh_sync(lvbh_ctx *ctx) {
     if (err & ERR_LOOKBACK_TIMEOUT) return fail(ctx, LVBH_ETIMEOUT, "radix sort look-back wait exceeded its bound");
     if (err & ERR_COPY_TIMEOUT) return fail(ctx, LVBH_ETIMEOUT, "leaf gather copy wait exceeded its bound");
     if (err & ERR_CLIMB) return fail(ctx, LVBH_EDEVICE, "refit climb exceeded the maximum tree depth");
+    if (err & ERR_SORT_RANGE)
+        return fail(ctx, LVBH_EDEVICE, "radix sort scatter target out of range (digit counts inconsistent with the keys)");
     return LVBH_OK;
 }
 

@@ -118,5 +118,8 @@ extern "C" int lvbh_sort_pairs_noalloc(const uint32_t *keys_in, uint32_t num_key
         cudaGetLastError();
         return LVBH_ECUDA;
     }
-    return (err & ERR_LOOKBACK_TIMEOUT) ? LVBH_ETIMEOUT : LVBH_OK;
+    // a look-back wait that gave up, or any other device-side error (a scatter target out of
+    // range: keys_out / perm_out are then incomplete)
+    if (err & ERR_LOOKBACK_TIMEOUT) return LVBH_ETIMEOUT;
+    return err ? LVBH_EDEVICE : LVBH_OK;
 }

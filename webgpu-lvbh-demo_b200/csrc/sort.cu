@@ -287,14 +287,14 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
     for (uint32_t j = tid; j < tile_n; j += T) {
         const uint32_t key = S.keys[j];
         const uint32_t o = S.out[(key >> shift) & (D - 1)] + j;
-        if (o < n) {  // always true unless a look-back wait gave up
+        if (o < n) {  // always true unless a look-back wait gave up or the counts are wrong
             keys_out[o] = key;
             vals_out[o] = S.vals[j];
         } else {
             oob = true;
         }
     }
-    if (oob) atomicOr(&ctl->err, ERR_LOOKBACK_TIMEOUT);
+    if (oob) atomicOr(&ctl->err, ERR_SORT_RANGE);
 }
 
 
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(T, 4) k_scatter(const uint32_t *__restrict__ k
             oob = true;
         }
     }
-    if (oob) atomicOr(&ctl->err, ERR_CLIMB);
+    if (oob) atomicOr(&ctl->err, ERR_SORT_RANGE);
 }
 
 template <int BITS, class Segs>
