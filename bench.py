@@ -368,24 +368,53 @@ def run_ours(args, world, rank, local):
                                 "frac_of_measured": MODEL_TOTAL * n / (ms * 1e-3) / 1e9 / peak,
                                 "frac_of_8tbs": MODEL_TOTAL * n / (ms * 1e-3) / 1e9 / 8000.0}}
 
-    # end to end through the public API from pinned host memory
+    # end to end through the public API from pinned host memory (the library uploads a large
+    # soup in chunks and runs each chunk's first pass behind the copy of the next): without
+    # host bounds (the box reduced on the device, the headline) and with them (MODEL_BOUNDS
+    # given, as the reference's caller always does)
     htri = torch.from_numpy(tri).pin_memory()
     hroot = torch.empty(16, dtype=torch.int32).pin_memory()
-    e2e_ms = []
+    v = tri.reshape(-1, 3, 4)[:, :, :3]
+    host_box = np.concatenate([v.min(axis=(0, 1)), v.max(axis=(0, 1))]).astype(np.float32)
+
+    def e2e_run(bounds):
+        ms = []
+        for i in range(args.warmup + args.steps):
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            builder.build_soup(htri.numpy(), bounds, outputs=outs, stream=stream, sync=True)
+            with torch.cuda.stream(stream):
+                hroot.copy_(outs["nodes"][0], non_blocking=True)
+            e1.record(stream)
+            e1.synchronize()
+            if i >= args.warmup:
+                ms.append(e0.elapsed_time(e1))
+        return max_over_ranks(statistics.mean(ms), world)
+
+    e2e = e2e_run(None)
+    e2e_hb = e2e_run(host_box)
+    # the pure upload of the same bytes, for scale
+    dst = torch.empty_like(dtri)
+    up_ms = []
     for i in range(args.warmup + args.steps):
-        torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        builder.build_soup(htri.numpy(), None, outputs=outs, stream=stream, sync=True)
         with torch.cuda.stream(stream):
-            hroot.copy_(outs["nodes"][0], non_blocking=True)
-        e1.record(stream)
+            e0.record(stream)
+            dst.copy_(htri.view(dst.shape), non_blocking=True)
+            e1.record(stream)
         e1.synchronize()
         if i >= args.warmup:
-            e2e_ms.append(e0.elapsed_time(e1))
-    e2e = max_over_ranks(statistics.mean(e2e_ms), world)
+            up_ms.append(e0.elapsed_time(e1))
+    del dst
+    up = max_over_ranks(statistics.mean(up_ms), world)
     e2e_line = {"value": world * n / (e2e * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": e2e,
-                "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 64}
+                "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 64,
+                "bounds": "reduced on the device",
+                "host_bounds": {"value": world * n / (e2e_hb * 1e-3) / 1e6, "unit": UNIT,
+                                "ms_per_step": e2e_hb, "h2d_bytes_per_step": 48 * n,
+                                "d2h_bytes_per_step": 64},
+                "upload_only_ms": up, "upload_gbs": 48 * n / (up * 1e-3) / 1e9}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -437,7 +466,10 @@ def summarize(line):
     out = {"build_ms": r(line["ms_per_step"], 4), "stage_ms": {k: r(v, 4) for k, v in line["stage_ms"].items()},
            "roofline_frac": r(line["roofline"]["frac"]),
            "whole_build_frac": r(line["roofline"]["whole_build"]["frac_of_measured"]),
-           "e2e_mprims_per_s": r(line["e2e"]["value"], 1)}
+           "e2e_mprims_per_s": r(line["e2e"]["value"], 1),
+           "e2e_ms": r(line["e2e"]["ms_per_step"], 3),
+           "e2e_host_bounds_ms": r(line["e2e"]["host_bounds"]["ms_per_step"], 3),
+           "upload_only_ms": r(line["e2e"]["upload_only_ms"], 3)}
     b = line.get("batched")
     if b:
         out["batched"] = {"ms_per_batch": r(b["ms_per_batch"]), "builds_per_s": r(b["builds_per_s"], 0),
@@ -445,7 +477,7 @@ def summarize(line):
                           "identical_trees": b["identical_trees"], "num_tris": b["num_tris"]}
     sv = line.get("served")
     if sv:
-        out["served"] = [{"rate": x["rate"], "requests": x["requests"],
+        out["served"] = [{"mode": x["mode"], "rate": x["rate"], "requests": x["requests"],
                           "p50_p99_p999_ms": [r(x["latency_ms"][k]) for k in ("p50", "p99", "p999")],
                           "mean_batch_reqs": r(x["mean_batch_reqs"], 2), "builds_per_s": r(x["builds_per_s"], 1),
                           "plain_p50_p99_ms": [r(x["plain"]["latency_ms"][k]) for k in ("p50", "p99")]}
@@ -856,65 +888,109 @@ def percentiles(x):
             "p999": float(np.percentile(a, 99.9))}
 
 
+def clustered_pool(n, seed, dev):
+    """n triangles of the clustered distribution (64 isotropic Gaussians, means uniform in
+    [0,1]^3, sigma log-uniform in [0.002, 0.05], 10 % uniform background, vertex offsets uniform
+    in [-0.001, 0.001]^3) drawn on the device with torch from `seed`: the served requests' input
+    pool, made in milliseconds instead of seconds of numpy per soup (same recipe as
+    scenes.clustered_soup, not the same numbers)."""
+    import math
+    import torch
+    from lvbh import scenes
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    k = 64
+    means = torch.rand((k, 3), generator=g, device=dev, dtype=torch.float64)
+    sig = torch.exp(torch.rand(k, generator=g, device=dev, dtype=torch.float64)
+                    * (math.log(0.05) - math.log(0.002)) + math.log(0.002))
+    nb = int(round(n * 0.1))
+    nc = n - nb
+    which = torch.randint(0, k, (nc,), generator=g, device=dev)
+    c = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    c[:nc] = means[which] + torch.randn((nc, 3), generator=g, device=dev, dtype=torch.float64) * sig[which, None]
+    c[nc:] = torch.rand((nb, 3), generator=g, device=dev, dtype=torch.float64)
+    c = c[torch.randperm(n, generator=g, device=dev)].float()
+    tri = torch.empty((n, 12), dtype=torch.float32, device=dev)
+    for v in range(3):
+        off = torch.rand((n, 3), generator=g, device=dev) * 2.0 - 1.0
+        tri[:, 4 * v:4 * v + 3] = c + off * 0.001
+        tri[:, 4 * v + 3] = float(scenes.PAD)
+    return tri
+
+
 def run_served(args, world, rank, local):
-    """Served builds: Poisson arrivals at each rate of the sweep, request sizes log-uniform in
-    [1024, 4194304] triangles of the clustered distribution, a 96 GB budget.  Each request's
-    triangles are a prefix of one of a few pooled, seeded clustered soups kept in device memory
-    (the payloads are resident before the run, as the server keeps vertex state resident).
-    Latency = submit -> the request's batch finished on the GPU (server clock).  Beside it the
-    plain per-request builder (lvbh_build_soup, one request at a time in arrival order) serves
-    the same trace."""
+    """Served builds (the served-requests workload): Poisson arrivals at each rate of the plan,
+    `count` requests per rate, sizes log-uniform in [1024, 4194304] triangles of the clustered
+    distribution, a 96 GB budget.  Request i draws its own soup and window from the trace's
+    generator: triangles [o_i, o_i + n_i) of one of `--serve-pool` seeded clustered soups of
+    2^22 triangles - an i.i.d. sample of its soup's mixture, since the soups are drawn triangle
+    by triangle.  Inputs are either device-resident (the server keeps vertex state on the GPU)
+    or pinned host memory, uploaded inside each request's latency.  Latency = submit -> the
+    request's batch finished on the GPU (server clock).  Beside it the plain per-request builder
+    (lvbh_build_soup, one request at a time in arrival order) serves the first
+    `--serve-plain-max` requests of the same trace from the same inputs."""
+    import ctypes
+    from collections import deque
+
     import numpy as np
     import torch
 
     import lvbh
-    from lvbh import scenes
+    from lvbh import _native, scenes
     from lvbh.server import Server
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    pool = [torch.from_numpy(scenes.clustered_soup(1 << 22, seed=100 + k)).to(dev)
-            for k in range(args.serve_pool)]
-    rates = [float(r) for r in args.serve_rates.split(",")]
-    srv = Server(local, hbm_budget=96 << 30, slots=3, max_batch_tris=1 << 24, max_batch_reqs=4096)
-    plain = lvbh.BVHBuilder(local, reserve_tris=1 << 22)
-    pstream = torch.cuda.Stream(dev)
-    pouts = lvbh.empty_outputs(1 << 22, dev)
-    out = {"workload": "served_requests", "budget_gb": 96, "slots": 3, "rates": []}
-    # warm-up of both paths before the sweep: every kernel, every slot, the result memory
-    wsizes = scenes.request_sizes(args.warmup * 64, seed=99)
-    wt = [srv.submit(pool[i % len(pool)][: int(m)]) for i, m in enumerate(wsizes)]
-    for t in wt:
-        srv.wait(t)
-        srv.release(t)
-    for i, m in enumerate(wsizes[: args.warmup * 8]):
-        m = int(m)
-        plain.build_soup(pool[i % len(pool)][:m], None, stream=pstream, graph=False,
-                         outputs={k: v[: m * (2 if k == "parents" else 1)] for k, v in pouts.items()})
+    plan = []
+    for item in args.serve_plan.split(","):
+        mode, rate, count = item.split(":")
+        plan.append((mode, float(rate), int(count)))
+    pool_n = 1 << 22
+    pool = [clustered_pool(pool_n, 100 + k, dev) for k in range(args.serve_pool)]
+    hpool = None
+    if any(m == "host" for m, _, _ in plan):
+        hpool = [p.cpu().pin_memory().numpy() for p in pool]
     torch.cuda.synchronize(dev)
-    for rate in rates:
-        count = int(min(args.serve_max_requests, max(args.serve_min_requests, rate * args.serve_seconds)))
-        sizes = scenes.request_sizes(count, seed=4)
-        rng = np.random.default_rng(int(rate))
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
-        srcs = [pool[i % len(pool)][: int(sizes[i])] for i in range(count)]
-        # warm-up: a few requests through both paths
-        for i in range(min(8, count)):
-            t = srv.submit(srcs[i])
+    srv = Server(local, hbm_budget=96 << 30, slots=3, max_batch_tris=1 << 24, max_batch_reqs=4096)
+    plain = lvbh.BVHBuilder(local, reserve_tris=pool_n)
+    pstream = torch.cuda.Stream(dev)
+    pouts = lvbh.empty_outputs(pool_n, dev)
+    out = {"workload": "served_requests", "budget_gb": 96, "slots": 3, "pool_soups": len(pool),
+           "pool_tris": pool_n, "rates": []}
+
+    def src(mode, j, o, m):
+        return pool[j][o:o + m] if mode == "device" else hpool[j][o:o + m]
+
+    def plain_build(x, m):
+        plain.build_soup(x, None, outputs={k: v[: m * (2 if k == "parents" else 1)] for k, v in pouts.items()},
+                         stream=pstream, graph=False)
+
+    # warm-up of both paths: every kernel, every slot, the result memory, both input kinds
+    wsizes = scenes.request_sizes(args.warmup * 64, seed=99)
+    modes = sorted({m for m, _, _ in plan})
+    for mode in modes:
+        wt = [srv.submit(src(mode, i % len(pool), 0, int(m))) for i, m in enumerate(wsizes)]
+        for t in wt:
             srv.wait(t)
             srv.release(t)
-            plain.build_soup(srcs[i], None, outputs={k: v[: int(sizes[i]) * (2 if k == "parents" else 1)] for k, v in pouts.items()},
-                             stream=pstream, graph=False)
-        # one client thread: submits at the arrival times and, between arrivals, polls the
-        # oldest outstanding requests and releases the finished ones
-        import ctypes
-        from collections import deque
-        from lvbh import _native
-        L, h = _native.lib, srv._h
-        rinfo = _native.RequestInfo()
+        for i, m in enumerate(wsizes[: args.warmup * 8]):
+            plain_build(src(mode, i % len(pool), 0, int(m)), int(m))
+    torch.cuda.synchronize(dev)
+    L, h = _native.lib, srv._h
+    rinfo = _native.RequestInfo()
+    for mode, rate, count in plan:
+        seed = int(rate) * 7 + (1 if mode == "host" else 0)
+        sizes = scenes.request_sizes(count, seed=seed)
+        rng = np.random.default_rng(seed + 1)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+        which = rng.integers(0, len(pool), count)
+        offs = np.floor(rng.random(count) * (pool_n - sizes + 1)).astype(np.int64)
+        srcs = [src(mode, int(which[i]), int(offs[i]), int(sizes[i])) for i in range(count)]
         infos = []
         outstanding = deque()
 
+        # one client thread: submits at the arrival times and, between arrivals, polls the
+        # oldest outstanding requests and releases the finished ones
         def reap(block=False):
             while outstanding:
                 t = outstanding[0]
@@ -941,31 +1017,39 @@ def run_served(args, world, rank, local):
         s1 = srv.stats()
         lat = [x[0] for x in infos]
         span = max(t_end - t0, 1e-9)
-        served = {"rate": rate, "requests": count, "latency_ms": percentiles(lat),
-                  "queued_ms": percentiles([x[1] for x in infos]),
+        nb = max(1, s1["batches"] - s0["batches"])
+        served = {"mode": mode, "rate": rate, "requests": count,
+                  "inputs": ("device-resident windows of the pool soups" if mode == "device" else
+                             "pinned host windows of the pool soups, uploaded inside the latency"),
+                  "h2d_bytes": int(48 * sizes.sum()) if mode == "host" else 0,
+                  "latency_ms": percentiles(lat), "queued_ms": percentiles([x[1] for x in infos]),
                   "exec_ms": percentiles([x[0] - x[1] for x in infos]),
                   "builds_per_s": count / span, "mprims_per_s": float(sizes.sum()) / span / 1e6,
-                  "batches": s1["batches"] - s0["batches"],
-                  "mean_batch_reqs": count / max(1, s1["batches"] - s0["batches"]),
-                  "max_batch_seen": s1["max_batch_seen"], "admission_waits": s1["admission_waits"] - s0["admission_waits"],
+                  "arrival_span_s": float(arrivals[-1]), "served_span_s": span,
+                  "batches": s1["batches"] - s0["batches"], "mean_batch_reqs": count / nb,
+                  "batch_reqs_p50_p99": [float(np.percentile([x[2] for x in infos], q)) for q in (50, 99)],
+                  "max_batch_seen": s1["max_batch_seen"],
+                  "admission_waits": s1["admission_waits"] - s0["admission_waits"],
                   "peak_result_gb": s1["peak_bytes"] / 2**30}
-        # the plain per-request builder on the same trace
+        # the plain per-request builder on the first requests of the same trace
+        pc = min(count, args.serve_plain_max)
         plat = []
         t0 = time.perf_counter()
-        for i in range(count):
+        for i in range(pc):
             while time.perf_counter() - t0 < arrivals[i]:
                 pass
-            m = int(sizes[i])
-            plain.build_soup(srcs[i], None, outputs={k: v[: m * (2 if k == "parents" else 1)] for k, v in pouts.items()},
-                             stream=pstream, graph=False)
+            plain_build(srcs[i], int(sizes[i]))
             plat.append((time.perf_counter() - t0 - arrivals[i]) * 1e3)
         pspan = time.perf_counter() - t0
-        served["plain"] = {"latency_ms": percentiles(plat), "builds_per_s": count / pspan}
+        served["plain"] = {"requests": pc, "latency_ms": percentiles(plat), "builds_per_s": pc / pspan}
         out["rates"].append(served)
+        del srcs
     st = srv.stats()
     out["server_stats"] = {k: st[k] for k in ("batches", "completed", "failed", "max_batch_seen")}
     srv.close()
     plain.close()
+    del pool, hpool
+    torch.cuda.empty_cache()
     return out
 
 
@@ -994,11 +1078,10 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-obj", action="store_true")
     ap.add_argument("--no-trace", action="store_true")
-    ap.add_argument("--serve-rates", default="200,500,1000,2000,5000")
-    ap.add_argument("--serve-seconds", type=float, default=2.0)
-    ap.add_argument("--serve-min-requests", type=int, default=1000)
-    ap.add_argument("--serve-max-requests", type=int, default=100_000)
-    ap.add_argument("--serve-pool", type=int, default=4)
+    # served requests: mode (device | host input) : rate (req/s) : requests, comma-separated
+    ap.add_argument("--serve-plan", default="device:2000:100000,device:5000:100000,host:2000:100000")
+    ap.add_argument("--serve-plain-max", type=int, default=10_000)
+    ap.add_argument("--serve-pool", type=int, default=16)
     ap.add_argument("--rays", type=int, default=1 << 22)
     ap.add_argument("--obj-quads", type=int, default=1024)  # OBJ workload: sphere grid side
     ap.add_argument("--pt-width", type=int, default=1920)

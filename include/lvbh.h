@@ -380,6 +380,17 @@ LVBH_API int  lvbh_parse_obj(lvbh_ctx *ctx, const char *text, uint64_t bytes, ui
                              const float **tri_out, uint32_t *num_tris, double *bounds6,
                              uint64_t *err_line, void *stream);
 
+/* ---- test hook: a device wait that runs out --------------------------------------------
+ * No counterpart in the reference (its shaders spin without a bound).  For tests of the
+ * bounded waits: on this context, sort tile `stall_tile` (0-based, in the order tiles start) of
+ * every decoupled look-back sort pass (the batched build's) publishes no counts, so the tiles
+ * after it in its mesh wait until their bound runs out; the build then returns LVBH_ETIMEOUT
+ * and builds no tree from the unfinished sort.  spin_cycles, when not 0, replaces the bound
+ * (about 2e9 clock cycles, a second).  lvbh_test_stall_lookback(ctx, UINT32_MAX, 0) restores
+ * normal builds.  Finishes a pending LVBH_ASYNC build first (returning its status if it
+ * failed).  Returns LVBH_OK, LVBH_EINVAL or LVBH_ECUDA. */
+LVBH_API int  lvbh_test_stall_lookback(lvbh_ctx *ctx, uint32_t stall_tile, uint32_t spin_cycles);
+
 #ifdef __cplusplus
 }
 #endif

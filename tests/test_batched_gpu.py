@@ -221,3 +221,33 @@ def test_async_batched_then_larger_batch_keeps_first_status_and_bounds():
                 assert_same(got, ref, f"mesh {i}")
     finally:
         b.close()
+
+
+def test_lookback_wait_runs_out_then_clean_build(builder):
+    """A device wait that runs out, made on the host side: with the test hook, sort tile 1 (the
+    second tile of mesh 0) never publishes its look-back counts, so the later tiles of mesh 0
+    wait until their lowered bound (2e6 cycles, about a millisecond) runs out.  The build must
+    report LVBH_ETIMEOUT, build no tree from the unfinished sort, and leave the context usable:
+    the next build on it, hook cleared, equals the build on an untouched context."""
+    import time
+    import torch
+    import lvbh
+    import lvbh._native as nat
+    tri, offs = make_batch([20_000, 300, 9000], seed=21)  # mesh 0 spans sort tiles 0..4
+    t = torch.from_numpy(tri).cuda()
+    ref = builder.build_batched(t, offs)
+    b = lvbh.BVHBuilder(0)
+    try:
+        assert nat.lib.lvbh_test_stall_lookback(b.ctx, 1, 2_000_000) == nat.OK
+        t0 = time.perf_counter()
+        with pytest.raises(nat.LvbhError) as ei:
+            b.build_batched(t, offs)
+        assert ei.value.code == nat.ETIMEOUT, str(ei.value)
+        assert "look-back" in str(ei.value)
+        assert time.perf_counter() - t0 < 5.0
+        assert nat.lib.lvbh_test_stall_lookback(b.ctx, 0xFFFFFFFF, 0) == nat.OK
+        got = b.build_batched(t, offs)
+        for i in range(len(offs) - 1):
+            assert_same(mesh_np(got, i), mesh_np(ref, i), f"mesh {i} after the timed-out build")
+    finally:
+        b.close()

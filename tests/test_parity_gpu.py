@@ -325,3 +325,27 @@ def test_shrinking_builds_on_one_context(builder):
 def oracle_build(tri):
     import oracle
     return oracle.build(tri, None, threads=0)
+
+
+def test_chunked_host_upload(builder):
+    """A host soup of 2^21 + 4099 triangles without host bounds is uploaded in chunks, each
+    chunk's box and centroid pass running while the next chunk is copied: bit-exact against the
+    oracle and the device-input build, from pageable and pinned host memory, after an
+    LVBH_ASYNC build that still reads the staging buffer, and again on graph replay."""
+    import torch
+    from lvbh import scenes
+    import oracle
+    n = (1 << 21) + 4099
+    tri = scenes.clustered_soup(n, seed=12)
+    ref = oracle.build(tri, None, threads=0)
+    _, dev = build_np(builder, tri)
+    assert_same(dev, ref, "device input")
+    other = scenes.clustered_soup(n, seed=13)
+    pending = builder.build_soup(other, None, sync=False)
+    _, got = build_np(builder, tri, host=True)
+    assert_same(got, ref, "chunked upload after an async build")
+    del pending
+    pinned = torch.from_numpy(tri).pin_memory()
+    for tag in ("pinned", "pinned, replayed"):
+        _, got = build_np(builder, pinned.numpy(), host=True)
+        assert_same(got, ref, tag)

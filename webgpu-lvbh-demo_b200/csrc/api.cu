@@ -4,6 +4,7 @@
 // module's execute(): 69 queue submits and 20 host waits per build) with one stream-ordered
 // chain of 8 kernels and a memset, replayed as a cached CUDA graph when the same build shape
 // repeats, and a single host wait at the end (none with LVBH_ASYNC).
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -37,7 +38,16 @@ using namespace lvbh;
 namespace {
 
 constexpr size_t kAlign = 256;
+// A host soup whose box is reduced on the device is uploaded in up to kUploadChunks chunks of
+// at least kUploadChunkTris triangles (a multiple of the sort tile); each chunk's box and
+// centroid pass runs on the build stream while the next chunk is copied.
+constexpr uint32_t kUploadChunks = 8;
+constexpr uint32_t kUploadChunkTris = 1u << 20;
 inline size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+// The head of the control block (test words, error words, tile counters, reduced bounds) is
+// read back with each build into a 64-byte pinned buffer.
+static_assert(offsetof(Control, pad1) <= 64, "control block head fits the pinned readback");
 
 // The control block and the sort's tile / chunk histograms.
 size_t control_bytes(uint32_t n) {
@@ -48,7 +58,7 @@ size_t control_bytes(uint32_t n) {
 // pass's open-node buffers, the control block and the look-back words.
 size_t arena_bytes(uint32_t cap) {
     const size_t groups = emit_groups(cap);
-    return 4 * align_up((size_t)cap * 4) + align_up((size_t)cap * 32) + align_up((size_t)cap) +
+    return 4 * align_up((size_t)cap * 4) + align_up((size_t)cap * 12) + align_up((size_t)cap * 32) + align_up((size_t)cap) +
            align_up(groups * kOpenCap * sizeof(OpenItem)) + align_up(2 * groups * sizeof(uint32_t)) +
            align_up(sizeof(uint32_t)) + control_bytes(cap);
 }
@@ -59,6 +69,7 @@ struct GraphKey {
     uint32_t nverts = 0;
     uint32_t n = 0;
     HostBounds hb{};
+    int pre = 0;
     void *outs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     bool operator==(const GraphKey &o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
@@ -100,6 +111,7 @@ struct lvbh_ctx {
     void *arena = nullptr;
     uint32_t *keys_b = nullptr, *vals_b = nullptr;
     uint32_t *keys_a = nullptr;  // unsorted Morton keys (input of the first sort pass)
+    float *cen = nullptr;        // triangle centroids, x / y / z arrays of `cap` floats
     OpenItem *items = nullptr;
     uint32_t *counts = nullptr, *arrive = nullptr, *epoch = nullptr;
     float4 *pend = nullptr;
@@ -111,10 +123,15 @@ struct lvbh_ctx {
     void *stage = nullptr;
     // pinned readback of the control block head
     uint32_t *host_ctl = nullptr;
+    // the control block's test words (lvbh_test_stall_lookback), restored when the arena moves
+    uint32_t test_stall1 = 0, test_spin = 0;
     uint32_t *trace_counter = nullptr;  // ray counter of the persistent traversal
     ObjScratch obj;                     // OBJ ingest buffers (the parsed soup among them)
     cudaEvent_t ev[LVBH_NUM_STAGES + 1] = {};
     bool ev_valid = false;
+    // chunked upload of a host soup: its copy stream and events (start, one per chunk)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t up_ev[1 + kUploadChunks] = {};
     // cached graph of the last build shape
     cudaStream_t cap_stream = nullptr;
     GraphKey gkey;
@@ -272,6 +289,7 @@ int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
     ctx->vals_b = reinterpret_cast<uint32_t *>(c); c += kb;
     ctx->arrive = reinterpret_cast<uint32_t *>(c); c += kb;
     ctx->keys_a = reinterpret_cast<uint32_t *>(c); c += kb;
+    ctx->cen = reinterpret_cast<float *>(c); c += align_up((size_t)cap * 12);
     ctx->pend = reinterpret_cast<float4 *>(c); c += align_up((size_t)cap * 32);
     ctx->pend_d = reinterpret_cast<uint8_t *>(c); c += align_up((size_t)cap);
     ctx->items = reinterpret_cast<OpenItem *>(c); c += align_up(groups * kOpenCap * sizeof(OpenItem));
@@ -282,6 +300,9 @@ int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
     // arrival words and the epoch start at zero; from then on the epoch keeps them valid
     LVBH_CUDA(ctx, cudaMemset(ctx->arrive, 0, kb));
     LVBH_CUDA(ctx, cudaMemset(ctx->epoch, 0, sizeof(uint32_t)));
+    // the control block's test words (zero unless lvbh_test_stall_lookback set them)
+    const uint32_t test_words[2] = {ctx->test_stall1, ctx->test_spin};
+    LVBH_CUDA(ctx, cudaMemcpy(ctx->ctl, test_words, sizeof test_words, cudaMemcpyHostToDevice));
     ctx->cap = cap;
     return LVBH_OK;
 }
@@ -307,14 +328,24 @@ struct MeshIn {
     const uint32_t *idx3;
 };
 
+// What upload_chunked did already, chunk by chunk behind the soup's upload (the control block
+// is then cleared too): nothing, the box and centroids (no host bounds), or the keys (host
+// bounds).
+enum Pre : int { kPreNone = 0, kPreCen = 1, kPreKeys = 2 };
+
 void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
-                   const lvbh_result *out, cudaStream_t s, bool profile, const MeshIn *mesh = nullptr) {
+                   const lvbh_result *out, cudaStream_t s, bool profile, const MeshIn *mesh = nullptr,
+                   int pre = kPreNone) {
     if (profile) cudaEventRecord(ctx->ev[1], s);
-    cudaMemsetAsync(reinterpret_cast<char *>(ctx->ctl) + offsetof(Control, err), 0,
-                    sizeof(Control) - offsetof(Control, err), s);
-    if (!hb.use) {
+    if (pre == kPreNone)
+        cudaMemsetAsync(reinterpret_cast<char *>(ctx->ctl) + offsetof(Control, err), 0,
+                        sizeof(Control) - offsetof(Control, err), s);
+    // a soup whose box is reduced here: box and centroids in one pass, then the keys from the
+    // centroids
+    const bool cen_path = !hb.use && !mesh;
+    if (!hb.use && pre == kPreNone) {
         if (mesh) launch_bounds_mesh(mesh->verts, mesh->nverts, mesh->idx3, n, ctx->ctl, s);
-        else launch_bounds(tri, n, ctx->ctl, s);
+        else launch_bounds_cen(tri, 0, n, ctx->cen, ctx->cap, ctx->ctl, s);
     }
     if (profile) cudaEventRecord(ctx->ev[2], s);
     // unsorted keys go to keys_a, so that the three passes ping-pong keys_a -> result ->
@@ -322,7 +353,8 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
     uint32_t *keys_a = ctx->keys_a;
     if (mesh) launch_morton_mesh(mesh->verts, mesh->nverts, mesh->idx3, n, hb, ctx->ctl, keys_a, ctx->epoch,
                                  ctx->lookback, s);
-    else launch_morton(tri, n, hb, ctx->ctl, keys_a, ctx->epoch, ctx->lookback, s);
+    else if (cen_path) launch_morton_cen(ctx->cen, ctx->cap, n, ctx->ctl, keys_a, ctx->epoch, ctx->lookback, s);
+    else if (pre != kPreKeys) launch_morton(tri, n, hb, ctx->ctl, keys_a, ctx->epoch, ctx->lookback, s);
     if (profile) cudaEventRecord(ctx->ev[3], s);
     launch_sort_pass(keys_a, nullptr, out->morton, out->leaf_index, n, 0, true, ctx->ctl, ctx->lookback, s);
     launch_sort_pass(out->morton, out->leaf_index, ctx->keys_b, ctx->vals_b, n, 1, false, ctx->ctl, ctx->lookback, s);
@@ -417,7 +449,7 @@ int launch_batch_graph(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bo
 }
 
 int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
-                 const lvbh_result *out, cudaStream_t s, const MeshIn *mesh) {
+                 const lvbh_result *out, cudaStream_t s, const MeshIn *mesh, int pre) {
     GraphKey key;
     std::memset(static_cast<void *>(&key), 0, sizeof key);  // padding takes part in the compare
     key.tri = tri;
@@ -428,12 +460,13 @@ int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds 
     }
     key.n = n;
     key.hb = hb;
+    key.pre = pre;
     key.outs[0] = out->nodes; key.outs[1] = out->tris; key.outs[2] = out->parents;
     key.outs[3] = out->leaf_index; key.outs[4] = out->morton;
     if (!ctx->gexec || !(key == ctx->gkey)) {
         if (!ctx->cap_stream) LVBH_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
         LVBH_CUDA(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_build(ctx, tri, n, hb, out, ctx->cap_stream, false, mesh);
+        enqueue_build(ctx, tri, n, hb, out, ctx->cap_stream, false, mesh, pre);
         cudaGraph_t g = nullptr;
         LVBH_CUDA(ctx, cudaStreamEndCapture(ctx->cap_stream, &g));
         bool updated = false;
@@ -482,7 +515,7 @@ int alloc_outputs(lvbh_ctx *ctx, uint32_t n, lvbh_result *out, size_t tri_row = 
 
 int build_common(lvbh_ctx *ctx, const float4 *tri_dev, uint32_t n, const float *model_bounds,
                  uint32_t flags, lvbh_result *out, cudaStream_t s, bool profile_upload,
-                 const MeshIn *mesh = nullptr) {
+                 const MeshIn *mesh = nullptr, int pre = kPreNone) {
     HostBounds hb{};
     if (model_bounds) {
         std::memcpy(hb.v, model_bounds, sizeof hb.v);
@@ -498,11 +531,11 @@ int build_common(lvbh_ctx *ctx, const float4 *tri_dev, uint32_t n, const float *
     int rc = LVBH_OK;
     if (profile && !profile_upload) cudaEventRecord(ctx->ev[0], s);
     if (profile || (flags & LVBH_NO_GRAPH)) {
-        enqueue_build(ctx, tri_dev, n, hb, out, s, profile, mesh);
+        enqueue_build(ctx, tri_dev, n, hb, out, s, profile, mesh, pre);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
     } else {
-        rc = launch_graph(ctx, tri_dev, n, hb, out, s, mesh);
+        rc = launch_graph(ctx, tri_dev, n, hb, out, s, mesh, pre);
         if (rc) return rc;
     }
     ctx->ev_valid = profile;
@@ -546,6 +579,52 @@ int check_out(lvbh_ctx *ctx, uint32_t n, uint32_t flags, lvbh_result *out, size_
 // A build entry first completes the context's pending LVBH_ASYNC build, before it touches
 // any buffer that build may still use (arena, staging copy, pinned mirrors).  When the pending
 // build failed, its status is returned and no new build starts, so the status is not lost.
+// A host soup to the staging buffer in chunks on the context's copy stream; the build stream
+// runs each chunk's first pass as soon as the chunk has landed, so that pass hides behind the
+// upload: the box and centroid pass without host bounds, the Morton keys with them.  Clears
+// the control block first (the build then skips its clear).  Returns the Pre the build goes on
+// from.
+int upload_chunked(lvbh_ctx *ctx, const float *host, uint32_t n, const float *model_bounds, cudaStream_t s,
+                   int *pre) {
+    if (!ctx->copy_stream) LVBH_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    for (auto &e : ctx->up_ev)
+        if (!e) LVBH_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    LVBH_CUDA(ctx, cudaMemsetAsync(reinterpret_cast<char *>(ctx->ctl) + offsetof(Control, err), 0,
+                                   sizeof(Control) - offsetof(Control, err), s));
+    // the copies wait for earlier work on s (an earlier build may still read the staging buffer)
+    LVBH_CUDA(ctx, cudaEventRecord(ctx->up_ev[0], s));
+    LVBH_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->up_ev[0], 0));
+    HostBounds hb{};
+    if (model_bounds) {
+        std::memcpy(hb.v, model_bounds, sizeof hb.v);
+        hb.use = 1;
+    }
+    // chunks end on Morton-pass chunks of sort tiles (the key pass runs per chunk)
+    const uint32_t unit = sort_chunk_tiles(n) * (uint32_t)kSortTile, units = sort_chunks(n);
+    uint32_t chunks = n / kUploadChunkTris;
+    if (chunks > kUploadChunks) chunks = kUploadChunks;
+    if (chunks < 1) chunks = 1;
+    const uint32_t per = (units + chunks - 1) / chunks;  // Morton chunks per upload chunk
+    char *stage = static_cast<char *>(ctx->stage);
+    const float4 *tri = static_cast<const float4 *>(ctx->stage);
+    const char *src = reinterpret_cast<const char *>(host);
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const uint32_t u0 = c * per, u1 = std::min(units, (c + 1) * per);
+        if (u0 >= u1) break;
+        const uint32_t t0 = u0 * unit, t1 = std::min(n, u1 * unit);
+        LVBH_CUDA(ctx, cudaMemcpyAsync(stage + 48ull * t0, src + 48ull * t0, 48ull * (t1 - t0),
+                                       cudaMemcpyHostToDevice, ctx->copy_stream));
+        LVBH_CUDA(ctx, cudaEventRecord(ctx->up_ev[1 + c], ctx->copy_stream));
+        LVBH_CUDA(ctx, cudaStreamWaitEvent(s, ctx->up_ev[1 + c], 0));
+        if (hb.use) launch_morton_chunks(tri, n, hb, ctx->ctl, ctx->keys_a, ctx->epoch, ctx->lookback, u0, u1, s);
+        else launch_bounds_cen(tri, t0, t1, ctx->cen, ctx->cap, ctx->ctl, s);
+    }
+    *pre = hb.use ? kPreKeys : kPreCen;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+    return LVBH_OK;
+}
+
 int finish_pending(lvbh_ctx *ctx) {
     if (!ctx->pending) return LVBH_OK;
     const int rc = lvbh_sync(ctx);
@@ -616,6 +695,8 @@ void lvbh_destroy(lvbh_ctx *ctx) {
     if (ctx->stage) cudaFree(ctx->stage);
     for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    for (auto &e : ctx->up_ev) if (e) cudaEventDestroy(e);
     if (ctx->host_ctl) cudaFreeHost(ctx->host_ctl);
     if (ctx->trace_counter) cudaFree(ctx->trace_counter);
     obj_free(ctx->obj);
@@ -643,6 +724,12 @@ int lvbh_build_soup(lvbh_ctx *ctx, const float *tri_array, uint32_t num_tris,
     bool profile_upload = false;
     if ((flags & LVBH_INPUT_HOST) && num_tris) {
         if (int rc = ensure_stage(ctx, 48ull * num_tris)) return rc;
+        if (!(flags & LVBH_PROFILE) && num_tris >= 2 * kUploadChunkTris) {
+            int pre = kPreNone;
+            if (int rc = upload_chunked(ctx, tri_array, num_tris, model_bounds, s, &pre)) return rc;
+            return build_common(ctx, static_cast<const float4 *>(ctx->stage), num_tris, model_bounds, flags,
+                                out, s, false, nullptr, pre);
+        }
         if (flags & LVBH_PROFILE) { cudaEventRecord(ctx->ev[0], s); profile_upload = true; }
         LVBH_CUDA(ctx, cudaMemcpyAsync(ctx->stage, tri_array, 48ull * num_tris, cudaMemcpyHostToDevice, s));
         tri = static_cast<const float4 *>(ctx->stage);
@@ -899,7 +986,7 @@ int lvbh_sync(lvbh_ctx *ctx) {
     ctx->pending = false;
     cudaError_t e = cudaStreamSynchronize(ctx->last_stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamSynchronize");
-    const uint32_t err = ctx->host_ctl[0] | ctx->host_ctl[1];
+    const uint32_t err = ctx->host_ctl[offsetof(Control, aux_err) / 4] | ctx->host_ctl[offsetof(Control, err) / 4];
     if (ctx->last_batch) {
         if (ctx->last_bounds_out) {
             for (uint64_t i = 0; i < ctx->last_segs * 6ull; ++i) {
@@ -931,6 +1018,19 @@ int lvbh_sync(lvbh_ctx *ctx) {
     if (err & ERR_CLIMB) return fail(ctx, LVBH_EDEVICE, "refit climb exceeded the maximum tree depth");
     if (err & ERR_SORT_RANGE)
         return fail(ctx, LVBH_EDEVICE, "radix sort scatter target out of range (digit counts inconsistent with the keys)");
+    return LVBH_OK;
+}
+
+int lvbh_test_stall_lookback(lvbh_ctx *ctx, uint32_t stall_tile, uint32_t spin_cycles) {
+    if (!ctx) return LVBH_EINVAL;
+    DeviceGuard g(ctx->device);
+    if (int rc = finish_pending(ctx)) return rc;
+    ctx->test_stall1 = stall_tile + 1u;  // UINT32_MAX -> 0: no tile stalls
+    ctx->test_spin = spin_cycles;
+    if (ctx->ctl) {
+        const uint32_t test_words[2] = {ctx->test_stall1, ctx->test_spin};
+        LVBH_CUDA(ctx, cudaMemcpy(ctx->ctl, test_words, sizeof test_words, cudaMemcpyHostToDevice));
+    }
     return LVBH_OK;
 }
 

@@ -153,6 +153,8 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
     extern __shared__ __align__(16) unsigned char smem[];
     ClimbSmem<EB> &S = *reinterpret_cast<ClimbSmem<EB> *>(smem);
     const int t = threadIdx.x, lane = t & 31;
+    // a sort whose look-back gave up left unsorted keys: build nothing from them (uniform)
+    if (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT) return;
     const int nblk = segs.blocks();
     const uint32_t lt = lanemask_lt();
 
@@ -429,6 +431,7 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
                                                   Control *ctl) {
     const int gw = (blockIdx.x * 256 + threadIdx.x) / LANES, lane = threadIdx.x % LANES;
     if (gw >= segs.blocks()) return;
+    if (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT) return;  // unsorted keys: nothing to build
     const int cnt = (int)min(counts[gw], (uint32_t)cap);
     if (lane >= cnt) return;
     const uint32_t epoch = *epoch_p;
@@ -560,6 +563,7 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, Open
     GroupSmem &S = *reinterpret_cast<GroupSmem *>(smem_raw);
     const int t = threadIdx.x;
     const int g = blockIdx.x;
+    if (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT) return;  // unsorted keys: nothing to build
     const GroupSpan gs = groups.group(g);
     const int n = gs.n, blk0 = gs.blk0, blk1 = gs.blk1;
     const int lo_leaf = gs.leaf0, hi_leaf = min(n, gs.leaf0 + (blk1 - blk0) * EB);

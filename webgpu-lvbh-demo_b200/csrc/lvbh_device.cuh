@@ -39,10 +39,15 @@ __device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) 
 //   cen = (max + min) * .5f;  rel = (cen - umin) / (umax - umin);  q = u32(rel * 1023.99f)
 // Every operation is rounded on its own (no contraction), division is correctly rounded,
 // and the float->u32 conversion truncates and saturates (NaN -> 0).
-__device__ __forceinline__ uint32_t quantise(float bmin, float bmax, float umin, float umax) {
-    const float cen = __fmul_rn(__fadd_rn(bmax, bmin), 0.5f);
+// Split in two for the path that stores centroids before the scene box is known: centroid()
+// needs only the triangle, quantise_cen() the scene box; quantise() is the two in a row.
+__device__ __forceinline__ float centroid(float bmin, float bmax) { return __fmul_rn(__fadd_rn(bmax, bmin), 0.5f); }
+__device__ __forceinline__ uint32_t quantise_cen(float cen, float umin, float umax) {
     const float rel = __fdiv_rn(__fsub_rn(cen, umin), __fsub_rn(umax, umin));
     return __float2uint_rz(__fmul_rn(rel, 1023.99f));
+}
+__device__ __forceinline__ uint32_t quantise(float bmin, float bmax, float umin, float umax) {
+    return quantise_cen(centroid(bmin, bmax), umin, umax);
 }
 
 // Common-prefix length delta(i, j) of the sorted keys (radix-tree.js:160-185): -1 when j is

@@ -68,8 +68,14 @@ struct __align__(16) OpenItem {
 
 // Per-build control block in device memory.  Everything from `err` on is zeroed by one memset
 // at the start of a build; `aux_err` collects errors of steps that run before that memset (the
-// indexed-mesh gather) and is cleared by the host before them.
+// indexed-mesh gather) and is cleared by the host before them.  The two test words at the front
+// (lvbh_test_stall_lookback) persist across builds: when test_stall_tile1 is not zero, sort
+// tile test_stall_tile1 - 1 of every look-back pass publishes nothing, so the tiles after it
+// wait until their bound runs out; test_spin_limit, when not zero, replaces kSpinLimitCycles
+// as that bound.  Both are zero in normal use.
 struct Control {
+    uint32_t test_stall_tile1;
+    uint32_t test_spin_limit;
     uint32_t aux_err;
     uint32_t err;
     uint32_t tile_counter[kSortPasses32];
@@ -117,6 +123,17 @@ void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s);
 // non-finite vertices in ctl->err and advances the build epoch *epoch used by K3c.
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl,
                    uint32_t *keys_out, uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s);
+// K1b over the sort-tile chunks [c0, c1) only (chunk = sort_chunk_tiles(n) tiles): the keys of
+// a soup uploaded chunk by chunk, each part launched once its triangles have landed.
+void launch_morton_chunks(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl, uint32_t *keys,
+                          uint32_t *epoch, uint32_t *sort_scratch, uint32_t c0, uint32_t c1, cudaStream_t s);
+// K1a + K1b split for a soup whose box is reduced on the device: K1a over triangles [t0, t1)
+// also stores each triangle's centroid (cen[t], cen[stride + t], cen[2 stride + t]); K1b then
+// quantises the centroids (12 bytes per triangle instead of the 48-byte soup).
+void launch_bounds_cen(const float4 *tri, uint32_t t0, uint32_t t1, float *cen, uint32_t cen_stride,
+                       Control *ctl, cudaStream_t s);
+void launch_morton_cen(const float *cen, uint32_t cen_stride, uint32_t n, Control *ctl, uint32_t *keys,
+                       uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s);
 // K2: one reduce-then-scan pass over 10-bit digit `pass` (0..2) of 30-bit keys (the global
 // digit counts come from ctl->hist).  counted: the tile histograms and chunk sums of this
 // pass are already in scratch (K1b writes those of pass 0).  vals_in == nullptr generates the

@@ -68,28 +68,103 @@ __global__ void __launch_bounds__(kThreads) k_bounds(const float4 *__restrict__ 
     }
 }
 
+// K1a for a soup whose box is reduced on the device: the box and every triangle's centroid in
+// one read of triangles [t0, t1).  A warp loads a row of 32 triangles as three coalesced
+// 512-byte loads (its next row in flight meanwhile), transposes it through shared memory so
+// that each lane owns one triangle, and stores the centroids (box.max + box.min) * .5 in
+// structure-of-arrays form (three coalesced 128-byte stores); K1b then reads 12 bytes per
+// triangle instead of the soup's 48.  Box mins and maxes feed the scene box (fminf / fmaxf are
+// exact, so the box is the min / max over every vertex whatever the order); non-finite
+// vertices set ERR_NONFINITE.  Launched per chunk of the soup, it can run behind the chunk's
+// upload.
+__global__ void __launch_bounds__(kThreads) k_bounds_cen(const float4 *__restrict__ tri, uint32_t t0, uint32_t t1,
+                                                         float *__restrict__ cen, uint32_t stride,
+                                                         Control *__restrict__ ctl) {
+    __shared__ float4 stage[kWarps][96];
+    __shared__ float s[kWarps][6];
+    float mn[3] = {INFINITY, INFINITY, INFINITY};
+    float mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rows = (t1 - t0 + 31u) / 32u;
+    const uint32_t nw = gridDim.x * kWarps;
+    const uint64_t nv = 3ull * t1;
+    bool bad = false;
+    float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0, q2 = q0;
+    auto ld_row = [&](uint32_t r) {
+        const uint64_t base = 3ull * (t0 + 32ull * r);
+        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+        q0 = base + lane < nv ? ld_stream(tri + base + lane) : z;
+        q1 = base + 32 + lane < nv ? ld_stream(tri + base + 32 + lane) : z;
+        q2 = base + 64 + lane < nv ? ld_stream(tri + base + 64 + lane) : z;
+    };
+    uint32_t r = blockIdx.x * kWarps + warp;
+    if (r < rows) ld_row(r);
+    for (; r < rows; r += nw) {
+        const float4 a0 = q0, a1 = q1, a2 = q2;
+        if (r + nw < rows) ld_row(r + nw);
+        stage[warp][lane] = a0;
+        stage[warp][32 + lane] = a1;
+        stage[warp][64 + lane] = a2;
+        __syncwarp();
+        const float4 v0 = stage[warp][3 * lane], v1 = stage[warp][3 * lane + 1], v2 = stage[warp][3 * lane + 2];
+        __syncwarp();
+        const uint32_t t = t0 + 32u * r + lane;
+        if (t < t1) {
+            bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
+            // box.min = min(v0, min(v1, v2)); box.max = max(v0, max(v1, v2))   (aabb-z-idx.js:186-187)
+            const float nx = fminf(v0.x, fminf(v1.x, v2.x)), ny = fminf(v0.y, fminf(v1.y, v2.y)), nz = fminf(v0.z, fminf(v1.z, v2.z));
+            const float xx = fmaxf(v0.x, fmaxf(v1.x, v2.x)), xy = fmaxf(v0.y, fmaxf(v1.y, v2.y)), xz = fmaxf(v0.z, fmaxf(v1.z, v2.z));
+            __stcs(cen + t, centroid(nx, xx));
+            __stcs(cen + stride + t, centroid(ny, xy));
+            __stcs(cen + 2ull * stride + t, centroid(nz, xz));
+            mn[0] = fminf(mn[0], nx); mn[1] = fminf(mn[1], ny); mn[2] = fminf(mn[2], nz);
+            mx[0] = fmaxf(mx[0], xx); mx[1] = fmaxf(mx[1], xy); mx[2] = fmaxf(mx[2], xz);
+        }
+    }
+    warp_minmax(mn, mx);
+    if (lane == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { s[warp][a] = mn[a]; s[warp][3 + a] = mx[a]; }
+    }
+    if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int a = threadIdx.x;
+        float v = s[0][a];
+        for (int w = 1; w < kWarps; ++w) v = a < 3 ? fminf(v, s[w][a]) : fmaxf(v, s[w][a]);
+        if (a < 3) atomicMax(&ctl->bounds_ord[a], ~ord_lo(v));
+        else atomicMax(&ctl->bounds_ord[a], ord_lo(v));
+    }
+}
+
 // K1b: per triangle box, centroid, quantisation and 30-bit Morton key, written in input order.
 // One block per chunk of sort_chunk_tiles(n) sort tiles: per tile each warp takes chunks of 32
 // triangles (96 consecutive float4, three coalesced 512-byte loads, transposed through shared
 // memory so that each lane owns a triangle); the digit counts of all three sort passes
 // accumulate over the block, and the counts of the first pass's digit per tile and per chunk
 // go straight to the sort's scratch, so the first sort pass starts from them.
-// MESH: the triangles are index triples into a buffer of 16-byte vertex rows (the indexed leaf
-// format's input); each lane gathers its triangle's three rows, an index past the buffer reads
-// row 0 and sets ERR_BAD_INDEX.
-template <bool MESH>
+// kSrcMesh: the triangles are index triples into a buffer of 16-byte vertex rows (the indexed
+// leaf format's input); each lane gathers its triangle's three rows, an index past the buffer
+// reads row 0 and sets ERR_BAD_INDEX.  kSrcCen: the centroids K1a stored (structure of arrays,
+// `cen_stride` floats apart), quantised with the device-reduced box; K1a checked the vertices.
+constexpr int kSrcSoup = 0, kSrcMesh = 1, kSrcCen = 2;
+template <int SRC>
 __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ tri, uint32_t n,
                                                      HostBounds hb, Control *__restrict__ ctl,
                                                      uint32_t *__restrict__ keys,
                                                      uint32_t *__restrict__ epoch, uint32_t chunk_tiles,
                                                      uint32_t *__restrict__ tile_hist,
                                                      uint32_t *__restrict__ chunk_sum,
-                                                     const uint32_t *__restrict__ idx3, uint32_t nverts) {
+                                                     const uint32_t *__restrict__ idx3, uint32_t nverts,
+                                                     const float *__restrict__ cen, uint32_t cen_stride,
+                                                     uint32_t chunk0) {
+    constexpr bool MESH = SRC == kSrcMesh;
+    const uint32_t chunk = chunk0 + blockIdx.x;  // this block's chunk of sort tiles
     constexpr int P = kDigits / kThreads;  // digits per thread in the per-tile counts
     __shared__ float4 stage[kWarps][96];
     __shared__ uint32_t hist[kSortPasses][kDigits];
     __shared__ uint32_t th[kDigits];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
+    if (chunk == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
         const uint32_t e = *epoch + 1u;
         *epoch = e == 0u ? 1u : e;
     }
@@ -115,7 +190,7 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
     for (int j = 0; j < P; ++j) acc[j] = 0;
     bool bad = false, bad_index = false;
     for (uint32_t tt = 0; tt < chunk_tiles; ++tt) {
-        const uint32_t tile = blockIdx.x * chunk_tiles + tt;
+        const uint32_t tile = chunk * chunk_tiles + tt;
         if (tile >= tiles) break;  // uniform across the block
         for (int i = threadIdx.x; i < kDigits; i += kThreads) th[i] = 0;
         __syncthreads();
@@ -124,6 +199,12 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
         // while it works on this one (0.179 -> 0.157 ms on 16.7 M triangles)
         float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0, q2 = q0;
         auto ld_row = [&](uint32_t cc) {
+            if constexpr (SRC == kSrcCen) {  // this lane's centroid of the row (x, y, z in q0)
+                const uint32_t t = tile * (uint32_t)kSortTile + 32u * cc + lane;
+                if (t < n) q0 = make_float4(__ldcs(cen + t), __ldcs(cen + cen_stride + t),
+                                            __ldcs(cen + 2ull * cen_stride + t), 0.f);
+                return;
+            }
             const uint64_t base = 3ull * (tile * (uint32_t)kSortTile + 32u * cc);
             const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
             q0 = base + lane < nv ? ld_stream(tri + base + lane) : z;
@@ -153,6 +234,10 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
                 v0 = __ldg(tri + i0);
                 v1 = __ldg(tri + i1);
                 v2 = __ldg(tri + i2);
+            } else if constexpr (SRC == kSrcCen) {
+                v0 = q0;  // the centroid
+                v1 = v2 = v0;
+                if (c + kWarps < (uint32_t)kSortTile / 32 && t0 + 32u * kWarps < n) ld_row(c + kWarps);
             } else {
                 const float4 a0 = q0, a1 = q1, a2 = q2;
                 if (c + kWarps < (uint32_t)kSortTile / 32 && t0 + 32u * kWarps < n) ld_row(c + kWarps);
@@ -166,7 +251,11 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
                 __syncwarp();
             }
             uint32_t key = 0;
-            if (valid) {
+            if (SRC == kSrcCen && valid) {
+                key = morton3(quantise_cen(v0.x, umin[0], umax[0]), quantise_cen(v0.y, umin[1], umax[1]),
+                              quantise_cen(v0.z, umin[2], umax[2]));
+                keys[t] = key;
+            } else if (valid) {
                 bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
                 // box.min = min(v0, min(v1, v2)); box.max = max(v0, max(v1, v2))   (:186-187)
                 const uint32_t qx = quantise(fminf(v0.x, fminf(v1.x, v2.x)), fmaxf(v0.x, fmaxf(v1.x, v2.x)), umin[0], umax[0]);
@@ -198,7 +287,7 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
         }
         __syncthreads();
     }
-    uint32_t *crow = chunk_sum + (size_t)blockIdx.x * kDigits + threadIdx.x * P;
+    uint32_t *crow = chunk_sum + (size_t)chunk * kDigits + threadIdx.x * P;
 #pragma unroll
     for (int j = 0; j < P; ++j) crow[j] = acc[j];
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
@@ -436,8 +525,33 @@ void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s) 
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl, uint32_t *keys,
                    uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
     if (n == 0) return;
-    k_morton<false><<<sort_chunks(n), kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch, sort_chunk_tiles(n),
-                                                        sort_scratch, sort_chunk_sums(sort_scratch, n), nullptr, 0u);
+    launch_morton_chunks(tri, n, hb, ctl, keys, epoch, sort_scratch, 0, sort_chunks(n), s);
+}
+
+void launch_morton_chunks(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl, uint32_t *keys,
+                          uint32_t *epoch, uint32_t *sort_scratch, uint32_t c0, uint32_t c1, cudaStream_t s) {
+    if (n == 0 || c1 <= c0) return;
+    k_morton<kSrcSoup><<<c1 - c0, kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch, sort_chunk_tiles(n),
+                                                    sort_scratch, sort_chunk_sums(sort_scratch, n), nullptr, 0u,
+                                                    nullptr, 0u, c0);
+}
+
+void launch_bounds_cen(const float4 *tri, uint32_t t0, uint32_t t1, float *cen, uint32_t cen_stride,
+                       Control *ctl, cudaStream_t s) {
+    if (t1 <= t0) return;
+    uint32_t blocks = (t1 - t0 + 32u * kWarps - 1) / (32u * kWarps);
+    const uint32_t cap = (uint32_t)sm_count() * 8u;
+    if (blocks > cap) blocks = cap;
+    k_bounds_cen<<<blocks, kThreads, 0, s>>>(tri, t0, t1, cen, cen_stride, ctl);
+}
+
+void launch_morton_cen(const float *cen, uint32_t cen_stride, uint32_t n, Control *ctl, uint32_t *keys,
+                       uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
+    if (n == 0) return;
+    k_morton<kSrcCen><<<sort_chunks(n), kThreads, 0, s>>>(nullptr, n, HostBounds{}, ctl, keys, epoch,
+                                                          sort_chunk_tiles(n), sort_scratch,
+                                                          sort_chunk_sums(sort_scratch, n), nullptr, 0u, cen,
+                                                          cen_stride, 0u);
 }
 
 void launch_bounds_mesh(const float4 *verts, uint32_t nverts, const uint32_t *idx3, uint32_t n, Control *ctl,
@@ -452,8 +566,9 @@ void launch_bounds_mesh(const float4 *verts, uint32_t nverts, const uint32_t *id
 void launch_morton_mesh(const float4 *verts, uint32_t nverts, const uint32_t *idx3, uint32_t n, HostBounds hb,
                         Control *ctl, uint32_t *keys, uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
     if (n == 0) return;
-    k_morton<true><<<sort_chunks(n), kThreads, 0, s>>>(verts, n, hb, ctl, keys, epoch, sort_chunk_tiles(n),
-                                                       sort_scratch, sort_chunk_sums(sort_scratch, n), idx3, nverts);
+    k_morton<kSrcMesh><<<sort_chunks(n), kThreads, 0, s>>>(verts, n, hb, ctl, keys, epoch, sort_chunk_tiles(n),
+                                                           sort_scratch, sort_chunk_sums(sort_scratch, n), idx3,
+                                                           nverts, nullptr, 0u, 0u);
 }
 
 void launch_leaf_idx(const uint32_t *idx3, const uint32_t *perm, uint32_t n, uint32_t *sidx, cudaStream_t s) {

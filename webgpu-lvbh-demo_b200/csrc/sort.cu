@@ -15,8 +15,9 @@
 //     are numbered by an atomic counter in launch order, each publishes its counts (flag
 //     AGGREGATE) and then its inclusive prefix (flag PREFIX) in one 32-bit word per digit, and
 //     looks back only at tiles that have already started, so the waits always end;
-//   * every wait is bounded (kSpinLimitCycles); past it the kernel records ERR_LOOKBACK_TIMEOUT
-//     and carries on, so it never hangs;
+//   * every wait is bounded (kSpinLimitCycles, or the control block's test bound); past it the
+//     kernel records ERR_LOOKBACK_TIMEOUT and carries on, so it never hangs, and the tree
+//     kernels that follow in a build see the flag and build nothing from the unfinished sort;
 //   * keys and values are staged in digit order in shared memory and written out so that
 //     consecutive threads write consecutive addresses of each digit's run.
 //
@@ -123,6 +124,9 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) S.tile = atomicAdd(&ctl->tile_counter[pass], 1u);
+    // test hook words (zero in normal use): a tile that publishes nothing, the wait bound
+    const uint32_t stall1 = ctl->test_stall_tile1;
+    const long long spin_limit = ctl->test_spin_limit ? (long long)ctl->test_spin_limit : kSpinLimitCycles;
     for (int i = tid; i < W * D / 2; i += T) reinterpret_cast<uint32_t *>(&S.whist[0][0])[i] = 0;
     __syncthreads();
     const uint32_t tile = S.tile;
@@ -189,8 +193,10 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
     // tile), so that later tiles can look back past it while it stages its keys.
     uint32_t *lb = lookback + (size_t)tile * D + tid * P;
     const bool first = tile == sp.first;
+    const bool publish = tile + 1u != stall1;
 #pragma unroll
-    for (int j = 0; j < P; ++j) st_relaxed_gpu(lb + j, (first ? kFlagPrefix : kFlagAgg) | cnt[j]);
+    for (int j = 0; j < P; ++j)
+        if (publish) st_relaxed_gpu(lb + j, (first ? kFlagPrefix : kFlagAgg) | cnt[j]);
 
     // The tile's start of each digit in the staging buffer (exclusive scan of its counts).
     uint32_t tst[P], tsum = 0;
@@ -258,7 +264,7 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
             }
             if (done == kAll || !stalled) continue;
             if (!timed) { t0 = clock64(); timed = true; }
-            else if (clock64() - t0 > kSpinLimitCycles ||
+            else if (clock64() - t0 > spin_limit ||
                      (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT)) {
                 // give up; once one wait has timed out every other one gives up at once
                 atomicOr(&ctl->err, ERR_LOOKBACK_TIMEOUT);
@@ -267,7 +273,8 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
             __nanosleep(20);
         }
 #pragma unroll
-        for (int j = 0; j < P; ++j) st_relaxed_gpu(lb + j, kFlagPrefix | ((excl[j] + cnt[j]) & kCountMask));
+        for (int j = 0; j < P; ++j)
+            if (publish) st_relaxed_gpu(lb + j, kFlagPrefix | ((excl[j] + cnt[j]) & kCountMask));
     }
 
     // Global start of each digit: exclusive scan of the pass's counts.

@@ -118,6 +118,8 @@ def _load():
     L.lvbh_copy_to_host.argtypes = [vp, vp, vp, ctypes.c_size_t, vp]
     L.lvbh_sort_pairs_noalloc.restype = i32
     L.lvbh_sort_pairs_noalloc.argtypes = [vp, u32, vp, vp, vp]
+    L.lvbh_test_stall_lookback.restype = i32
+    L.lvbh_test_stall_lookback.argtypes = [vp, u32, u32]
     L.lvbh_server_create.restype = i32
     L.lvbh_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ServerConfig)]
     L.lvbh_server_destroy.restype = None
