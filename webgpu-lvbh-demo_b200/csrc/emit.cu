@@ -158,7 +158,11 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
     const int nblk = segs.blocks();
     const uint32_t lt = lanemask_lt();
 
-    // two blocks ahead: this thread's permutation entry (its three vertex indices for a mesh)
+    // Leaves come in three steps ahead of their block: this thread's permutation entry (its three
+    // vertex indices for a mesh) three blocks ahead, its triangle copied into S.tri two blocks
+    // ahead, its key one block ahead.  Two buffers, S.tri[0] and S.tri[1], serve the copies two
+    // blocks ahead: a block's buffer is refilled right after its own leaf phase has read it, so
+    // the copies of two blocks are in flight while a block climbs.
     uint32_t pa = 0, pb = 0, pc = 0;
     auto fetch_perm = [&](int blk) {
         const Span sp = segs.span(blk);
@@ -173,19 +177,15 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             }
         }
     };
-    // one block ahead: its span, this thread's key and triangle (into S.tri[buf]), edge keys
-    Span nsp{0, 0, 0};
-    uint32_t nk = 0, nk_lo = 0, nk_hi = 0;
     bool bad_perm = false;
-    auto fetch_leaf = [&](int blk, int buf) {
-        nsp = segs.span(blk);
-        const uint32_t *keys = keys_all + nsp.start;
-        const int b0 = nsp.b0, n = nsp.n, k = b0 + t;
-        // soup: the phase expects 48 bytes per leaf of the block; thread 0's arrival is its only
-        // one.  Mesh: the vertex rows (mostly in L2) come by cp.async.
+    // the block's triangles into S.tri[buf].  Soup: one 48-byte bulk copy per leaf on the buffer's
+    // mbarrier, whose phase expects 48 bytes per leaf of the block (thread 0's arrival is its
+    // only one).  Mesh: the vertex rows (mostly in L2) by cp.async, one commit group per block.
+    auto fetch_tri = [&](int blk, int buf) {
+        const Span sp = segs.span(blk);
+        const int b0 = sp.b0, n = sp.n, k = b0 + t;
         if (!Leaves::kMesh && t == 0) mbar_arrive_tx(&S.bar[buf], 48u * (uint32_t)min(EB, n - b0));
         if (k < n) {
-            nk = __ldg(keys + k);
             if constexpr (Leaves::kMesh) {
                 // an index past the vertex buffer was reported by the Morton pass; read row 0
                 const uint32_t nv = lv.nverts;
@@ -195,12 +195,30 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             } else {
                 uint32_t ti = pa;
                 if (ti >= (uint32_t)n) { bad_perm = true; ti = 0; }
-                bulk_g2s(&S.tri[buf][t][0], lv.tri + 3ull * (nsp.start + ti), 48u, &S.bar[buf]);
+                bulk_g2s(&S.tri[buf][t][0], lv.tri + 3ull * (sp.start + ti), 48u, &S.bar[buf]);
             }
         }
         if constexpr (Leaves::kMesh) cp_async_commit();
+    };
+    // one block ahead: its span, this thread's key, the keys on either side of the block
+    Span nsp{0, 0, 0};
+    uint32_t nk = 0, nk_lo = 0, nk_hi = 0;
+    auto fetch_keys = [&](int blk) {
+        nsp = segs.span(blk);
+        const uint32_t *keys = keys_all + nsp.start;
+        const int b0 = nsp.b0, n = nsp.n, k = b0 + t;
+        if (k < n) nk = __ldg(keys + k);
         if (t == 0) nk_lo = b0 > 0 ? __ldg(keys + b0 - 1) : 0u;
         if (t == EB - 1) nk_hi = (b0 + EB < n) ? __ldg(keys + b0 + EB) : 0u;
+    };
+    const int grid = (int)gridDim.x;
+    // after every thread has read S.tri[buf] (a barrier between): refill it with the block two
+    // ahead, and load the permutation three ahead
+    auto refill = [&](int blk, int buf) {
+        if (blk + 2 * grid >= nblk) return;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // reads above, copies below
+        fetch_tri(blk + 2 * grid, buf);
+        if (blk + 3 * grid < nblk) fetch_perm(blk + 3 * grid);
     };
     int buf = 0;
     uint32_t phase = 0;  // bit b: parity of the next phase of S.bar[b] (uniform over the block)
@@ -210,11 +228,16 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
     __syncthreads();
     if ((int)blockIdx.x < nblk) {
         fetch_perm(blockIdx.x);
-        fetch_leaf(blockIdx.x, 0);
-        if ((int)(blockIdx.x + gridDim.x) < nblk) fetch_perm(blockIdx.x + gridDim.x);
+        fetch_tri(blockIdx.x, 0);
+        fetch_keys(blockIdx.x);
+        if ((int)blockIdx.x + grid < nblk) {
+            fetch_perm(blockIdx.x + grid);
+            fetch_tri(blockIdx.x + grid, 1);
+            if ((int)blockIdx.x + 2 * grid < nblk) fetch_perm(blockIdx.x + 2 * grid);
+        }
     }
 
-    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x, buf ^= 1) {
+    for (int blk = blockIdx.x; blk < nblk; blk += grid, buf ^= 1) {
         const Span sp = nsp;
         const int b0 = sp.b0, n = sp.n;
         float4 *nodes = nodes_all + 4ull * sp.start;
@@ -233,7 +256,9 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         // this leaf's triangle: to the output soup, and its box (exact-zero components nudged
         // by 1e-8 as bvh-up-pass.js:209-210 does)
         if constexpr (Leaves::kMesh) {
-            cp_async_wait_all();
+            // the next block's group may still be in flight (the newest one), not this one's
+            if (blk + grid < nblk) asm volatile("cp.async.wait_group 1;" ::: "memory");
+            else cp_async_wait_all();
         } else {
             if (!mbar_wait(&S.bar[buf], (phase >> buf) & 1u)) copy_timeout = true;
             phase ^= 1u << buf;
@@ -255,10 +280,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             leaf_lo = make_float4(nx, ny, nz, __int_as_float(-(k + 1)));
             leaf_hi0 = make_float4(xx, xy, xz, 0.f);
         }
-        if (blk + (int)gridDim.x < nblk) {
-            fetch_leaf(blk + gridDim.x, buf ^ 1);
-            if (blk + 2 * (int)gridDim.x < nblk) fetch_perm(blk + 2 * gridDim.x);
-        }
+        if (blk + grid < nblk) fetch_keys(blk + grid);
         if (n == 1) {  // one leaf, one arrival at node 0: left slot only, f_1 = 1
             if (t == 0) {
                 nodes[0] = make_float4(leaf_lo.x, leaf_lo.y, leaf_lo.z, __int_as_float(-1));
@@ -272,6 +294,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             // uniform across the block; no other thread reads what this one wrote.  The barrier
             // keeps every thread's wait on this buffer's phase ahead of its next arming.
             __syncthreads();
+            refill(blk, buf);
             continue;
         }
         if (k == 0) {  // the root has no parent; slot N-1 and record N-1 stay zero
@@ -281,7 +304,8 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             float4 *last = nodes + 4ull * (n - 1);
             last[0] = z; last[1] = z; last[2] = z; last[3] = z;
         }
-        __syncthreads();
+        __syncthreads();  // every thread has waited on and read S.tri[buf]: it may be refilled
+        refill(blk, buf);
         auto dval = [&](int x) -> int {  // d of split b0 + x, x in [-1, EB - 1]
             const int g = b0 + x;
             if (g < 0 || g >= n - 1) return -1;

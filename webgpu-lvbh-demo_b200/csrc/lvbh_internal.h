@@ -66,6 +66,8 @@ struct __align__(16) OpenItem {
     int xl, xr, pad0, pad1;  // pad0: d[xl - 1]
 };
 
+constexpr int kHistParts = 16;
+
 // Per-build control block in device memory.  Everything from `err` on is zeroed by one memset
 // at the start of a build; `aux_err` collects errors of steps that run before that memset (the
 // indexed-mesh gather) and is cleared by the host before them.  The two test words at the front
@@ -83,6 +85,10 @@ struct Control {
     uint32_t bounds_ord[6];   // scene min (ord_hi) and max (ord_lo), see lvbh_device.cuh
     uint32_t pad1[2];
     uint32_t hist[kHistWords];  // global digit counts of the unsorted keys, pass-major
+    // The plain build's global digit counts in kHistParts partial rows per pass: each per-chunk
+    // block adds its chunk's counts into row (chunk % kHistParts), so that hundreds of blocks
+    // finishing together do not queue on one address per digit; the chunk scan sums the rows.
+    uint32_t hist_part[kSortPasses][kHistParts][kDigits];
 };
 
 struct HostBounds {
@@ -118,8 +124,8 @@ size_t ctx_device_bytes(const lvbh_ctx *ctx);
 
 // K1a: scene box over every vertex of the 48-byte triangle soup.
 void launch_bounds(const float4 *tri, uint32_t n, Control *ctl, cudaStream_t s);
-// K1b: triangle box centroid -> Morton key (input order), the global digit counts of all
-// three sort passes and the first pass's tile histograms and chunk sums (sort_scratch); flags
+// K1b: triangle box centroid -> Morton key (input order), the first sort pass's tile
+// histograms, chunk sums (sort_scratch) and global digit counts (ctl->hist_part, zero before); flags
 // non-finite vertices in ctl->err and advances the build epoch *epoch used by K3c.
 void launch_morton(const float4 *tri, uint32_t n, HostBounds hb, Control *ctl,
                    uint32_t *keys_out, uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s);
@@ -134,9 +140,10 @@ void launch_bounds_cen(const float4 *tri, uint32_t t0, uint32_t t1, float *cen, 
                        Control *ctl, cudaStream_t s);
 void launch_morton_cen(const float *cen, uint32_t cen_stride, uint32_t n, Control *ctl, uint32_t *keys,
                        uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s);
-// K2: one reduce-then-scan pass over 10-bit digit `pass` (0..2) of 30-bit keys (the global
-// digit counts come from ctl->hist).  counted: the tile histograms and chunk sums of this
-// pass are already in scratch (K1b writes those of pass 0).  vals_in == nullptr generates the
+// K2: one reduce-then-scan pass over 10-bit digit `pass` (0..2) of 30-bit keys.  counted: the
+// tile histograms, chunk sums and global digit counts (ctl->hist_part) of this pass are there
+// already (K1b makes those of pass 0); otherwise the pass's tile-histogram kernel makes them
+// (ctl->hist_part of the pass zero before).  vals_in == nullptr generates the
 // identity.  scratch: sort_scratch_words(n) words, no initialisation needed.
 size_t sort_scratch_words(uint32_t n);
 void launch_sort_pass(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,

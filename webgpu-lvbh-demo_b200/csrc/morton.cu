@@ -148,8 +148,8 @@ __global__ void __launch_bounds__(kThreads) k_bounds_cen(const float4 *__restric
 // reads row 0 and sets ERR_BAD_INDEX.  kSrcCen: the centroids K1a stored (structure of arrays,
 // `cen_stride` floats apart), quantised with the device-reduced box; K1a checked the vertices.
 constexpr int kSrcSoup = 0, kSrcMesh = 1, kSrcCen = 2;
-template <int SRC>
-__global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ tri, uint32_t n,
+template <int SRC, int THREADS = kThreads>
+__global__ void __launch_bounds__(THREADS) k_morton(const float4 *__restrict__ tri, uint32_t n,
                                                      HostBounds hb, Control *__restrict__ ctl,
                                                      uint32_t *__restrict__ keys,
                                                      uint32_t *__restrict__ epoch, uint32_t chunk_tiles,
@@ -160,15 +160,14 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
                                                      uint32_t chunk0) {
     constexpr bool MESH = SRC == kSrcMesh;
     const uint32_t chunk = chunk0 + blockIdx.x;  // this block's chunk of sort tiles
-    constexpr int P = kDigits / kThreads;  // digits per thread in the per-tile counts
-    __shared__ float4 stage[kWarps][96];
-    __shared__ uint32_t hist[kSortPasses][kDigits];
+    constexpr int P = kDigits / THREADS;  // digits per thread in the per-tile counts
+    constexpr int WARPS = THREADS / 32;
+    __shared__ float4 stage[SRC == kSrcSoup ? WARPS : 1][96];
     __shared__ uint32_t th[kDigits];
     if (chunk == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
         const uint32_t e = *epoch + 1u;
         *epoch = e == 0u ? 1u : e;
     }
-    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) (&hist[0][0])[i] = 0;
 
     float umin[3], umax[3];
     if (hb.use) {
@@ -192,7 +191,7 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
     for (uint32_t tt = 0; tt < chunk_tiles; ++tt) {
         const uint32_t tile = chunk * chunk_tiles + tt;
         if (tile >= tiles) break;  // uniform across the block
-        for (int i = threadIdx.x; i < kDigits; i += kThreads) th[i] = 0;
+        for (int i = threadIdx.x; i < kDigits; i += THREADS) th[i] = 0;
         __syncthreads();
         bool coherent = false;
         // soup: a warp's next row of 32 triangles (three coalesced float4 per lane) is loaded
@@ -212,7 +211,7 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
             q2 = base + 64 + lane < nv ? ld_stream(tri + base + 64 + lane) : z;
         };
         if (!MESH && tile * (uint32_t)kSortTile + 32u * warp < n) ld_row(warp);
-        for (uint32_t c = warp; c < (uint32_t)kSortTile / 32; c += kWarps) {
+        for (uint32_t c = warp; c < (uint32_t)kSortTile / 32; c += WARPS) {
             const uint32_t t0 = tile * (uint32_t)kSortTile + 32u * c;
             if (t0 >= n) break;
             const uint32_t t = t0 + lane;
@@ -237,10 +236,10 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
             } else if constexpr (SRC == kSrcCen) {
                 v0 = q0;  // the centroid
                 v1 = v2 = v0;
-                if (c + kWarps < (uint32_t)kSortTile / 32 && t0 + 32u * kWarps < n) ld_row(c + kWarps);
+                if (c + WARPS < (uint32_t)kSortTile / 32 && t0 + 32u * WARPS < n) ld_row(c + WARPS);
             } else {
                 const float4 a0 = q0, a1 = q1, a2 = q2;
-                if (c + kWarps < (uint32_t)kSortTile / 32 && t0 + 32u * kWarps < n) ld_row(c + kWarps);
+                if (c + WARPS < (uint32_t)kSortTile / 32 && t0 + 32u * WARPS < n) ld_row(c + WARPS);
                 stage[warp][lane] = a0;
                 stage[warp][32 + lane] = a1;
                 stage[warp][64 + lane] = a2;
@@ -264,18 +263,11 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
                 key = morton3(qx, qy, qz);
                 keys[t] = key;
             }
-            // coherent input (a mesh in its file order) shares the top digit over long runs;
+            // repeated digits over consecutive lanes (coherent input) are counted once per run;
             // the warp tests its first chunk of each tile and keeps the answer for the tile
-            if (c == (uint32_t)warp) coherent = runs_few(key >> (kDigitBits * (kSortPasses - 1)), valid);
-            if (coherent) {
-#pragma unroll
-                for (int p = 0; p < kSortPasses; ++p) add_runs(hist[p], (key >> (kDigitBits * p)) & (kDigits - 1), valid);
-                add_runs(th, key & (kDigits - 1), valid);
-            } else if (valid) {
-#pragma unroll
-                for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (kDigitBits * p)) & (kDigits - 1)], 1u);
-                atomicAdd(&th[key & (kDigits - 1)], 1u);
-            }
+            if (c == (uint32_t)warp) coherent = runs_few(key & (kDigits - 1), valid);
+            if (coherent) add_runs(th, key & (kDigits - 1), valid);
+            else if (valid) atomicAdd(&th[key & (kDigits - 1)], 1u);
         }
         __syncthreads();
         uint32_t *row = tile_hist + (size_t)tile * kDigits + threadIdx.x * P;
@@ -287,16 +279,16 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float4 *__restrict__ 
         }
         __syncthreads();
     }
+    // the chunk's counts, and its share of the pass's global digit counts (one of the partial
+    // rows; the later passes' counts come from their own tile-histogram pass)
     uint32_t *crow = chunk_sum + (size_t)chunk * kDigits + threadIdx.x * P;
 #pragma unroll
-    for (int j = 0; j < P; ++j) crow[j] = acc[j];
+    for (int j = 0; j < P; ++j) {
+        crow[j] = acc[j];
+        if (acc[j]) atomicAdd(&ctl->hist_part[0][chunk % kHistParts][threadIdx.x * P + j], acc[j]);
+    }
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
     if (__any_sync(0xFFFFFFFFu, bad_index) && lane == 0) atomicOr(&ctl->err, ERR_BAD_INDEX);
-    __syncthreads();
-    for (int i = threadIdx.x; i < kSortPasses * kDigits; i += kThreads) {
-        const uint32_t c = (&hist[0][0])[i];
-        if (c) atomicAdd(ctl->hist + i, c);
-    }
 }
 
 // K1a for a mesh: min / max over the vertices the triangles use (the rows of unused vertices
@@ -548,7 +540,8 @@ void launch_bounds_cen(const float4 *tri, uint32_t t0, uint32_t t1, float *cen, 
 void launch_morton_cen(const float *cen, uint32_t cen_stride, uint32_t n, Control *ctl, uint32_t *keys,
                        uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
     if (n == 0) return;
-    k_morton<kSrcCen><<<sort_chunks(n), kThreads, 0, s>>>(nullptr, n, HostBounds{}, ctl, keys, epoch,
+    // 512 threads: the chunks (two per SM) fill the GPU with one wave of 16-warp blocks
+    k_morton<kSrcCen, 512><<<sort_chunks(n), 512, 0, s>>>(nullptr, n, HostBounds{}, ctl, keys, epoch,
                                                           sort_chunk_tiles(n), sort_scratch,
                                                           sort_chunk_sums(sort_scratch, n), nullptr, 0u, cen,
                                                           cen_stride, 0u);

@@ -6,7 +6,8 @@
 // and this pass keeps that contract.  The build's keys have 30 bits, sorted in three passes of
 // 10-bit digits; full 32-bit keys (the allocation-free entry point) take four 8-bit passes.
 //
-//   * the global digit counts of every pass come from K1b's histograms (one read of the keys);
+//   * the global digit counts of a pass are summed by its tile-histogram kernel (pass 0's by the
+//     Morton kernel, which writes pass 0's tile histograms with the keys);
 //   * a tile of 4096 keys (256 threads x 16) is ranked in shared memory: each warp walks its
 //     keys in input order; the lanes holding the same digit (its peers) are found with one
 //     ballot per digit bit, and the peers' lane order plus a per-warp running count in a
@@ -213,7 +214,8 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
     }
     __syncthreads();
 
-    // Stage keys and values in digit order.
+    // Stage keys and values in digit order (values by 4-byte asynchronous copies, in flight
+    // during the look-back).
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
         const uint32_t idx = wbase + i * 32 + lane;
@@ -221,9 +223,11 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
             const uint32_t d = (k[i] >> shift) & (D - 1);
             const uint32_t pos = S.whist[warp][d] + ((rank[i / 2] >> (16 * (i & 1))) & 0xFFFFu);
             S.keys[pos] = k[i];
-            S.vals[pos] = vals_in ? __ldcs(vals_in + idx) : idx;
+            if (vals_in) cp_async4(&S.vals[pos], vals_in + idx);
+            else S.vals[pos] = idx;
         }
     }
+    cp_async_commit();
 
     // Decoupled look-back across tiles, all P digits together: read kLookback predecessors
     // per digit at a time (independent loads), add their counts newest first until a PREFIX.
@@ -287,6 +291,7 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
         S.out[tid * P + j] = gbase + excl[j] - tst[j];
         gbase += g[j];
     }
+    cp_async_wait_all();
     __syncthreads();
 
     const uint32_t tile_n = min((uint32_t)kSortTile, n - tile_base);
@@ -306,11 +311,13 @@ __global__ void __launch_bounds__(T, 4) k_onesweep(Segs segs, const uint32_t *__
 
 
 // Reduce: digit counts of every tile (tile_hist[tile][digit]) and of every chunk of chunk_tiles
-// tiles (chunk_sum[chunk][digit]).  One block per chunk; each thread owns P contiguous digits.
+// tiles (chunk_sum[chunk][digit]), added up into the pass's global counts (ghist: kHistParts
+// partial rows, zero before; the chunk goes to row chunk % kHistParts).  One block per chunk;
+// each thread owns P contiguous digits.
 template <int BITS>
 __global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ keys, uint32_t n, int pass,
                                                  uint32_t chunk_tiles, uint32_t *__restrict__ tile_hist,
-                                                 uint32_t *__restrict__ chunk_sum) {
+                                                 uint32_t *__restrict__ chunk_sum, uint32_t *__restrict__ ghist) {
     constexpr int D = 1 << BITS, P = D / T;
     __shared__ __align__(16) uint32_t h[D];
     const int tid = threadIdx.x, shift = pass * BITS;
@@ -351,11 +358,15 @@ __global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ ke
     }
     uint32_t *row = chunk_sum + (size_t)blockIdx.x * D + tid * P;
 #pragma unroll
-    for (int j = 0; j < P; ++j) row[j] = acc[j];
+    for (int j = 0; j < P; ++j) {
+        row[j] = acc[j];
+        if (acc[j]) atomicAdd(ghist + (blockIdx.x % kHistParts) * D + tid * P + j, acc[j]);
+    }
 }
 
 // Scan: chunk_off[c][d] = start of digit d in the pass's output (exclusive scan of the global
-// counts ghist over digits) + counts of digit d in chunks before c.  Block b covers digits
+// counts over digits, the kHistParts partial rows of ghist summed) + counts of digit d in chunks
+// before c.  Block b covers digits
 // 32b .. 32b+31 (lane = digit); its 32 warps split the chunks.
 constexpr int kScanThreads = 1024;
 template <int BITS>
@@ -370,7 +381,9 @@ __global__ void __launch_bounds__(kScanThreads) k_chunk_scan(const uint32_t *__r
     __shared__ uint32_t s_part[SW][32];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // digit starts: exclusive scan of the global counts, one digit per thread
-    const uint32_t g = __ldg(ghist + tid);
+    uint32_t g = 0;
+#pragma unroll
+    for (int r = 0; r < kHistParts; ++r) g += __ldg(ghist + r * D + tid);
     uint32_t incl = g;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -497,6 +510,9 @@ __global__ void __launch_bounds__(T, 4) k_scatter(const uint32_t *__restrict__ k
     }
     __syncthreads();
 
+    // the values go straight from global memory to their staged slots by 4-byte asynchronous
+    // copies: all of a thread's copies are in flight at once and hold no registers (loads
+    // followed by shared stores waited for each value in turn)
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
         const uint32_t idx = wbase + i * 32 + lane;
@@ -504,9 +520,12 @@ __global__ void __launch_bounds__(T, 4) k_scatter(const uint32_t *__restrict__ k
             const uint32_t d = (k[i] >> shift) & (D - 1);
             const uint32_t pos = S.whist[warp][d] + ((rank[i / 2] >> (16 * (i & 1))) & 0xFFFFu);
             S.keys[pos] = k[i];
-            S.vals[pos] = vals_in ? __ldcs(vals_in + idx) : idx;
+            if (vals_in) cp_async4(&S.vals[pos], vals_in + idx);
+            else S.vals[pos] = idx;
         }
     }
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
 
     const uint32_t tile_n = min((uint32_t)kSortTile, n - tile_base);
@@ -561,9 +580,10 @@ void launch_sort_pass(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t
     uint32_t *chunk_sum = sort_chunk_sums(scratch, n);
     uint32_t *chunk_off = chunk_sum + (size_t)chunks * kDigits;
     const uint32_t ct = sort_chunk_tiles(n);
-    if (!counted) k_tile_hist<kDigitBits><<<chunks, T, 0, s>>>(keys_in, n, pass, ct, tile_hist, chunk_sum);
-    k_chunk_scan<kDigitBits><<<kDigits / 32, kScanThreads, 0, s>>>(chunk_sum, chunks,
-                                                                   ctl->hist + pass * kDigits, chunk_off);
+    uint32_t *ghist = &ctl->hist_part[pass][0][0];
+    if (!counted)
+        k_tile_hist<kDigitBits><<<chunks, T, 0, s>>>(keys_in, n, pass, ct, tile_hist, chunk_sum, ghist);
+    k_chunk_scan<kDigitBits><<<kDigits / 32, kScanThreads, 0, s>>>(chunk_sum, chunks, ghist, chunk_off);
     k_scatter<kDigitBits><<<tiles, T, sizeof(SortSmem<kDigitBits>), s>>>(
         keys_in, vals_in, keys_out, vals_out, n, pass, tile_hist, chunk_off, ct, ctl);
 }
