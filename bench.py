@@ -4,9 +4,9 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload clustered16M|sphere2M|uniform64K]
 
-One step = one complete build (scene box, Morton keys, 4-pass onesweep sort, and one pass that
-emits the radix tree, gathers and rearranges the triangles and refits the boxes) of the
-workload's triangle soup.  Default workload: the 16,777,216-triangle
+One step = one complete build (scene box and centroids, Morton keys, the three-pass stable radix
+sort, one pass that emits the radix tree, gathers and rearranges the triangles and refits the
+boxes, and the pass over the nodes that straddle its blocks) of the workload's triangle soup.  Default workload: the 16,777,216-triangle
 Gaussian-mixture scene (seeded synthetic data; the reference publishes no scene set).  The
 805 MB input soup is larger than the 126 MB L2, so steps run back to back without a flush.
 
@@ -14,13 +14,16 @@ Prints one JSON line (rank 0).  Fields beyond the base contract:
   roofline      dominant kernel's algorithmic bytes / its CUDA-event duration vs measured HBM
   stage_ms      per-stage device times (CUDA events on the build stream, profiled steps)
   cpu_baseline  the CPU restatement of the reference build timed on this host's cores
-  e2e           through the public C ABI from pinned host memory: H2D of the soup, the build,
-                D2H of the root node record, every step
+  e2e           through the public C ABI from pinned host memory: H2D of the soup (in chunks,
+                each chunk's first pass behind the copy of the next), the build, D2H of the root
+                node record, every step; also with host bounds, and the bare upload for scale
   batched       the 4096-mesh batch (log-uniform 64..262,144 triangles per mesh) built by one
                 lvbh_build_batched call vs the plain builder called once per mesh, identical trees
-  served        the build server under Poisson arrivals at 200..5000 requests/s (sizes
-                log-uniform in 1,024..4,194,304): p50/p99/p99.9 latency and builds/s beside the
-                plain per-request builder on the same arrival trace (1 GPU only)
+  served        the build server under Poisson arrivals, 100,000 requests per rate (sizes
+                log-uniform in 1,024..4,194,304, each request its own window of a seeded clustered
+                soup; device-resident inputs at 2000 and 5000 req/s, pinned host inputs uploaded
+                inside the latency at 2000 req/s): p50/p99/p99.9 latency, batch sizes and
+                builds/s beside the plain per-request builder on the same trace (1 GPU only)
   trace         closest-hit traversal of 4,194,304 rays through the built 2M-triangle sphere
   obj           OBJ ingest: the sphere's 80 MB OBJ text -> soup + bounds on the GPU, and end to
                 end through parse + build from pinned host text, beside the oracle's parse
@@ -56,12 +59,14 @@ UNIT = "Mprims/s"
 # pass 1 read 4 write 8, passes 2-3 read 8 write 8); leaf gather perm 4 + gather 48 + write 48
 # and tree keys 4 + parents 8 + child links 8 + node words 56 + parent reads 8 + flag atomics 8,
 # both done by the one tree-pass kernel (the gather stage is fused into it).  The
-# straddling-node pass completes part of the same tree and has no bytes of its own.
+# straddling-node pass completes part of the same tree and has no bytes of its own.  The model
+# is fixed; the build moves less in its first two stages (box and centroids: read 48, write 12;
+# keys from the centroids: read 12, write 4 - 76 bytes where the model counts 100).
 MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "gather": 0, "tree": 192, "top": 0}
-KERNELS = {"bounds": ("k_bounds", 1), "morton": ("k_morton", 1), "sort": ("k_scatter", 3),
+KERNELS = {"bounds": ("k_bounds_cen", 1), "morton": ("k_morton", 1), "sort": ("k_scatter", 3),
            "gather": (None, 0), "tree": ("k_tree_climb", 1), "top": ("k_emit_top", 2)}
-# bounds, morton (+ the first pass's tile histograms), 3 sort passes x (chunk scan, scatter) and
-# 2 tile-histogram passes, tree, straddling pass in two levels (group, global)
+# box and centroids, Morton keys (+ the first pass's tile histograms), 3 sort passes x (chunk
+# scan, scatter) and 2 tile-histogram passes, tree, straddling pass in two levels (group, global)
 LAUNCHES_PER_BUILD = 13
 MODEL_TOTAL = sum(MODEL_BYTES.values())  # 340 B per triangle
 

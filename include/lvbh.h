@@ -84,7 +84,7 @@ extern "C" {
 
 /* Stage indices for lvbh_stage_times(). */
 #define LVBH_STAGE_UPLOAD  0  /* host->device copy of the input (LVBH_INPUT_HOST only) */
-#define LVBH_STAGE_BOUNDS  1  /* scene box reduction (skipped when bounds are supplied) */
+#define LVBH_STAGE_BOUNDS  1  /* scene box reduction with the triangle centroids (skipped when bounds are supplied) */
 #define LVBH_STAGE_MORTON  2  /* triangle centroid -> 30-bit Morton key + digit histograms */
 #define LVBH_STAGE_SORT    3  /* stable LSD radix sort of (key, triangle index) */
 #define LVBH_STAGE_GATHER  4  /* empty: the leaf gather runs inside the tree stage */
@@ -306,7 +306,7 @@ LVBH_API const char *lvbh_server_last_error(const lvbh_server *srv);
  *   stream    cudaStream_t or NULL; the call returns once the sort has finished
  * All other memory (ping-pong keys and values, histograms, look-back words, error word) is one
  * file-scope device array inside the library, sized for LVBH_NOALLOC_MAX_KEYS keys (about
- * 9.5 MB, held by every GPU that loads the library until the process exits); larger inputs are
+ * 9.6 MB, held by every GPU that loads the library until the process exits); larger inputs are
  * rejected with LVBH_ERANGE before any GPU work.  The first call on each device looks up that
  * array's device address (cudaGetSymbolAddress, with the device current); make it before any
  * stream capture.  Calls share the array: two calls that overlap on the GPU (unordered

@@ -349,3 +349,27 @@ def test_chunked_host_upload(builder):
     for tag in ("pinned", "pinned, replayed"):
         _, got = build_np(builder, pinned.numpy(), host=True)
         assert_same(got, ref, tag)
+
+
+def test_caller_outputs_one_element_off_16_bytes(builder):
+    """Caller-provided result buffers need 16-byte alignment only for nodes and tris; parents,
+    leaf_index and morton may start anywhere 4-byte aligned, as slices of a larger buffer do
+    when meshes are built one by one into it.  With those three one element past a 16-byte
+    boundary (and in the sort's ping-pong, where leaf_index is read back as the values of the
+    second pass) the build stays bit-exact."""
+    import torch
+    import oracle
+    from lvbh import scenes
+    n = 70_001
+    tri = scenes.clustered_soup(n, seed=31)
+    dev = torch.device("cuda")
+    outs = {"nodes": torch.empty((n, 16), dtype=torch.int32, device=dev),
+            "tris": torch.empty((n, 12), dtype=torch.float32, device=dev),
+            "parents": torch.empty(2 * n + 1, dtype=torch.int32, device=dev)[1:],
+            "leaf_index": torch.empty(n + 1, dtype=torch.int32, device=dev)[1:],
+            "morton": torch.empty(n + 3, dtype=torch.int32, device=dev)[3:]}
+    for k in ("parents", "leaf_index", "morton"):
+        assert outs[k].data_ptr() % 16 != 0
+    builder.build_soup(torch.from_numpy(tri).cuda(), None, outputs=outs)
+    got = {k: v.cpu().numpy() for k, v in outs.items()}
+    assert_same(got, oracle.build(tri, None, threads=0), "outputs off 16-byte boundaries")

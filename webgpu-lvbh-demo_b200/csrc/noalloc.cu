@@ -8,7 +8,7 @@
 // the two output arrays; everything else the sort needs - the ping-pong keys and values, the
 // digit histograms, the decoupled look-back words and the error word - lives in one
 // file-scope device array, g_scratch, sized for kMaxKeys keys.  Every GPU that loads the
-// library holds that array (about 9.5 MB) until the process exits.
+// library holds that array (about 9.6 MB) until the process exits.
 //
 // In host code the name g_scratch is a host-side stand-in, not a device address: handing it
 // to a kernel would fault, or silently use the wrong memory where the GPU can reach host
