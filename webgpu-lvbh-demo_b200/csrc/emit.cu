@@ -178,13 +178,19 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         }
     };
     bool bad_perm = false;
-    // the block's triangles into S.tri[buf].  Soup: one 48-byte bulk copy per leaf on the buffer's
-    // mbarrier, whose phase expects 48 bytes per leaf of the block (thread 0's arrival is its
-    // only one).  Mesh: the vertex rows (mostly in L2) by cp.async, one commit group per block.
+    // The block's triangles into S.tri[buf].  Soup: the leaves of the first three quarters of the
+    // warps by one 48-byte bulk copy each (the copy engine) on the buffer's mbarrier, whose phase
+    // expects their bytes (thread 0's arrival is its only one); the last quarter's by three
+    // 16-byte cp.async each (the load/store unit), waited for by each such thread on its own.
+    // The copy engine takes about one small copy per 17 cycles per SM, which the whole gather
+    // saturates (a thread stalled ~4,600 cycles per block issuing its copy); a quarter of the
+    // leaves on the other path keeps both busy (tree pass 1.04 -> 0.98 ms on 16.7 M).  Mesh: the
+    // vertex rows (mostly in L2) by cp.async.  One commit group per thread and block.
+    constexpr int kAsyncFrom = EB - EB / 4;  // first thread of the cp.async quarter (whole warps)
     auto fetch_tri = [&](int blk, int buf) {
         const Span sp = segs.span(blk);
         const int b0 = sp.b0, n = sp.n, k = b0 + t;
-        if (!Leaves::kMesh && t == 0) mbar_arrive_tx(&S.bar[buf], 48u * (uint32_t)min(EB, n - b0));
+        if (!Leaves::kMesh && t == 0) mbar_arrive_tx(&S.bar[buf], 48u * (uint32_t)min(min(EB, n - b0), kAsyncFrom));
         if (k < n) {
             if constexpr (Leaves::kMesh) {
                 // an index past the vertex buffer was reported by the Morton pass; read row 0
@@ -195,10 +201,17 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             } else {
                 uint32_t ti = pa;
                 if (ti >= (uint32_t)n) { bad_perm = true; ti = 0; }
-                bulk_g2s(&S.tri[buf][t][0], lv.tri + 3ull * (sp.start + ti), 48u, &S.bar[buf]);
+                const float4 *src = lv.tri + 3ull * (sp.start + ti);
+                if (t >= kAsyncFrom) {
+                    cp_async16(&S.tri[buf][t][0], src);
+                    cp_async16(&S.tri[buf][t][1], src + 1);
+                    cp_async16(&S.tri[buf][t][2], src + 2);
+                } else {
+                    bulk_g2s(&S.tri[buf][t][0], src, 48u, &S.bar[buf]);
+                }
             }
         }
-        if constexpr (Leaves::kMesh) cp_async_commit();
+        cp_async_commit();
     };
     // one block ahead: its span, this thread's key, the keys on either side of the block
     Span nsp{0, 0, 0};
@@ -255,11 +268,12 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         if (t == 0) S.open = 0;
         // this leaf's triangle: to the output soup, and its box (exact-zero components nudged
         // by 1e-8 as bvh-up-pass.js:209-210 does)
-        if constexpr (Leaves::kMesh) {
+        if (Leaves::kMesh || t >= kAsyncFrom) {
             // the next block's group may still be in flight (the newest one), not this one's
             if (blk + grid < nblk) asm volatile("cp.async.wait_group 1;" ::: "memory");
             else cp_async_wait_all();
-        } else {
+        }
+        if constexpr (!Leaves::kMesh) {
             if (!mbar_wait(&S.bar[buf], (phase >> buf) & 1u)) copy_timeout = true;
             phase ^= 1u << buf;
         }
