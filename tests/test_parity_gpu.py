@@ -328,10 +328,11 @@ def oracle_build(tri):
 
 
 def test_chunked_host_upload(builder):
-    """A host soup of 2^21 + 4099 triangles without host bounds is uploaded in chunks, each
-    chunk's box and centroid pass running while the next chunk is copied: bit-exact against the
-    oracle and the device-input build, from pageable and pinned host memory, after an
-    LVBH_ASYNC build that still reads the staging buffer, and again on graph replay."""
+    """A host soup of 2^21 + 4099 triangles is uploaded in chunks, each chunk's first pass (the
+    box and centroids, or with host bounds the Morton keys) running while the next chunk is
+    copied: bit-exact against the oracle and the device-input build, from pageable and pinned
+    host memory, after an LVBH_ASYNC build that still reads the staging buffer, again on graph
+    replay, and with MODEL_BOUNDS wider than the scene."""
     import torch
     from lvbh import scenes
     import oracle
@@ -349,6 +350,15 @@ def test_chunked_host_upload(builder):
     for tag in ("pinned", "pinned, replayed"):
         _, got = build_np(builder, pinned.numpy(), host=True)
         assert_same(got, ref, tag)
+    # with MODEL_BOUNDS the Morton keys of each chunk are made while the next chunk is copied
+    hb = oracle.scene_bounds(tri)
+    hb[:3] -= np.float32(0.25)
+    hb[3:] += np.float32(0.5)
+    ref_hb = oracle.build(tri, hb, threads=0)
+    _, got = build_np(builder, pinned.numpy(), hb, host=True)
+    assert_same(got, ref_hb, "chunked upload with host bounds")
+    _, got = build_np(builder, tri, hb)
+    assert_same(got, ref_hb, "device input with host bounds")
 
 
 def test_caller_outputs_one_element_off_16_bytes(builder):
