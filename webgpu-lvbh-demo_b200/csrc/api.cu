@@ -278,7 +278,8 @@ int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
     if (n <= ctx->cap && ctx->arena) return LVBH_OK;
     if (ctx->pending) cudaStreamSynchronize(ctx->last_stream);
     free_arena(ctx);
-    const uint32_t cap = n < 4096 ? 4096 : n;
+    // a multiple of 4: the centroid runs (stride cap) start on 16-byte boundaries
+    const uint32_t cap = n < 4096 ? 4096 : (n + 3u) & ~3u;
     void *p = nullptr;
     LVBH_CUDA(ctx, cudaMalloc(&p, arena_bytes(cap)));
     char *c = static_cast<char *>(p);
@@ -673,7 +674,7 @@ int lvbh_create(lvbh_ctx **out, const lvbh_config *cfg) {
     for (auto &e : ctx->ev) {
         if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); lvbh_destroy(ctx); return LVBH_ECUDA; }
     }
-    if (emit_init() != cudaSuccess || sort_init() != cudaSuccess) {
+    if (emit_init() != cudaSuccess || sort_init() != cudaSuccess || morton_init() != cudaSuccess) {
         cudaGetLastError();
         lvbh_destroy(ctx);
         return LVBH_ECUDA;

@@ -184,8 +184,10 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
     // 16-byte cp.async each (the load/store unit), waited for by each such thread on its own.
     // The copy engine takes about one small copy per 17 cycles per SM, which the whole gather
     // saturates (a thread stalled ~4,600 cycles per block issuing its copy); a quarter of the
-    // leaves on the other path keeps both busy (tree pass 1.04 -> 0.98 ms on 16.7 M).  Mesh: the
-    // vertex rows (mostly in L2) by cp.async.  One commit group per thread and block.
+    // leaves on the other path keeps both busy (tree pass 1.04 -> 0.98 ms on 16.7 M).  That
+    // quarter's L2 fetches are limited to 64 bytes (the pass's DRAM reads 162 -> 147 B per leaf,
+    // same time; the bulk copies take no such limit).  Mesh: the vertex rows (mostly in L2) by
+    // cp.async.  One commit group per thread and block.
     constexpr int kAsyncFrom = EB - EB / 4;  // first thread of the cp.async quarter (whole warps)
     auto fetch_tri = [&](int blk, int buf) {
         const Span sp = segs.span(blk);
@@ -203,9 +205,9 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
                 if (ti >= (uint32_t)n) { bad_perm = true; ti = 0; }
                 const float4 *src = lv.tri + 3ull * (sp.start + ti);
                 if (t >= kAsyncFrom) {
-                    cp_async16(&S.tri[buf][t][0], src);
-                    cp_async16(&S.tri[buf][t][1], src + 1);
-                    cp_async16(&S.tri[buf][t][2], src + 2);
+                    cp_async16_l64(&S.tri[buf][t][0], src);
+                    cp_async16_l64(&S.tri[buf][t][1], src + 1);
+                    cp_async16_l64(&S.tri[buf][t][2], src + 2);
                 } else {
                     bulk_g2s(&S.tri[buf][t][0], src, 48u, &S.bar[buf]);
                 }

@@ -112,6 +112,14 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
 }
+// The same with the L2's fetch from DRAM limited to the 64-byte half line around the address
+// (the `.L2::64B` prefetch size): for rows read at random it cuts the DRAM bytes per 48-byte
+// row from ~155 to ~98 (16.7 M random rows on a B200), since a whole line's other half is
+// rarely wanted.
+__device__ __forceinline__ void cp_async16_l64(void *smem_dst, const void *gmem_src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global.L2::64B [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
 // 4-byte asynchronous copy global -> shared (cached at all levels): a scattered destination per
 // thread, no register held while it is in flight.
 __device__ __forceinline__ void cp_async4(void *smem_dst, const void *gmem_src) {

@@ -140,6 +140,7 @@ void launch_bounds_cen(const float4 *tri, uint32_t t0, uint32_t t1, float *cen, 
                        Control *ctl, cudaStream_t s);
 void launch_morton_cen(const float *cen, uint32_t cen_stride, uint32_t n, Control *ctl, uint32_t *keys,
                        uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s);
+cudaError_t morton_init();  // once per device, before the first launch
 // K2: one reduce-then-scan pass over 10-bit digit `pass` (0..2) of 30-bit keys.  counted: the
 // tile histograms, chunk sums and global digit counts (ctl->hist_part) of this pass are there
 // already (K1b makes those of pass 0); otherwise the pass's tile-histogram kernel makes them

@@ -145,9 +145,8 @@ __global__ void __launch_bounds__(kThreads) k_bounds_cen(const float4 *__restric
 // go straight to the sort's scratch, so the first sort pass starts from them.
 // kSrcMesh: the triangles are index triples into a buffer of 16-byte vertex rows (the indexed
 // leaf format's input); each lane gathers its triangle's three rows, an index past the buffer
-// reads row 0 and sets ERR_BAD_INDEX.  kSrcCen: the centroids K1a stored (structure of arrays,
-// `cen_stride` floats apart), quantised with the device-reduced box; K1a checked the vertices.
-constexpr int kSrcSoup = 0, kSrcMesh = 1, kSrcCen = 2;
+// reads row 0 and sets ERR_BAD_INDEX.  The centroids K1a stored are quantised by k_morton_cen.
+constexpr int kSrcSoup = 0, kSrcMesh = 1;
 template <int SRC, int THREADS = kThreads>
 __global__ void __launch_bounds__(THREADS) k_morton(const float4 *__restrict__ tri, uint32_t n,
                                                      HostBounds hb, Control *__restrict__ ctl,
@@ -156,13 +155,12 @@ __global__ void __launch_bounds__(THREADS) k_morton(const float4 *__restrict__ t
                                                      uint32_t *__restrict__ tile_hist,
                                                      uint32_t *__restrict__ chunk_sum,
                                                      const uint32_t *__restrict__ idx3, uint32_t nverts,
-                                                     const float *__restrict__ cen, uint32_t cen_stride,
                                                      uint32_t chunk0) {
     constexpr bool MESH = SRC == kSrcMesh;
     const uint32_t chunk = chunk0 + blockIdx.x;  // this block's chunk of sort tiles
     constexpr int P = kDigits / THREADS;  // digits per thread in the per-tile counts
     constexpr int WARPS = THREADS / 32;
-    __shared__ float4 stage[SRC == kSrcSoup ? WARPS : 1][96];
+    __shared__ float4 stage[MESH ? 1 : WARPS][96];
     __shared__ uint32_t th[kDigits];
     if (chunk == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
         const uint32_t e = *epoch + 1u;
@@ -198,12 +196,6 @@ __global__ void __launch_bounds__(THREADS) k_morton(const float4 *__restrict__ t
         // while it works on this one (0.179 -> 0.157 ms on 16.7 M triangles)
         float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0, q2 = q0;
         auto ld_row = [&](uint32_t cc) {
-            if constexpr (SRC == kSrcCen) {  // this lane's centroid of the row (x, y, z in q0)
-                const uint32_t t = tile * (uint32_t)kSortTile + 32u * cc + lane;
-                if (t < n) q0 = make_float4(__ldcs(cen + t), __ldcs(cen + cen_stride + t),
-                                            __ldcs(cen + 2ull * cen_stride + t), 0.f);
-                return;
-            }
             const uint64_t base = 3ull * (tile * (uint32_t)kSortTile + 32u * cc);
             const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
             q0 = base + lane < nv ? ld_stream(tri + base + lane) : z;
@@ -233,10 +225,6 @@ __global__ void __launch_bounds__(THREADS) k_morton(const float4 *__restrict__ t
                 v0 = __ldg(tri + i0);
                 v1 = __ldg(tri + i1);
                 v2 = __ldg(tri + i2);
-            } else if constexpr (SRC == kSrcCen) {
-                v0 = q0;  // the centroid
-                v1 = v2 = v0;
-                if (c + WARPS < (uint32_t)kSortTile / 32 && t0 + 32u * WARPS < n) ld_row(c + WARPS);
             } else {
                 const float4 a0 = q0, a1 = q1, a2 = q2;
                 if (c + WARPS < (uint32_t)kSortTile / 32 && t0 + 32u * WARPS < n) ld_row(c + WARPS);
@@ -250,11 +238,7 @@ __global__ void __launch_bounds__(THREADS) k_morton(const float4 *__restrict__ t
                 __syncwarp();
             }
             uint32_t key = 0;
-            if (SRC == kSrcCen && valid) {
-                key = morton3(quantise_cen(v0.x, umin[0], umax[0]), quantise_cen(v0.y, umin[1], umax[1]),
-                              quantise_cen(v0.z, umin[2], umax[2]));
-                keys[t] = key;
-            } else if (valid) {
+            if (valid) {
                 bad |= !(finite3(v0) && finite3(v1) && finite3(v2));
                 // box.min = min(v0, min(v1, v2)); box.max = max(v0, max(v1, v2))   (:186-187)
                 const uint32_t qx = quantise(fminf(v0.x, fminf(v1.x, v2.x)), fmaxf(v0.x, fmaxf(v1.x, v2.x)), umin[0], umax[0]);
@@ -289,6 +273,101 @@ __global__ void __launch_bounds__(THREADS) k_morton(const float4 *__restrict__ t
     }
     if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(&ctl->err, ERR_NONFINITE);
     if (__any_sync(0xFFFFFFFFu, bad_index) && lane == 0) atomicOr(&ctl->err, ERR_BAD_INDEX);
+}
+
+// K1b from the centroids K1a stored (structure of arrays, `cen_stride` floats apart, a multiple
+// of 4): one block per chunk of sort tiles, each tile's three 16 KB centroid runs copied into
+// shared memory by 16-byte cp.async while the block quantises the tile before (two buffers), so
+// that a whole tile's loads are in flight at once.  Row i of warp w is keys 32 (w + WARPS i) ..
+// + 31 of the tile, one per lane; counts as k_morton.  On 16.7 M clustered centroids (B200):
+// 0.104 ms as k_morton's centroid mode (a warp's next row of 32 loaded while it works on this
+// one: about 12 KB in flight per SM), 0.091 ms so with 512 threads, 0.087 ms with 1024.  The
+// division of quantise_cen is not what bounds it: taking it out of the common case (a product
+// with a per-axis reciprocal, exact except within 2^-11 of a step, those keys divided) was
+// slower (0.089 -> 0.100 ms at 512 threads), though exact over every float.
+constexpr int kCenThreads = 1024;
+struct CenSmem {
+    float c[2][3][kSortTile];  // [buffer][axis][key of the tile]
+};
+__global__ void __launch_bounds__(kCenThreads) k_morton_cen(const float *__restrict__ cen, uint32_t cen_stride,
+                                                            uint32_t n, Control *__restrict__ ctl,
+                                                            uint32_t *__restrict__ keys, uint32_t *__restrict__ epoch,
+                                                            uint32_t chunk_tiles, uint32_t *__restrict__ tile_hist,
+                                                            uint32_t *__restrict__ chunk_sum) {
+    constexpr int WARPS = kCenThreads / 32, P = kDigits / kCenThreads, R = kSortTile / 32 / WARPS;
+    static_assert(R * WARPS * 32 == kSortTile && P * kCenThreads == kDigits, "whole rows and digits");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CenSmem &S = *reinterpret_cast<CenSmem *>(smem_raw);
+    __shared__ uint32_t th[kDigits];
+    const uint32_t chunk = blockIdx.x;
+    if (chunk == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
+        const uint32_t e = *epoch + 1u;
+        *epoch = e == 0u ? 1u : e;
+    }
+    float umin[3], umax[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        umin[a] = ord_lo_inv(~ctl->bounds_ord[a]);
+        umax[a] = ord_lo_inv(ctl->bounds_ord[3 + a]);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t tiles = sort_tiles(n), t0 = chunk * chunk_tiles, t1 = min(tiles, t0 + chunk_tiles);
+    // a tile's 16-byte pieces of the three runs up to the one holding key n - 1 (the stride
+    // keeps every run on a 16-byte boundary; a partial last piece reads stride slack)
+    auto issue = [&](uint32_t tile, int b) {
+        const uint32_t first = tile * (uint32_t)kSortTile;
+        const uint32_t pieces = min((uint32_t)kSortTile, n - first + 3u) / 4u;
+        for (uint32_t q = threadIdx.x; q < 3u * (kSortTile / 4); q += kCenThreads) {
+            const uint32_t a = q / (kSortTile / 4), p = q % (kSortTile / 4);
+            if (p < pieces) cp_async16(&S.c[b][a][4 * p], cen + (size_t)a * cen_stride + first + 4 * p);
+        }
+        cp_async_commit();
+    };
+    uint32_t acc[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) acc[j] = 0;
+    if (t0 < t1) issue(t0, 0);
+    for (uint32_t tile = t0; tile < t1; ++tile) {
+        const int b = (int)((tile - t0) & 1u);
+        if (tile + 1 < t1) issue(tile + 1, b ^ 1);
+        else cp_async_commit();  // an empty group keeps the count below uniform
+        for (int i = threadIdx.x; i < kDigits; i += kCenThreads) th[i] = 0;
+        asm volatile("cp.async.wait_group 1;" ::: "memory");  // this tile's pieces (own ones)
+        __syncthreads();  // everyone's pieces, and the cleared counts
+        bool coherent = false;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int j = 32 * (warp + WARPS * i) + lane;
+            const uint32_t t = tile * (uint32_t)kSortTile + j;
+            const bool valid = t < n;
+            uint32_t key = 0;
+            if (valid) {
+                key = morton3(quantise_cen(S.c[b][0][j], umin[0], umax[0]), quantise_cen(S.c[b][1][j], umin[1], umax[1]),
+                              quantise_cen(S.c[b][2][j], umin[2], umax[2]));
+                keys[t] = key;
+            }
+            // repeated digits over consecutive lanes (coherent input) are counted once per run;
+            // the warp tests its first row of each tile and keeps the answer for the tile
+            if (i == 0) coherent = runs_few(key & (kDigits - 1), valid);
+            if (coherent) add_runs(th, key & (kDigits - 1), valid);
+            else if (valid) atomicAdd(&th[key & (kDigits - 1)], 1u);
+        }
+        __syncthreads();  // the tile's counts are complete; buffer b is read
+        uint32_t *row = tile_hist + (size_t)tile * kDigits + threadIdx.x * P;
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            const uint32_t c = th[threadIdx.x * P + j];
+            row[j] = c;
+            acc[j] += c;
+        }
+        __syncthreads();  // counts read before the next tile clears them
+    }
+    uint32_t *crow = chunk_sum + (size_t)chunk * kDigits + threadIdx.x * P;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        crow[j] = acc[j];
+        if (acc[j]) atomicAdd(&ctl->hist_part[0][chunk % kHistParts][threadIdx.x * P + j], acc[j]);
+    }
 }
 
 // K1a for a mesh: min / max over the vertices the triangles use (the rows of unused vertices
@@ -525,7 +604,7 @@ void launch_morton_chunks(const float4 *tri, uint32_t n, HostBounds hb, Control 
     if (n == 0 || c1 <= c0) return;
     k_morton<kSrcSoup><<<c1 - c0, kThreads, 0, s>>>(tri, n, hb, ctl, keys, epoch, sort_chunk_tiles(n),
                                                     sort_scratch, sort_chunk_sums(sort_scratch, n), nullptr, 0u,
-                                                    nullptr, 0u, c0);
+                                                    c0);
 }
 
 void launch_bounds_cen(const float4 *tri, uint32_t t0, uint32_t t1, float *cen, uint32_t cen_stride,
@@ -540,11 +619,13 @@ void launch_bounds_cen(const float4 *tri, uint32_t t0, uint32_t t1, float *cen, 
 void launch_morton_cen(const float *cen, uint32_t cen_stride, uint32_t n, Control *ctl, uint32_t *keys,
                        uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
     if (n == 0) return;
-    // 512 threads: the chunks (two per SM) fill the GPU with one wave of 16-warp blocks
-    k_morton<kSrcCen, 512><<<sort_chunks(n), 512, 0, s>>>(nullptr, n, HostBounds{}, ctl, keys, epoch,
-                                                          sort_chunk_tiles(n), sort_scratch,
-                                                          sort_chunk_sums(sort_scratch, n), nullptr, 0u, cen,
-                                                          cen_stride, 0u);
+    k_morton_cen<<<sort_chunks(n), kCenThreads, sizeof(CenSmem), s>>>(cen, cen_stride, n, ctl, keys, epoch,
+                                                                      sort_chunk_tiles(n), sort_scratch,
+                                                                      sort_chunk_sums(sort_scratch, n));
+}
+
+cudaError_t morton_init() {
+    return cudaFuncSetAttribute(k_morton_cen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CenSmem));
 }
 
 void launch_bounds_mesh(const float4 *verts, uint32_t nverts, const uint32_t *idx3, uint32_t n, Control *ctl,
@@ -561,7 +642,7 @@ void launch_morton_mesh(const float4 *verts, uint32_t nverts, const uint32_t *id
     if (n == 0) return;
     k_morton<kSrcMesh><<<sort_chunks(n), kThreads, 0, s>>>(verts, n, hb, ctl, keys, epoch, sort_chunk_tiles(n),
                                                            sort_scratch, sort_chunk_sums(sort_scratch, n), idx3,
-                                                           nverts, nullptr, 0u, 0u);
+                                                           nverts, 0u);
 }
 
 void launch_leaf_idx(const uint32_t *idx3, const uint32_t *perm, uint32_t n, uint32_t *sidx, cudaStream_t s) {

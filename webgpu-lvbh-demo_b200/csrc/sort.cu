@@ -325,18 +325,27 @@ __global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ ke
     uint32_t acc[P];
 #pragma unroll
     for (int j = 0; j < P; ++j) acc[j] = 0;
-    for (uint32_t tt = 0; tt < chunk_tiles; ++tt) {
-        const uint32_t tile = blockIdx.x * chunk_tiles + tt;
-        if (tile >= tiles) break;  // uniform across the block
-        for (int i = tid; i < D; i += T) h[i] = 0;
-        __syncthreads();
+    // the next tile's keys are loaded while this one is counted
+    uint32_t kn[IPT];
+    auto load = [&](uint32_t tile) {
         const uint32_t base = tile * (uint32_t)kSortTile;
-        uint32_t k[IPT];
 #pragma unroll
         for (int i = 0; i < IPT; ++i) {
             const uint32_t idx = base + i * T + tid;
-            k[i] = idx < n ? __ldcs(keys + idx) : 0xFFFFFFFFu;
+            kn[i] = idx < n ? __ldcs(keys + idx) : 0xFFFFFFFFu;
         }
+    };
+    if (blockIdx.x * chunk_tiles < tiles) load(blockIdx.x * chunk_tiles);
+    for (uint32_t tt = 0; tt < chunk_tiles; ++tt) {
+        const uint32_t tile = blockIdx.x * chunk_tiles + tt;
+        if (tile >= tiles) break;  // uniform across the block
+        uint32_t k[IPT];
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) k[i] = kn[i];
+        if (tt + 1 < chunk_tiles && tile + 1 < tiles) load(tile + 1);
+        for (int i = tid; i < D; i += T) h[i] = 0;
+        __syncthreads();
+        const uint32_t base = tile * (uint32_t)kSortTile;
         // keys grouped by the previous digit repeat this one over long runs when the input was
         // spatially coherent; the warp tests its first 32 keys and keeps the answer for the tile
         const bool coherent = runs_few((k[0] >> shift) & (D - 1), base + tid < n);
