@@ -334,9 +334,10 @@ struct MeshIn {
 // bounds).
 enum Pre : int { kPreNone = 0, kPreCen = 1, kPreKeys = 2 };
 
-void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
-                   const lvbh_result *out, cudaStream_t s, bool profile, const MeshIn *mesh = nullptr,
-                   int pre = kPreNone) {
+// An error: a launch could not be made (the tree pass's tensor map); the rest was enqueued.
+cudaError_t enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds &hb,
+                          const lvbh_result *out, cudaStream_t s, bool profile, const MeshIn *mesh = nullptr,
+                          int pre = kPreNone) {
     if (profile) cudaEventRecord(ctx->ev[1], s);
     if (pre == kPreNone)
         cudaMemsetAsync(reinterpret_cast<char *>(ctx->ctl) + offsetof(Control, err), 0,
@@ -367,18 +368,18 @@ void enqueue_build(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBound
         launch_emit_mesh(mesh->verts, mesh->nverts, sidx, out->morton, n, static_cast<float4 *>(out->nodes),
                          out->parents, ctx->items, ctx->counts, ctx->arrive, ctx->pend, ctx->pend_d, ctx->epoch,
                          ctx->ctl, s, profile ? ctx->ev + 5 : nullptr);
-        return;
+        return cudaSuccess;
     }
-    launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
-                static_cast<float4 *>(out->nodes), out->parents, ctx->items, ctx->counts,
-                ctx->arrive, ctx->pend, ctx->pend_d, ctx->epoch, ctx->ctl, s,
-                profile ? ctx->ev + 5 : nullptr);
+    return launch_emit(tri, out->leaf_index, out->morton, n, static_cast<float4 *>(out->tris),
+                       static_cast<float4 *>(out->nodes), out->parents, ctx->items, ctx->counts,
+                       ctx->arrive, ctx->pend, ctx->pend_d, ctx->epoch, ctx->ctl, s,
+                       profile ? ctx->ev + 5 : nullptr);
 }
 
 // The batched build: every launch on `s`.  The segment table (and host bounds) are copied from
 // the pinned mirror, so a replayed graph picks up the table of the current call.
-void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool use_bounds,
-                   const lvbh_result *out, cudaStream_t s, bool profile) {
+cudaError_t enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool use_bounds,
+                          const lvbh_result *out, cudaStream_t s, bool profile) {
     if (profile) cudaEventRecord(ctx->ev[1], s);
     cudaMemcpyAsync(ctx->b_rows, ctx->bh_rows, (bp.num_segs + 1ull) * sizeof(SegRow),
                     cudaMemcpyHostToDevice, s);
@@ -411,10 +412,10 @@ void enqueue_batch(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool u
         launch_onesweep_batch(bp, kb, vb, ko, vo, 3, ctx->b_hist, ctx->ctl, ctx->b_lookback, s);
     }
     if (profile) cudaEventRecord(ctx->ev[4], s);
-    launch_emit_batch(bp, tri, out->leaf_index, out->morton, static_cast<float4 *>(out->tris),
-                      static_cast<float4 *>(out->nodes), out->parents, ctx->b_items,
-                      ctx->b_counts, ctx->arrive, ctx->pend, ctx->pend_d, ctx->epoch, ctx->ctl, s,
-                      profile ? ctx->ev + 5 : nullptr);
+    return launch_emit_batch(bp, tri, out->leaf_index, out->morton, static_cast<float4 *>(out->tris),
+                             static_cast<float4 *>(out->nodes), out->parents, ctx->b_items,
+                             ctx->b_counts, ctx->arrive, ctx->pend, ctx->pend_d, ctx->epoch, ctx->ctl, s,
+                             profile ? ctx->ev + 5 : nullptr);
 }
 
 int launch_batch_graph(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bool use_bounds,
@@ -437,9 +438,10 @@ int launch_batch_graph(lvbh_ctx *ctx, const float4 *tri, const BatchPlan &bp, bo
         if (ctx->bgexec) { cudaGraphExecDestroy(ctx->bgexec); ctx->bgexec = nullptr; }
         if (!ctx->cap_stream) LVBH_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
         LVBH_CUDA(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_batch(ctx, tri, bp, use_bounds, out, ctx->cap_stream, false);
+        const cudaError_t qe = enqueue_batch(ctx, tri, bp, use_bounds, out, ctx->cap_stream, false);
         cudaGraph_t g = nullptr;
         LVBH_CUDA(ctx, cudaStreamEndCapture(ctx->cap_stream, &g));
+        if (qe != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(ctx, qe, "tree pass tensor map"); }
         cudaError_t e = cudaGraphInstantiate(&ctx->bgexec, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) { ctx->bgexec = nullptr; return cuda_fail(ctx, e, "cudaGraphInstantiate(batch)"); }
@@ -467,9 +469,10 @@ int launch_graph(lvbh_ctx *ctx, const float4 *tri, uint32_t n, const HostBounds 
     if (!ctx->gexec || !(key == ctx->gkey)) {
         if (!ctx->cap_stream) LVBH_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
         LVBH_CUDA(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_build(ctx, tri, n, hb, out, ctx->cap_stream, false, mesh, pre);
+        const cudaError_t qe = enqueue_build(ctx, tri, n, hb, out, ctx->cap_stream, false, mesh, pre);
         cudaGraph_t g = nullptr;
         LVBH_CUDA(ctx, cudaStreamEndCapture(ctx->cap_stream, &g));
+        if (qe != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(ctx, qe, "tree pass tensor map"); }
         bool updated = false;
         if (ctx->gexec) {
             cudaGraphExecUpdateResultInfo info;
@@ -532,8 +535,9 @@ int build_common(lvbh_ctx *ctx, const float4 *tri_dev, uint32_t n, const float *
     int rc = LVBH_OK;
     if (profile && !profile_upload) cudaEventRecord(ctx->ev[0], s);
     if (profile || (flags & LVBH_NO_GRAPH)) {
-        enqueue_build(ctx, tri_dev, n, hb, out, s, profile, mesh, pre);
+        const cudaError_t qe = enqueue_build(ctx, tri_dev, n, hb, out, s, profile, mesh, pre);
         cudaError_t e = cudaGetLastError();
+        if (qe != cudaSuccess) return cuda_fail(ctx, qe, "tree pass tensor map");
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
     } else {
         rc = launch_graph(ctx, tri_dev, n, hb, out, s, mesh, pre);
@@ -914,7 +918,7 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
                 float ms = 0.f;
                 for (int rep = 0; rep < 2; ++rep) {
                     LVBH_CUDA(ctx, cudaEventRecord(e0, s));
-                    enqueue_batch(ctx, tri, cp, seg_bounds != nullptr, out, s, false);
+                    LVBH_CUDA(ctx, enqueue_batch(ctx, tri, cp, seg_bounds != nullptr, out, s, false));
                     LVBH_CUDA(ctx, cudaEventRecord(e1, s));
                     LVBH_CUDA(ctx, cudaEventSynchronize(e1));
                     LVBH_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
@@ -930,8 +934,9 @@ int lvbh_build_batched(lvbh_ctx *ctx, const float *tri_array, const uint32_t *se
     ctx->last_tuned = choice;
     const BatchPlan bp = plan(choice.t);
     if (profile || (flags & LVBH_NO_GRAPH)) {
-        enqueue_batch(ctx, tri, bp, seg_bounds != nullptr, out, s, profile);
+        const cudaError_t qe = enqueue_batch(ctx, tri, bp, seg_bounds != nullptr, out, s, profile);
         cudaError_t e = cudaGetLastError();
+        if (qe != cudaSuccess) return cuda_fail(ctx, qe, "tree pass tensor map");
         if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
     } else {
         if (int rc = launch_batch_graph(ctx, tri, bp, seg_bounds != nullptr, out, s)) return rc;

@@ -18,8 +18,9 @@
 //
 // Passes.
 //   K3b (k_tree_climb)   blocks of 256 sorted leaves in shared memory, a persistent grid that
-//                        prefetches the next block: leaf k's triangle perm[k] arrives by one
-//                        48-byte bulk copy, goes to the output soup at k and is reduced to its
+//                        prefetches the next blocks: leaf k's triangle perm[k] arrives with
+//                        three others by one TMA gather of four 48-byte rows, goes to the
+//                        output soup at k and is reduced to its
 //                        box (exact-zero components nudged by 1e-8 as bvh-up-pass.js:209-210
 //                        does).  The random gather bounds the pass.  The climb runs in steps:
 //                        the items still climbing after a step are compacted into a queue, so
@@ -33,6 +34,9 @@
 //                        paths of a tree at most 64 deep).
 //   K3c (k_emit_top)     the nodes that straddle blocks (~3 % of them), built bottom-up from
 //                        the open items with arrival words in global memory (see below).
+#include <cstring>
+#include <cuda.h>  // CUtensorMap
+#include <cudaTypedefs.h>
 #include <type_traits>
 
 #include "lvbh_device.cuh"
@@ -118,40 +122,50 @@ struct MeshLeaves {
     uint32_t nverts;
 };
 
+// The gathered triangles of this block and the next: buffer b holds leaves 4g .. 4g + 3 in
+// slot[b][g], four 48-byte rows (float4 0..11, one tensor gather each) in a 256-byte slot, so
+// that every gather's destination starts on a 128-byte boundary.  The slots' last 64 bytes
+// (float4 12..15), which no copy writes, hold the step queues: [queue][min/max][item] of the
+// items of the current and the next step (a step after the first has at most EB / 2: every
+// merge takes two items), entry f = (queue * 2 + min/max) * EB / 2 + item at flat slot f / 4,
+// float4 12 + f % 4.
 template <int EB>
 struct ClimbSmem {
-    float4 tri[2][EB][3];   // the gathered triangles of this block and the next (bulk copies)
-    float4 pend[2][2][EB];  // [side][min/max][split] the child parked at each split
-    float4 q[2][2][EB / 2]; // [queue][min/max][item] the items of the current and the next
-                            // step (a step after the first has at most EB / 2: every merge
-                            // takes two items).  Split / item index innermost keeps the
-                            // 16-byte accesses of random splits off each other's banks.
+    float4 slot[2][EB / 4][16];
+    float4 pend[2][2][EB];  // [side][min/max][split] the child parked at each split.  Split
+                            // index innermost keeps the 16-byte accesses of random splits off
+                            // each other's banks.
     uint32_t key[EB + 2];   // keys of leaves b0-1 .. b0+EB
     uint32_t mask[EB];      // arrivals at each split: bit 0 left child, bit 1 right child
     int par[2 * EB];        // parent of internal node b0 + j at j, of leaf b0 + j at EB + j
                             // (-1 = not set here)
     int cnt[3];             // item counters, rotating over the steps
     int open;               // open items emitted
-    uint64_t bar[2];        // completion of the bulk copies into tri[0] / tri[1]
+    uint64_t bar[2];        // completion of the gathers into slot[0] / slot[1]
 };
 
 // K3b: leaf gather, rearrange and the tree over blocks of EB sorted leaves (see the pass list
-// above).  Leaf t of a block gathers triangle perm[b0 + t]: its index is loaded two blocks
-// ahead, its 48-byte row is copied into shared memory one block ahead (one bulk copy per leaf
-// on the copy engine, completing on the buffer's mbarrier; no registers held meanwhile), then
-// written to the output soup and reduced to the leaf box.  A mesh leaf's three 16-byte vertex
-// rows (mostly L2 hits) come by cp.async instead.
+// above).  Leaf t of a block gathers triangle perm[b0 + t]: its index is loaded three blocks
+// ahead, its 48-byte row is copied into shared memory two blocks ahead (with those of leaves
+// t+1..t+3 by one tile::gather4 copy through `soup_map`, the soup as a tensor of 12-float
+// rows, completing on the buffer's mbarrier; no registers held meanwhile), then written to the
+// output soup and reduced to the leaf box.  A mesh leaf's three 16-byte vertex rows (mostly L2
+// hits) come by cp.async instead (soup_map unused).
 template <int LOG, class Segs, class Leaves = SoupLeaves>
 __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_tree_climb(Segs segs,
                                                     const uint32_t *__restrict__ keys_all,
                                                     Leaves lv,
                                                     float4 *nodes_all, int32_t *parents_all,
                                                     OpenItem *out_items, uint32_t *out_counts,
-                                                    Control *ctl) {
+                                                    Control *ctl, const __grid_constant__ CUtensorMap soup_map) {
     using G = TreeGeo<LOG>;
     constexpr int EB = G::EB;
     extern __shared__ __align__(16) unsigned char smem[];
-    ClimbSmem<EB> &S = *reinterpret_cast<ClimbSmem<EB> *>(smem);
+    // the layout from the first 128-byte boundary (the launch adds 128 bytes of slack)
+    ClimbSmem<EB> &S = *reinterpret_cast<ClimbSmem<EB> *>(smem + ((128u - (smem_addr(smem) & 127u)) & 127u));
+    // leaf t's three rows in buffer b; entry f of the step queues (see ClimbSmem)
+    auto tri_row = [&](int b, int x) -> float4 * { return &S.slot[b][x >> 2][(x & 3) * 3]; };
+    auto qent = [&](int f) -> float4 & { return (&S.slot[0][0][0])[(f >> 2) * 16 + 12 + (f & 3)]; };
     const int t = threadIdx.x, lane = t & 31;
     // a sort whose look-back gave up left unsorted keys: build nothing from them (uniform)
     if (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT) return;
@@ -159,8 +173,8 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
     const uint32_t lt = lanemask_lt();
 
     // Leaves come in three steps ahead of their block: this thread's permutation entry (its three
-    // vertex indices for a mesh) three blocks ahead, its triangle copied into S.tri two blocks
-    // ahead, its key one block ahead.  Two buffers, S.tri[0] and S.tri[1], serve the copies two
+    // vertex indices for a mesh) three blocks ahead, its triangle copied into slot[] two blocks
+    // ahead, its key one block ahead.  Two buffers, slot[0] and slot[1], serve the copies two
     // blocks ahead: a block's buffer is refilled right after its own leaf phase has read it, so
     // the copies of two blocks are in flight while a block climbs.
     uint32_t pa = 0, pb = 0, pc = 0;
@@ -178,42 +192,41 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         }
     };
     bool bad_perm = false;
-    // The block's triangles into S.tri[buf].  Soup: the leaves of the first three quarters of the
-    // warps by one 48-byte bulk copy each (the copy engine) on the buffer's mbarrier, whose phase
-    // expects their bytes (thread 0's arrival is its only one); the last quarter's by three
-    // 16-byte cp.async each (the load/store unit), waited for by each such thread on its own.
-    // The copy engine takes about one small copy per 17 cycles per SM, which the whole gather
-    // saturates (a thread stalled ~4,600 cycles per block issuing its copy); a quarter of the
-    // leaves on the other path keeps both busy (tree pass 1.04 -> 0.98 ms on 16.7 M).  That
-    // quarter's L2 fetches are limited to 64 bytes (the pass's DRAM reads 162 -> 147 B per leaf,
-    // same time; the bulk copies take no such limit).  Mesh: the vertex rows (mostly in L2) by
-    // cp.async.  One commit group per thread and block.
-    constexpr int kAsyncFrom = EB - EB / 4;  // first thread of the cp.async quarter (whole warps)
+    // The block's triangles into slot[buf].  Soup: thread 4g issues one tile::gather4 copy of
+    // leaves 4g .. 4g+3 (rows sp.start + perm) on the buffer's mbarrier, whose phase expects 192
+    // bytes per group of four of the block (thread 0's arrival is its only one); a leaf past the
+    // segment in the last group repeats its group's first row (read, never used).  The copy
+    // engine takes about one small copy per 11 to 17 cycles per SM, which one 48-byte copy per
+    // leaf kept saturated; with four rows a copy and the tensor map's 64-byte L2 fills a random
+    // gather of 16.7 M rows takes 0.55 ms against 0.67 (B200; DRAM reads 154 -> 98 B per row).
+    // Mesh: the vertex rows (mostly in L2) by cp.async, one commit group per thread and block.
     auto fetch_tri = [&](int blk, int buf) {
         const Span sp = segs.span(blk);
         const int b0 = sp.b0, n = sp.n, k = b0 + t;
-        if (!Leaves::kMesh && t == 0) mbar_arrive_tx(&S.bar[buf], 48u * (uint32_t)min(min(EB, n - b0), kAsyncFrom));
-        if (k < n) {
-            if constexpr (Leaves::kMesh) {
+        if constexpr (Leaves::kMesh) {
+            if (k < n) {
                 // an index past the vertex buffer was reported by the Morton pass; read row 0
                 const uint32_t nv = lv.nverts;
-                cp_async16(&S.tri[buf][t][0], lv.verts + (pa < nv ? pa : 0u));
-                cp_async16(&S.tri[buf][t][1], lv.verts + (pb < nv ? pb : 0u));
-                cp_async16(&S.tri[buf][t][2], lv.verts + (pc < nv ? pc : 0u));
-            } else {
+                float4 *d = tri_row(buf, t);
+                cp_async16(d, lv.verts + (pa < nv ? pa : 0u));
+                cp_async16(d + 1, lv.verts + (pb < nv ? pb : 0u));
+                cp_async16(d + 2, lv.verts + (pc < nv ? pc : 0u));
+            }
+            cp_async_commit();
+        } else {
+            if (t == 0) mbar_arrive_tx(&S.bar[buf], 192u * (uint32_t)((min(EB, n - b0) + 3) / 4));
+            uint32_t row = 0;
+            if (k < n) {
                 uint32_t ti = pa;
                 if (ti >= (uint32_t)n) { bad_perm = true; ti = 0; }
-                const float4 *src = lv.tri + 3ull * (sp.start + ti);
-                if (t >= kAsyncFrom) {
-                    cp_async16_l64(&S.tri[buf][t][0], src);
-                    cp_async16_l64(&S.tri[buf][t][1], src + 1);
-                    cp_async16_l64(&S.tri[buf][t][2], src + 2);
-                } else {
-                    bulk_g2s(&S.tri[buf][t][0], src, 48u, &S.bar[buf]);
-                }
+                row = (uint32_t)(sp.start + ti);
             }
+            const uint32_t r1 = __shfl_down_sync(0xFFFFFFFFu, row, 1), r2 = __shfl_down_sync(0xFFFFFFFFu, row, 2),
+                           r3 = __shfl_down_sync(0xFFFFFFFFu, row, 3);
+            if ((t & 3) == 0 && k < n)
+                gather4_g2s(tri_row(buf, t), &soup_map, row, k + 1 < n ? r1 : row, k + 2 < n ? r2 : row,
+                            k + 3 < n ? r3 : row, &S.bar[buf]);
         }
-        cp_async_commit();
     };
     // one block ahead: its span, this thread's key, the keys on either side of the block
     Span nsp{0, 0, 0};
@@ -227,7 +240,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         if (t == EB - 1) nk_hi = (b0 + EB < n) ? __ldg(keys + b0 + EB) : 0u;
     };
     const int grid = (int)gridDim.x;
-    // after every thread has read S.tri[buf] (a barrier between): refill it with the block two
+    // after every thread has read slot[buf] (a barrier between): refill it with the block two
     // ahead, and load the permutation three ahead
     auto refill = [&](int blk, int buf) {
         if (blk + 2 * grid >= nblk) return;
@@ -270,19 +283,19 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         if (t == 0) S.open = 0;
         // this leaf's triangle: to the output soup, and its box (exact-zero components nudged
         // by 1e-8 as bvh-up-pass.js:209-210 does)
-        if (Leaves::kMesh || t >= kAsyncFrom) {
+        if constexpr (Leaves::kMesh) {
             // the next block's group may still be in flight (the newest one), not this one's
             if (blk + grid < nblk) asm volatile("cp.async.wait_group 1;" ::: "memory");
             else cp_async_wait_all();
-        }
-        if constexpr (!Leaves::kMesh) {
+        } else {
             if (!mbar_wait(&S.bar[buf], (phase >> buf) & 1u)) copy_timeout = true;
             phase ^= 1u << buf;
         }
         float4 leaf_lo = make_float4(0.f, 0.f, 0.f, __int_as_float(-(k + 1)));
         float4 leaf_hi0 = make_float4(0.f, 0.f, 0.f, 0.f);
         if (active) {
-            const float4 a = S.tri[buf][t][0], b = S.tri[buf][t][1], c = S.tri[buf][t][2];
+            const float4 *tr = tri_row(buf, t);
+            const float4 a = tr[0], b = tr[1], c = tr[2];
             if constexpr (!Leaves::kMesh) {
                 float4 *dst = lv.otri + 3ull * (sp.start + k);
                 st_stream(dst, a);
@@ -320,7 +333,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             float4 *last = nodes + 4ull * (n - 1);
             last[0] = z; last[1] = z; last[2] = z; last[3] = z;
         }
-        __syncthreads();  // every thread has waited on and read S.tri[buf]: it may be refilled
+        __syncthreads();  // every thread has waited on and read slot[buf]: it may be refilled
         refill(blk, buf);
         auto dval = [&](int x) -> int {  // d of split b0 + x, x in [-1, EB - 1]
             const int g = b0 + x;
@@ -386,8 +399,8 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             base = __shfl_sync(0xFFFFFFFFu, base, 0);
             if (cont) {
                 const int at = base + __popc(bal & lt);
-                S.q[oq][0][at] = nlo;
-                S.q[oq][1][at] = nhi;
+                qent((oq * 2) * (EB / 2) + at) = nlo;
+                qent((oq * 2 + 1) * (EB / 2) + at) = nhi;
             }
         };
 
@@ -408,7 +421,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             const int count = S.cnt[c];
             if (count <= kFreeClimb) {
                 if (t < count) {
-                    float4 lo = S.q[cur][0][t], hi = S.q[cur][1][t];
+                    float4 lo = qent((cur * 2) * (EB / 2) + t), hi = qent((cur * 2 + 1) * (EB / 2) + t);
                     for (int g2 = 0; g2 < 2 * EB; ++g2) {
                         if (!climb(lo, hi, nlo, nhi)) break;
                         lo = nlo;
@@ -419,7 +432,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             }
             const int nc = c == 2 ? 0 : c + 1, rc = nc == 2 ? 0 : nc + 1;
             cont = false;
-            if (t < count) cont = climb(S.q[cur][0][t], S.q[cur][1][t], nlo, nhi);
+            if (t < count) cont = climb(qent((cur * 2) * (EB / 2) + t), qent((cur * 2 + 1) * (EB / 2) + t), nlo, nhi);
             append(cont, nlo, nhi, cur ^ 1, nc);
             if (t == 0) S.cnt[rc] = 0;
             cur ^= 1;
@@ -743,11 +756,37 @@ struct ManyGroupSegs {  // the batched build's groups (ManySegGroups), counted i
     __device__ __forceinline__ size_t item_base(int g, int) const { return (size_t)gr.group(g).blk0 * kOpenCap; }
 };
 
+// the layout plus the slack that puts it on a 128-byte boundary
 template <int LOG>
-inline size_t leaves_smem_bytes() { return sizeof(ClimbSmem<TreeGeo<LOG>::EB>); }
+inline size_t leaves_smem_bytes() { return sizeof(ClimbSmem<TreeGeo<LOG>::EB>) + 128; }
+
+// The soup as a 2-D tensor of `rows` rows of 12 floats, 48 bytes apart, for the tree pass's
+// tile::gather4 copies: one-row boxes of a whole row, the L2 filling 64 bytes per DRAM request
+// (most of a randomly gathered row's 128-byte line is never used).  The base is 16-byte
+// aligned (every entry point checks it) and 1 <= rows <= LVBH_MAX_TRIS.
+cudaError_t soup_tensor_map(CUtensorMap *m, const float4 *tri, uint32_t rows) {
+    static const PFN_cuTensorMapEncodeTiled_v12000 enc = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            f = nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }();
+    if (!enc) return cudaErrorNotSupported;
+    const cuuint64_t dims[2] = {12, rows}, strides[1] = {48};
+    const cuuint32_t box[2] = {12, 1}, elem[2] = {1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float4 *>(tri), dims, strides, box, elem,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_64B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
 
 template <int LOG, class Segs, class Leaves>
-void launch_emit_impl(Segs segs, int groups, Leaves lv, const uint32_t *keys, float4 *nodes, int32_t *parents,
+void launch_emit_impl(Segs segs, int groups, Leaves lv, const CUtensorMap &soup_map, const uint32_t *keys,
+                      float4 *nodes, int32_t *parents,
                       OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
                       uint8_t *pend_d, const uint32_t *epoch, Control *ctl, bool top,
                       cudaStream_t s, cudaEvent_t *ev, int ctas_per_sm,
@@ -757,7 +796,7 @@ void launch_emit_impl(Segs segs, int groups, Leaves lv, const uint32_t *keys, fl
                                                                                 : TreeGeo<LOG>::kCtasPerSm;
     const int grid = min(groups, sm_count() * per_sm);
     k_tree_climb<LOG, Segs, Leaves><<<grid, TreeGeo<LOG>::EB, leaves_smem_bytes<LOG>(), s>>>(
-        segs, keys, lv, nodes, parents, items, counts, ctl);
+        segs, keys, lv, nodes, parents, items, counts, ctl, soup_map);
     if (ev) cudaEventRecord(ev[1], s);
     if (top) {
         if constexpr (std::is_same<Segs, OneSeg<LOG>>::value) {
@@ -818,15 +857,19 @@ cudaError_t emit_init() {
     return e;
 }
 
-void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
-                 float4 *otri, float4 *nodes, int32_t *parents, OpenItem *items,
-                 uint32_t *counts, uint32_t *arrive, float4 *pend, uint8_t *pend_d,
-                 const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev) {
-    if (n == 0) return;
+cudaError_t launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
+                        float4 *otri, float4 *nodes, int32_t *parents, OpenItem *items,
+                        uint32_t *counts, uint32_t *arrive, float4 *pend, uint8_t *pend_d,
+                        const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev) {
+    if (n == 0) return cudaSuccess;
+    CUtensorMap map;
+    const cudaError_t e = soup_tensor_map(&map, tri, n);
+    if (e != cudaSuccess) return e;
     const int groups = (int)emit_groups(n, kLogEmitBlock);
-    launch_emit_impl<kLogEmitBlock>(OneSeg<kLogEmitBlock>{(int)n}, groups, SoupLeaves{tri, perm, otri}, keys,
+    launch_emit_impl<kLogEmitBlock>(OneSeg<kLogEmitBlock>{(int)n}, groups, SoupLeaves{tri, perm, otri}, map, keys,
                                     nodes, parents, items, counts, arrive, pend, pend_d, epoch,
                                     ctl, groups > 1, s, ev, 0);
+    return cudaSuccess;
 }
 
 void launch_emit_mesh(const float4 *verts, uint32_t num_verts, const uint32_t *sidx, const uint32_t *keys,
@@ -835,25 +878,31 @@ void launch_emit_mesh(const float4 *verts, uint32_t num_verts, const uint32_t *s
                       cudaStream_t s, cudaEvent_t *ev) {
     if (n == 0) return;
     const int groups = (int)emit_groups(n, kLogEmitBlock);
+    CUtensorMap unused;  // mesh leaves come by cp.async
+    std::memset(&unused, 0, sizeof unused);
     launch_emit_impl<kLogEmitBlock>(OneSeg<kLogEmitBlock>{(int)n}, groups, MeshLeaves{verts, sidx, num_verts},
-                                    keys, nodes, parents, items, counts, arrive, pend, pend_d, epoch, ctl,
+                                    unused, keys, nodes, parents, items, counts, arrive, pend, pend_d, epoch, ctl,
                                     groups > 1, s, ev, 0);
 }
 
-void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
-                       const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
-                       OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
-                       uint8_t *pend_d, const uint32_t *epoch, Control *ctl, cudaStream_t s,
-                       cudaEvent_t *ev) {
-    if (bp.blocks == 0) return;
+cudaError_t launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
+                              const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
+                              OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
+                              uint8_t *pend_d, const uint32_t *epoch, Control *ctl, cudaStream_t s,
+                              cudaEvent_t *ev) {
+    if (bp.blocks == 0) return cudaSuccess;
+    CUtensorMap map;
+    const cudaError_t e = soup_tensor_map(&map, tri, bp.total);
+    if (e != cudaSuccess) return e;
     if (bp.log_block == 7)
         launch_emit_impl<7>(ManySegs<7>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks,
-                            SoupLeaves{tri, perm, otri}, keys, nodes, parents, items, counts, arrive, pend,
+                            SoupLeaves{tri, perm, otri}, map, keys, nodes, parents, items, counts, arrive, pend,
                             pend_d, epoch, ctl, true, s, ev, bp.tree_ctas_per_sm, bp.grp_seg, (int)bp.groups);
     else
         launch_emit_impl<8>(ManySegs<8>{bp.rows, bp.blk_seg, (int)bp.blocks}, (int)bp.blocks,
-                            SoupLeaves{tri, perm, otri}, keys, nodes, parents, items, counts, arrive, pend,
+                            SoupLeaves{tri, perm, otri}, map, keys, nodes, parents, items, counts, arrive, pend,
                             pend_d, epoch, ctl, true, s, ev, bp.tree_ctas_per_sm, bp.grp_seg, (int)bp.groups);
+    return cudaSuccess;
 }
 
 }  // namespace lvbh

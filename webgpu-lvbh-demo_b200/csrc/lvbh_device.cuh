@@ -149,6 +149,18 @@ __device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gmem_src, u
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(smem_addr(smem_dst)), "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
 }
+// Four rows of a 2-D tensor (rows r0..r3, the tensor map's one-row box from column 0) into
+// consecutive shared memory by one TMA tile::gather4 copy, completing on an mbarrier.  The
+// destination starts on a 128-byte boundary; the rows are inside the tensor.  No multicast.
+__device__ __forceinline__ void gather4_g2s(void *smem_dst, const void *tensor_map, uint32_t r0, uint32_t r1,
+                                            uint32_t r2, uint32_t r3, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+        ::"r"(smem_addr(smem_dst)), "l"(reinterpret_cast<uint64_t>(tensor_map)), "r"(0), "r"(r0), "r"(r1), "r"(r2),
+          "r"(r3), "r"(smem_addr(bar))
+        : "memory");
+}
 // Waits for the completion of the mbarrier phase of the given parity, at most kSpinLimitCycles;
 // false if the bound ran out.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {

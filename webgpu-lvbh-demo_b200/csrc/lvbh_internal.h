@@ -164,11 +164,12 @@ size_t emit_groups(uint32_t n, int log_eb = kLogEmitBlock);
 // Groups of the straddling pass's first level over `blocks` tree blocks of one segment.
 inline uint32_t straddle_groups(uint32_t blocks) { return (blocks + 15u) / 16u; }
 cudaError_t emit_init();  // once per device, before the first launch
-// ev (may be nullptr): three events, recorded before K3b, after K3b and after K3c.
-void launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
-                 float4 *otri, float4 *nodes, int32_t *parents, OpenItem *items,
-                 uint32_t *counts, uint32_t *arrive, float4 *pend, uint8_t *pend_d,
-                 const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev);
+// ev (may be nullptr): three events, recorded before K3b, after K3b and after K3c.  An error:
+// the soup's tensor map (K3b's gather) could not be made; nothing was launched.
+cudaError_t launch_emit(const float4 *tri, const uint32_t *perm, const uint32_t *keys, uint32_t n,
+                        float4 *otri, float4 *nodes, int32_t *parents, OpenItem *items,
+                        uint32_t *counts, uint32_t *arrive, float4 *pend, uint8_t *pend_d,
+                        const uint32_t *epoch, Control *ctl, cudaStream_t s, cudaEvent_t *ev);
 // Batched forms of K1a, K1b, K2 and K3 over the segments of `bp`.  seg_ord holds 6 ordered
 // bound words per segment (zeroed before K1a; min at 0-2 as ~ord_lo, max at 3-5 as ord_lo),
 // seg_hist 4 x 256 digit counts per segment (zeroed before K1b); host_bounds, when not null,
@@ -187,12 +188,12 @@ void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const u
                            const uint32_t *seg_hist, Control *ctl, uint32_t *lookback,
                            cudaStream_t s);
 // items / counts: bp.blocks * kOpenCap / 2 * bp.blocks entries (block counts, then group
-// counts of the straddling pass's first level).
-void launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
-                       const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
-                       OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
-                       uint8_t *pend_d, const uint32_t *epoch, Control *ctl, cudaStream_t s,
-                       cudaEvent_t *ev);
+// counts of the straddling pass's first level).  Errors as launch_emit.
+cudaError_t launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
+                              const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
+                              OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
+                              uint8_t *pend_d, const uint32_t *epoch, Control *ctl, cudaStream_t s,
+                              cudaEvent_t *ev);
 // Indexed mesh -> 48-byte soup (pad 0).  An index >= num_verts sets ERR_BAD_INDEX in
 // *err and gathers zeros instead of reading out of bounds.
 void launch_gather_indexed(const float *xyz, uint32_t num_verts, const uint32_t *idx3,
