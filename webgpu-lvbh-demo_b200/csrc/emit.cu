@@ -553,16 +553,18 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
     }
 }
 
-// K3c, first level (plain builds): one block per group of kGroupBlocks consecutive K3b blocks
+// K3c, first level: one block per group of Groups::kBlocks consecutive K3b blocks
 // climbs the group's open items through every split both of whose sides lie in the group, in
 // shared memory - the same park / merge handshake as K3b, splits found through a hash table,
 // each item climbing on its own thread with no barrier between levels - and writes those
 // records and parent links.  What is left (items whose next split leaves the group, children
 // parked at a split whose sibling never came) replaces the group's items, packed from its
 // first block's slot on, for the global pass (k_emit_top over groups), which so sees about
-// 1 / kGroupBlocks of the items.
+// 1 / kBlocks of the items.  A plain build's groups span 4096 leaves (16 blocks of 256, or
+// 32 of 128), a batched build's 16 blocks of its meshes.
 // A group with more than kGroupCap items packs them all for the global pass unchanged.
-constexpr int kGroupBlocks = 16;
+constexpr int kGroupBlocks = 16;  // a batched build's blocks per group
+constexpr int kMaxGroupBlocks = 32;
 constexpr int kGroupCap = 256;
 constexpr int kGroupHash = 512;   // slots (power of two); distinct splits <= 2 x items
 constexpr int kGroupThreads = 128;
@@ -574,7 +576,7 @@ struct GroupSmem {
     int hkey[kGroupHash];
     uint32_t hmask[kGroupHash];
     int hidx[kGroupHash][2];
-    int bstart[kGroupBlocks + 1];
+    int bstart[kMaxGroupBlocks + 1];
     int cnt[1];
     int nout;
 };
@@ -586,15 +588,18 @@ struct GroupSpan {
     int n, blk0, blk1, leaf0;
 };
 template <int LOG>
-struct OneSegGroups {  // plain build: blocks 16 g .. 16 g + 15 of the one segment
+struct OneSegGroups {  // plain build: blocks kBlocks g .. kBlocks g + kBlocks - 1 of the one segment
+    static constexpr int kBlocks = 4096 >> LOG;
+    static_assert(kBlocks <= kMaxGroupBlocks, "one warp scans a group's blocks");
     int n;
     __device__ __forceinline__ GroupSpan group(int g) const {
-        const int nblk = (n + (1 << LOG) - 1) >> LOG, b0 = g * kGroupBlocks;
-        return GroupSpan{0, n, b0, min(nblk, b0 + kGroupBlocks), b0 << LOG};
+        const int nblk = (n + (1 << LOG) - 1) >> LOG, b0 = g * kBlocks;
+        return GroupSpan{0, n, b0, min(nblk, b0 + kBlocks), b0 << LOG};
     }
 };
 template <int LOG>
 struct ManySegGroups {  // batched build: a segment's blocks in groups of 16, from its first group
+    static constexpr int kBlocks = kGroupBlocks;
     const SegRow *rows;
     const uint32_t *grp_seg;
     __device__ __forceinline__ GroupSpan group(int g) const {
@@ -611,7 +616,7 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, Open
                                                    const uint32_t *__restrict__ counts,
                                                    uint32_t *__restrict__ group_counts, float4 *nodes_all,
                                                    int32_t *parents_all, Control *ctl) {
-    constexpr int EB = 1 << LOG;
+    constexpr int EB = 1 << LOG, GB = Groups::kBlocks;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupSmem &S = *reinterpret_cast<GroupSmem *>(smem_raw);
     const int t = threadIdx.x;
@@ -624,15 +629,16 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, Open
     int32_t *parents = parents_all + 2ull * gs.start;
     OpenItem *gitems = items + (size_t)blk0 * kOpenCap;
     if (t < 32) {  // the blocks' item counts and their exclusive prefix (one warp)
-        const int c = (t < kGroupBlocks && blk0 + t < blk1) ? (int)min(counts[blk0 + t], (uint32_t)kOpenCap) : 0;
+        const int c = (t < GB && blk0 + t < blk1) ? (int)min(counts[blk0 + t], (uint32_t)kOpenCap) : 0;
         int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
             if (t >= o) incl += y;
         }
-        if (t <= kGroupBlocks) S.bstart[t] = incl - c;
+        if (t < GB) S.bstart[t] = incl - c;
         if (t == 31) {
+            S.bstart[GB] = incl;  // lanes from GB on count zero
             S.cnt[0] = min(incl, kGroupCap);
             S.nout = 0;
         }
@@ -642,7 +648,7 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, Open
         S.hmask[h] = 0u;
     }
     __syncthreads();
-    const int total = S.bstart[kGroupBlocks];  // blocks past blk1 count zero
+    const int total = S.bstart[GB];  // blocks past blk1 count zero
     if (total > kGroupCap) {
         // pack every item for the global pass, block by block through shared memory (the
         // packed slots lie at or below the ones they come from)
@@ -653,7 +659,7 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, Open
             for (int k = t; k < c; k += kGroupThreads) gitems[S.bstart[b - blk0] + k] = S.it[k];
             __syncthreads();
         }
-        if (t == 0) group_counts[g] = (uint32_t)min(total, kGroupBlocks * kOpenCap);
+        if (t == 0) group_counts[g] = (uint32_t)min(total, GB * kOpenCap);
         return;
     }
     for (int b = blk0; b < blk1; ++b) {
@@ -736,12 +742,13 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, Open
 // The global pass over groups: group g's items from its first block's slot on.
 template <int LOG>
 struct GroupSegs {
+    static constexpr int GB = OneSegGroups<LOG>::kBlocks;
     int n;
     __device__ __forceinline__ int blocks() const {
         const int tree_blocks = (n + (1 << LOG) - 1) >> LOG;
-        return (tree_blocks + kGroupBlocks - 1) / kGroupBlocks;
+        return (tree_blocks + GB - 1) / GB;
     }
-    __device__ __forceinline__ Span span(int g) const { return Span{0, n, g * kGroupBlocks * (1 << LOG)}; }
+    __device__ __forceinline__ Span span(int g) const { return Span{0, n, g * GB * (1 << LOG)}; }
     __device__ __forceinline__ size_t item_base(int g, int cap) const { return (size_t)g * cap; }
 };
 template <int LOG>
@@ -800,13 +807,14 @@ void launch_emit_impl(Segs segs, int groups, Leaves lv, const CUtensorMap &soup_
     if (ev) cudaEventRecord(ev[1], s);
     if (top) {
         if constexpr (std::is_same<Segs, OneSeg<LOG>>::value) {
-            const int ngroups = (groups + kGroupBlocks - 1) / kGroupBlocks;
+            constexpr int GB = OneSegGroups<LOG>::kBlocks;
+            const int ngroups = (groups + GB - 1) / GB;
             uint32_t *gcounts = counts + groups;  // the counts buffer holds 2 x groups words
             k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(OneSegGroups<LOG>{segs.n}, items,
                                                                    counts, gcounts, nodes, parents, ctl);
             // a group leaves a few dozen items: one lane each
             k_emit_top<GroupSegs<LOG>, kGroupLanes><<<(ngroups * kGroupLanes + 255) / 256, 256, 0, s>>>(
-                GroupSegs<LOG>{segs.n}, items, kGroupBlocks * kOpenCap, gcounts, nodes, parents, arrive, pend,
+                GroupSegs<LOG>{segs.n}, items, GB * kOpenCap, gcounts, nodes, parents, arrive, pend,
                 pend_d, epoch, ctl);
         } else if (grp_seg) {
             // batched: the same two levels over groups of 16 blocks that never cross a mesh
@@ -841,10 +849,11 @@ cudaError_t prefer_shared(K kernel, size_t bytes) {
 size_t emit_groups(uint32_t n, int log_eb) { return (n + (1u << log_eb) - 1) >> log_eb; }
 
 cudaError_t emit_init() {
-    cudaError_t e = prefer_shared(k_tree_climb<8, OneSeg<8>>, leaves_smem_bytes<8>());
+    cudaError_t e = prefer_shared(k_tree_climb<kLogEmitBlock, OneSeg<kLogEmitBlock>>, leaves_smem_bytes<kLogEmitBlock>());
     if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, ManySegs<8>>, leaves_smem_bytes<8>());
     if (e == cudaSuccess) e = prefer_shared(k_tree_climb<7, ManySegs<7>>, leaves_smem_bytes<7>());
-    if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, OneSeg<8>, MeshLeaves>, leaves_smem_bytes<8>());
+    if (e == cudaSuccess)
+        e = prefer_shared(k_tree_climb<kLogEmitBlock, OneSeg<kLogEmitBlock>, MeshLeaves>, leaves_smem_bytes<kLogEmitBlock>());
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_top_group<kLogEmitBlock, OneSegGroups<kLogEmitBlock>>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem));
