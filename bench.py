@@ -63,7 +63,7 @@ UNIT = "Mprims/s"
 # is fixed; the build moves less in its first two stages (box and centroids: read 48, write 12;
 # keys from the centroids: read 12, write 4 - 76 bytes where the model counts 100).
 MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "gather": 0, "tree": 192, "top": 0}
-KERNELS = {"bounds": ("k_bounds_cen", 1), "morton": ("k_morton", 1), "sort": ("k_scatter", 3),
+KERNELS = {"bounds": ("k_bounds_cen", 1), "morton": ("k_morton_cen", 1), "sort": ("k_scatter", 3),
            "gather": (None, 0), "tree": ("k_tree_climb", 1), "top": ("k_emit_top", 2)}
 # box and centroids, Morton keys (+ the first pass's tile histograms), 3 sort passes x (chunk
 # scan, scatter) and 2 tile-histogram passes, tree, straddling pass in two levels (group, global)

@@ -112,14 +112,6 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
 }
-// The same with the L2's fetch from DRAM limited to the 64-byte half line around the address
-// (the `.L2::64B` prefetch size): for rows read at random it cuts the DRAM bytes per 48-byte
-// row from ~155 to ~98 (16.7 M random rows on a B200), since a whole line's other half is
-// rarely wanted.
-__device__ __forceinline__ void cp_async16_l64(void *smem_dst, const void *gmem_src) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global.L2::64B [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
-}
 // 4-byte asynchronous copy global -> shared (cached at all levels): a scattered destination per
 // thread, no register held while it is in flight.
 __device__ __forceinline__ void cp_async4(void *smem_dst, const void *gmem_src) {
@@ -129,12 +121,12 @@ __device__ __forceinline__ void cp_async4(void *smem_dst, const void *gmem_src) 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Bulk asynchronous copies global -> shared (the TMA engine, no tensor map) completing on an
-// mbarrier in this CTA's shared memory.  A random gather of rows from DRAM runs far faster this
-// way than through per-thread 16-byte cp.async: on the B200 a gather of 16.7 M random 48-byte
-// rows into shared memory took 0.66 ms as one 48-byte bulk copy per row, 1.14 ms as three
-// cp.async.  For 16-byte rows that hit L2 cp.async stays ahead (less work per copy).
-// Addresses and sizes are multiples of 16 bytes.  No multicast.
+// TMA copies global -> shared completing on an mbarrier in this CTA's shared memory.  A random
+// gather of rows from DRAM runs far faster this way than through per-thread 16-byte cp.async:
+// on the B200 a gather of 16.7 M random 48-byte rows into shared memory took 1.14 ms as three
+// cp.async per row, 0.67 ms as one 48-byte bulk copy per row and 0.55 ms as one tile::gather4
+// copy per four rows through a tensor map with 64-byte L2 fills.  For 16-byte rows that hit L2
+// cp.async stays ahead (less work per copy).  No multicast.
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
@@ -144,10 +136,6 @@ __device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier
 // one arrival that also raises the phase's expected byte count
 __device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gmem_src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_addr(smem_dst)), "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
 }
 // Four rows of a 2-D tensor (rows r0..r3, the tensor map's one-row box from column 0) into
 // consecutive shared memory by one TMA tile::gather4 copy, completing on an mbarrier.  The
