@@ -64,10 +64,10 @@ UNIT = "Mprims/s"
 # keys from the centroids: read 12, write 4 - 76 bytes where the model counts 100).
 MODEL_BYTES = {"bounds": 48, "morton": 52, "sort": 48, "gather": 0, "tree": 192, "top": 0}
 KERNELS = {"bounds": ("k_bounds_cen", 1), "morton": ("k_morton_cen", 1), "sort": ("k_scatter", 3),
-           "gather": (None, 0), "tree": ("k_tree_climb", 1), "top": ("k_emit_top", 2)}
+           "gather": (None, 0), "tree": ("k_tree_climb", 1), "top": ("k_top_group", 1)}
 # box and centroids, Morton keys (+ the first pass's tile histograms), 3 sort passes x (chunk
-# scan, scatter) and 2 tile-histogram passes, tree, straddling pass in two levels (group, global)
-LAUNCHES_PER_BUILD = 13
+# scan, scatter) and 2 tile-histogram passes, tree, straddling pass (group level, then global)
+LAUNCHES_PER_BUILD = 12
 MODEL_TOTAL = sum(MODEL_BYTES.values())  # 340 B per triangle
 
 
@@ -607,8 +607,8 @@ def run_batched(args, world, rank, local, clocks=None):
             "mprims_per_s": world * n / (ms * 1e-3) / 1e6,
             "per_mesh_loop_ms": loop, "per_mesh_builds_per_s": world * count / (base_ms * 1e-3),
             "speedup_vs_per_mesh": base_ms / ms, "identical_trees": bool(identical),
-            "stage_ms": stage_ms, "kernels_per_batch": 9 if tuned["digit_bits"] == 10 else 10,
-            "graph_nodes_per_batch": 12 if tuned["digit_bits"] == 10 else 13,
+            "stage_ms": stage_ms, "kernels_per_batch": 8 if tuned["digit_bits"] == 10 else 9,
+            "graph_nodes_per_batch": 11 if tuned["digit_bits"] == 10 else 12,
             "tunables": {"chosen": {k: tuned[k] for k in ("digit_bits", "tree_block")},
                          "candidates_ms": dict(zip(["10-bit/256", "10-bit/128", "8-bit/256", "8-bit/128"],
                                                    tuned["candidates_ms"]))},

@@ -22,7 +22,7 @@
 //                        three others by one TMA gather of four 48-byte rows, goes to the
 //                        output soup at k and is reduced to its
 //                        box (exact-zero components nudged by 1e-8 as bvh-up-pass.js:209-210
-//                        does).  The random gather bounds the pass.  The climb runs in steps:
+//                        does).  The climb runs in steps:
 //                        the items still climbing after a step are compacted into a queue, so
 //                        warps stay full while the number of items shrinks.  Parking and
 //                        merging use an arrival mask per split (shared-memory atomics) and
@@ -32,8 +32,9 @@
 //                        arrives (the parent straddles the block boundary), leaves as an
 //                        "open item" (at most 2 x 64 per block: they hang off the two boundary
 //                        paths of a tree at most 64 deep).
-//   K3c (k_emit_top)     the nodes that straddle blocks (~3 % of them), built bottom-up from
-//                        the open items with arrival words in global memory (see below).
+//   K3c (k_top_group)    the nodes that straddle blocks (~3 % of them), built bottom-up from
+//                        the open items: per group of blocks in shared memory, then with
+//                        arrival words in global memory (see below).
 #include <cstring>
 #include <cuda.h>  // CUtensorMap
 #include <cudaTypedefs.h>
@@ -461,8 +462,9 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
     if (copy_timeout) atomicOr(&ctl->err, ERR_COPY_TIMEOUT);
 }
 
-// K3c: the nodes that straddle blocks.  kTopLanes threads per block of K3b; each climbs one of
-// the block's open items (a block leaves about 8) through the remaining splits.  At a split the
+// K3c, the arrival-word climb: each thread climbs an open item through the splits above it
+// (k_top_group calls it for what leaves a group; k_emit_top, with kTopLanes threads per K3b
+// block, over the blocks' items directly).  At a split the
 // first arriving child parks its box, link and far range end in pend[] and its far end's
 // separator in pend_d[], both at its own index (r when it is a left child, l when a right child -
 // no two pending children ever share one), and exchanges the build's epoch into the split's
@@ -474,6 +476,68 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
 // Nothing waits, so the kernel cannot hang; climbs are bounded and every index is
 // range-checked.  The epoch makes the arrival words reusable without clearing: a word left by
 // an older build never equals the current epoch.
+//
+// One open item's climb through the splits above it with the arrival words, in a
+// segment of n triangles whose node, parent, arrival and pending arrays start at the pointers
+// given.  False if the climb broke off (a range inconsistent with the tree, or more levels than
+// any tree has).
+__device__ __forceinline__ bool top_climb(const OpenItem &it, int n, float4 *nodes, int32_t *parents, uint32_t *arrive,
+                                          float4 *pend, uint8_t *pend_d, uint32_t epoch) {
+    int l = it.xl, r = it.xr, ref = __float_as_int(it.lo.w);
+    float nx = it.lo.x, ny = it.lo.y, nz = it.lo.z, xx = it.hi.x, xy = it.hi.y, xz = it.hi.z;
+    int dl = it.pad0, dr = __float_as_int(it.hi.w);
+    // the record completed at the previous split, stored after the next exchange
+    bool have = false;
+    float4 w0, w1, w2, w3;
+    int wP = 0, wl = 0, wr = 0;
+    auto flush = [&]() {
+        if (!have) return;
+        float4 *rc = nodes + 4ull * wP;
+        rc[0] = w0; rc[1] = w1; rc[2] = w2; rc[3] = w3;
+        parents[wl >= 0 ? wl : n - (wl + 1)] = wP;
+        parents[wr >= 0 ? wr : n - (wr + 1)] = wP;
+        have = false;
+    };
+    bool done = false;
+    for (int level = 0; level < 160; ++level) {
+        if (l == 0 && r == n - 1) { done = true; break; }  // root complete
+        const bool is_left = dr > dl;
+        const int s = is_left ? r : l - 1;
+        if (s < 0 || s >= n - 1 || l < 0 || r >= n) break;
+        const int own = is_left ? r : l, sib = is_left ? s + 1 : s;
+        const float4 h0 = make_float4(nx, ny, nz, __int_as_float(ref));
+        const float4 h1 = make_float4(xx, xy, xz, __int_as_float(is_left ? l : r));
+        pend[2ull * own] = h0;
+        pend[2ull * own + 1] = h1;
+        pend_d[own] = (uint8_t)((is_left ? dl : dr) + 1);
+        const bool first = atom_exch_acq_rel_gpu(arrive + s, epoch) != epoch;
+        flush();
+        if (first) { done = true; break; }  // the sibling completes the parent
+        const float4 g0 = __ldcg(pend + 2ull * sib), g1 = __ldcg(pend + 2ull * sib + 1);
+        const int gd = (int)__ldcg(pend_d + sib) - 1;
+        const int sib_ref = __float_as_int(g0.w), sib_far = __float_as_int(g1.w);
+        const int L = is_left ? l : sib_far, R = is_left ? sib_far : r;
+        if (L < 0 || R >= n || L > l || R < r || sib_ref < -n || sib_ref >= n - 1) break;
+        const float4 lo0 = is_left ? h0 : g0, lo1 = is_left ? h1 : g1;
+        const float4 hi0 = is_left ? g0 : h0, hi1 = is_left ? g1 : h1;
+        nx = fminf(nx, g0.x); ny = fminf(ny, g0.y); nz = fminf(nz, g0.z);
+        xx = fmaxf(xx, g1.x); xy = fmaxf(xy, g1.y); xz = fmaxf(xz, g1.z);
+        const int ndl = is_left ? dl : gd, ndr = is_left ? gd : dr;
+        const int P = (L == 0 && R == n - 1) ? 0 : (ndr > ndl ? R : L);
+        w0 = lo0;
+        w1 = make_float4(lo1.x, lo1.y, lo1.z, __int_as_float(2));
+        w2 = hi0;
+        w3 = make_float4(hi1.x, hi1.y, hi1.z, __int_as_float(0));
+        wP = P;
+        wl = __float_as_int(lo0.w);
+        wr = __float_as_int(hi0.w);
+        have = true;
+        l = L; r = R; ref = P; dl = ndl; dr = ndr;
+    }
+    flush();
+    return done;
+}
+
 template <class Segs, int LANES = kTopLanes>
 __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__restrict__ items, int cap,
                                                   const uint32_t *__restrict__ counts,
@@ -489,68 +553,11 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
     if (lane >= cnt) return;
     const uint32_t epoch = *epoch_p;
     const Span sp = segs.span(gw);
-    const int n = sp.n;
-    float4 *nodes = nodes_all + 4ull * sp.start;
-    int32_t *parents = parents_all + 2ull * sp.start;
-    uint32_t *arrive = arrive_all + sp.start;
-    float4 *pend = pend_all + 2ull * sp.start;
-    uint8_t *pend_d = pend_d_all + sp.start;
-    for (int q = lane; q < cnt; q += LANES) {
-        const OpenItem it = items[segs.item_base(gw, cap) + q];
-        int l = it.xl, r = it.xr, ref = __float_as_int(it.lo.w);
-        float nx = it.lo.x, ny = it.lo.y, nz = it.lo.z, xx = it.hi.x, xy = it.hi.y, xz = it.hi.z;
-        int dl = it.pad0, dr = __float_as_int(it.hi.w);
-        // the record completed at the previous split, stored after the next exchange
-        bool have = false;
-        float4 w0, w1, w2, w3;
-        int wP = 0, wl = 0, wr = 0;
-        auto flush = [&]() {
-            if (!have) return;
-            float4 *rc = nodes + 4ull * wP;
-            rc[0] = w0; rc[1] = w1; rc[2] = w2; rc[3] = w3;
-            parents[wl >= 0 ? wl : n - (wl + 1)] = wP;
-            parents[wr >= 0 ? wr : n - (wr + 1)] = wP;
-            have = false;
-        };
-        bool done = false;
-        for (int level = 0; level < 160; ++level) {
-            if (l == 0 && r == n - 1) { done = true; break; }  // root complete
-            const bool is_left = dr > dl;
-            const int s = is_left ? r : l - 1;
-            if (s < 0 || s >= n - 1 || l < 0 || r >= n) break;
-            const int own = is_left ? r : l, sib = is_left ? s + 1 : s;
-            const float4 h0 = make_float4(nx, ny, nz, __int_as_float(ref));
-            const float4 h1 = make_float4(xx, xy, xz, __int_as_float(is_left ? l : r));
-            pend[2ull * own] = h0;
-            pend[2ull * own + 1] = h1;
-            pend_d[own] = (uint8_t)((is_left ? dl : dr) + 1);
-            const bool first = atom_exch_acq_rel_gpu(arrive + s, epoch) != epoch;
-            flush();
-            if (first) { done = true; break; }  // the sibling completes the parent
-            const float4 g0 = __ldcg(pend + 2ull * sib), g1 = __ldcg(pend + 2ull * sib + 1);
-            const int gd = (int)__ldcg(pend_d + sib) - 1;
-            const int sib_ref = __float_as_int(g0.w), sib_far = __float_as_int(g1.w);
-            const int L = is_left ? l : sib_far, R = is_left ? sib_far : r;
-            if (L < 0 || R >= n || L > l || R < r || sib_ref < -n || sib_ref >= n - 1) break;
-            const float4 lo0 = is_left ? h0 : g0, lo1 = is_left ? h1 : g1;
-            const float4 hi0 = is_left ? g0 : h0, hi1 = is_left ? g1 : h1;
-            nx = fminf(nx, g0.x); ny = fminf(ny, g0.y); nz = fminf(nz, g0.z);
-            xx = fmaxf(xx, g1.x); xy = fmaxf(xy, g1.y); xz = fmaxf(xz, g1.z);
-            const int ndl = is_left ? dl : gd, ndr = is_left ? gd : dr;
-            const int P = (L == 0 && R == n - 1) ? 0 : (ndr > ndl ? R : L);
-            w0 = lo0;
-            w1 = make_float4(lo1.x, lo1.y, lo1.z, __int_as_float(2));
-            w2 = hi0;
-            w3 = make_float4(hi1.x, hi1.y, hi1.z, __int_as_float(0));
-            wP = P;
-            wl = __float_as_int(lo0.w);
-            wr = __float_as_int(hi0.w);
-            have = true;
-            l = L; r = R; ref = P; dl = ndl; dr = ndr;
-        }
-        flush();
-        if (!done) atomicOr(&ctl->err, ERR_CLIMB);
-    }
+    for (int q = lane; q < cnt; q += LANES)
+        if (!top_climb(items[segs.item_base(gw, cap) + q], sp.n, nodes_all + 4ull * sp.start,
+                       parents_all + 2ull * sp.start, arrive_all + sp.start, pend_all + 2ull * sp.start,
+                       pend_d_all + sp.start, epoch))
+            atomicOr(&ctl->err, ERR_CLIMB);
 }
 
 // K3c, first level: one block per group of Groups::kBlocks consecutive K3b blocks
@@ -558,17 +565,19 @@ __global__ void __launch_bounds__(256) k_emit_top(Segs segs, const OpenItem *__r
 // shared memory - the same park / merge handshake as K3b, splits found through a hash table,
 // each item climbing on its own thread with no barrier between levels - and writes those
 // records and parent links.  What is left (items whose next split leaves the group, children
-// parked at a split whose sibling never came) replaces the group's items, packed from its
-// first block's slot on, for the global pass (k_emit_top over groups), which so sees about
-// 1 / kBlocks of the items.  A plain build's groups span 4096 leaves (16 blocks of 256, or
-// 32 of 128), a batched build's 16 blocks of its meshes.
-// A group with more than kGroupCap items packs them all for the global pass unchanged.
+// parked at a split whose sibling never came; about 1 / kBlocks of the items) then climbs on in
+// the same block with the arrival words of k_emit_top (top_climb), while other groups still run
+// their shared-memory climbs: those touch only splits inside their own groups, the arrival words
+// only splits that straddle a group.  (As a kernel of its own after the group pass the global
+// climb took 80 us of the 16.7 M build's 155; in the group kernel the pass takes 151 us: the
+// chain of arrivals up to the root, not the launch, sets its length.)  A plain build's groups
+// span 4096 leaves (16 blocks of 256, or 32 of 128), a batched build's 16 blocks of its meshes.
+// A group with more than kGroupCap items climbs them all with the arrival words.
 constexpr int kGroupBlocks = 16;  // a batched build's blocks per group
 constexpr int kMaxGroupBlocks = 32;
 constexpr int kGroupCap = 256;
 constexpr int kGroupHash = 512;   // slots (power of two); distinct splits <= 2 x items
 constexpr int kGroupThreads = 128;
-constexpr int kGroupLanes = 64;   // threads per group in the global pass
 
 struct GroupSmem {
     OpenItem it[kGroupCap];
@@ -612,10 +621,11 @@ struct ManySegGroups {  // batched build: a segment's blocks in groups of 16, fr
 };
 
 template <int LOG, class Groups>
-__global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, OpenItem *items,
-                                                   const uint32_t *__restrict__ counts,
-                                                   uint32_t *__restrict__ group_counts, float4 *nodes_all,
-                                                   int32_t *parents_all, Control *ctl) {
+__global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, const OpenItem *__restrict__ items,
+                                                   const uint32_t *__restrict__ counts, float4 *nodes_all,
+                                                   int32_t *parents_all, uint32_t *arrive_all, float4 *pend_all,
+                                                   uint8_t *pend_d_all, const uint32_t *__restrict__ epoch_p,
+                                                   Control *ctl) {
     constexpr int EB = 1 << LOG, GB = Groups::kBlocks;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupSmem &S = *reinterpret_cast<GroupSmem *>(smem_raw);
@@ -627,7 +637,10 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, Open
     const int lo_leaf = gs.leaf0, hi_leaf = min(n, gs.leaf0 + (blk1 - blk0) * EB);
     float4 *nodes = nodes_all + 4ull * gs.start;
     int32_t *parents = parents_all + 2ull * gs.start;
-    OpenItem *gitems = items + (size_t)blk0 * kOpenCap;
+    uint32_t *arrive = arrive_all + gs.start;
+    float4 *pend = pend_all + 2ull * gs.start;
+    uint8_t *pend_d = pend_d_all + gs.start;
+    const uint32_t epoch = *epoch_p;
     if (t < 32) {  // the blocks' item counts and their exclusive prefix (one warp)
         const int c = (t < GB && blk0 + t < blk1) ? (int)min(counts[blk0 + t], (uint32_t)kOpenCap) : 0;
         int incl = c;
@@ -650,16 +663,13 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, Open
     __syncthreads();
     const int total = S.bstart[GB];  // blocks past blk1 count zero
     if (total > kGroupCap) {
-        // pack every item for the global pass, block by block through shared memory (the
-        // packed slots lie at or below the ones they come from)
+        // more items than shared memory holds: every item climbs with the arrival words
         for (int b = blk0; b < blk1; ++b) {
             const int c = S.bstart[b - blk0 + 1] - S.bstart[b - blk0];
-            for (int k = t; k < c; k += kGroupThreads) S.it[k] = items[(size_t)b * kOpenCap + k];
-            __syncthreads();
-            for (int k = t; k < c; k += kGroupThreads) gitems[S.bstart[b - blk0] + k] = S.it[k];
-            __syncthreads();
+            for (int k = t; k < c; k += kGroupThreads)
+                if (!top_climb(items[(size_t)b * kOpenCap + k], n, nodes, parents, arrive, pend, pend_d, epoch))
+                    atomicOr(&ctl->err, ERR_CLIMB);
         }
-        if (t == 0) group_counts[g] = (uint32_t)min(total, GB * kOpenCap);
         return;
     }
     for (int b = blk0; b < blk1; ++b) {
@@ -734,34 +744,12 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, Open
         if (mk == 1u || mk == 2u) push_out(S.hidx[h][mk == 1u ? 0 : 1]);
     }
     __syncthreads();
+    // what leaves the group climbs on at once with the arrival words, beside the other groups'
+    // shared-memory climbs (those touch only splits inside their groups)
     const int nout = S.nout;
-    for (int k = t; k < nout; k += kGroupThreads) gitems[k] = S.it[S.out[k]];
-    if (t == 0) group_counts[g] = (uint32_t)nout;
+    for (int k = t; k < nout; k += kGroupThreads)
+        if (!top_climb(S.it[S.out[k]], n, nodes, parents, arrive, pend, pend_d, epoch)) atomicOr(&ctl->err, ERR_CLIMB);
 }
-
-// The global pass over groups: group g's items from its first block's slot on.
-template <int LOG>
-struct GroupSegs {
-    static constexpr int GB = OneSegGroups<LOG>::kBlocks;
-    int n;
-    __device__ __forceinline__ int blocks() const {
-        const int tree_blocks = (n + (1 << LOG) - 1) >> LOG;
-        return (tree_blocks + GB - 1) / GB;
-    }
-    __device__ __forceinline__ Span span(int g) const { return Span{0, n, g * GB * (1 << LOG)}; }
-    __device__ __forceinline__ size_t item_base(int g, int cap) const { return (size_t)g * cap; }
-};
-template <int LOG>
-struct ManyGroupSegs {  // the batched build's groups (ManySegGroups), counted in ngroups
-    ManySegGroups<LOG> gr;
-    int ngroups;
-    __device__ __forceinline__ int blocks() const { return ngroups; }
-    __device__ __forceinline__ Span span(int g) const {
-        const GroupSpan q = gr.group(g);
-        return Span{q.start, q.n, q.leaf0};
-    }
-    __device__ __forceinline__ size_t item_base(int g, int) const { return (size_t)gr.group(g).blk0 * kOpenCap; }
-};
 
 // the layout plus the slack that puts it on a 128-byte boundary
 template <int LOG>
@@ -809,24 +797,14 @@ void launch_emit_impl(Segs segs, int groups, Leaves lv, const CUtensorMap &soup_
         if constexpr (std::is_same<Segs, OneSeg<LOG>>::value) {
             constexpr int GB = OneSegGroups<LOG>::kBlocks;
             const int ngroups = (groups + GB - 1) / GB;
-            uint32_t *gcounts = counts + groups;  // the counts buffer holds 2 x groups words
-            k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(OneSegGroups<LOG>{segs.n}, items,
-                                                                   counts, gcounts, nodes, parents, ctl);
-            // a group leaves a few dozen items: one lane each
-            k_emit_top<GroupSegs<LOG>, kGroupLanes><<<(ngroups * kGroupLanes + 255) / 256, 256, 0, s>>>(
-                GroupSegs<LOG>{segs.n}, items, GB * kOpenCap, gcounts, nodes, parents, arrive, pend,
-                pend_d, epoch, ctl);
+            k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(
+                OneSegGroups<LOG>{segs.n}, items, counts, nodes, parents, arrive, pend, pend_d, epoch, ctl);
         } else if (grp_seg) {
-            // batched: the same two levels over groups of 16 blocks that never cross a mesh
-            uint32_t *gcounts = counts + groups;  // the counts buffer holds 2 x blocks words
+            // batched: the same over groups of 16 blocks that never cross a mesh
             const ManySegGroups<LOG> gr{segs.rows, grp_seg};
-            if (ngroups > 0) {
-                k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(gr, items, counts, gcounts,
-                                                                                   nodes, parents, ctl);
-                k_emit_top<ManyGroupSegs<LOG>, kGroupLanes><<<(ngroups * kGroupLanes + 255) / 256, 256, 0, s>>>(
-                    ManyGroupSegs<LOG>{gr, ngroups}, items, kGroupBlocks * kOpenCap, gcounts, nodes, parents,
-                    arrive, pend, pend_d, epoch, ctl);
-            }
+            if (ngroups > 0)
+                k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(gr, items, counts, nodes, parents,
+                                                                                   arrive, pend, pend_d, epoch, ctl);
         } else {
             k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, kOpenCap, counts, nodes,
                                                                          parents, arrive, pend, pend_d,
