@@ -130,7 +130,7 @@ struct MeshLeaves {
 // items of the current and the next step (a step after the first has at most EB / 2: every
 // merge takes two items), entry f = (queue * 2 + min/max) * EB / 2 + item at flat slot f / 4,
 // float4 12 + f % 4.
-template <int EB>
+template <int EB, int PROW>
 struct ClimbSmem {
     float4 slot[2][EB / 4][16];
     float4 pend[2][2][EB];  // [side][min/max][split] the child parked at each split.  Split
@@ -140,9 +140,19 @@ struct ClimbSmem {
     uint32_t mask[EB];      // arrivals at each split: bit 0 left child, bit 1 right child
     int par[2 * EB];        // parent of internal node b0 + j at j, of leaf b0 + j at EB + j
                             // (-1 = not set here)
+    uint32_t prow[PROW];    // soup, one segment: the rows of the block two ahead, staged for its gathers
+    Span sp2[2];            // soup: the span of the block two ahead of an iteration on buffer b
     int cnt[3];             // item counters, rotating over the steps
     int open;               // open items emitted
     uint64_t bar[2];        // completion of the gathers into slot[0] / slot[1]
+};
+
+// Whether a tree pass issues its soup gathers late (see issue_next in k_tree_climb) and its
+// shared-memory layout.
+template <int LOG, class Segs, class Leaves>
+struct TreeLayout {
+    static constexpr bool kLate = !Leaves::kMesh && std::is_same<Segs, OneSeg<LOG>>::value;
+    using Smem = ClimbSmem<(1 << LOG), kLate ? (1 << LOG) : 1>;
 };
 
 // K3b: leaf gather, rearrange and the tree over blocks of EB sorted leaves (see the pass list
@@ -161,9 +171,15 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
                                                     Control *ctl, const __grid_constant__ CUtensorMap soup_map) {
     using G = TreeGeo<LOG>;
     constexpr int EB = G::EB;
+    static_assert(kFreeClimb <= EB / 2, "the free climb leaves threads EB / 2 .. EB / 2 + EB / 4 - 1 idle");
+    // the soup gathers of a one-segment build issued late, by threads the free climb leaves idle
+    // (a batch keeps them in the refill: its extra state spilled there, 13.6 -> 14.1 ms a batch)
+    using Layout = TreeLayout<LOG, Segs, Leaves>;
+    constexpr bool kLate = Layout::kLate;
     extern __shared__ __align__(16) unsigned char smem[];
     // the layout from the first 128-byte boundary (the launch adds 128 bytes of slack)
-    ClimbSmem<EB> &S = *reinterpret_cast<ClimbSmem<EB> *>(smem + ((128u - (smem_addr(smem) & 127u)) & 127u));
+    typename Layout::Smem &S =
+        *reinterpret_cast<typename Layout::Smem *>(smem + ((128u - (smem_addr(smem) & 127u)) & 127u));
     // leaf t's three rows in buffer b; entry f of the step queues (see ClimbSmem)
     auto tri_row = [&](int b, int x) -> float4 * { return &S.slot[b][x >> 2][(x & 3) * 3]; };
     auto qent = [&](int f) -> float4 & { return (&S.slot[0][0][0])[(f >> 2) * 16 + 12 + (f & 3)]; };
@@ -241,18 +257,42 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         if (t == EB - 1) nk_hi = (b0 + EB < n) ? __ldg(keys + b0 + EB) : 0u;
     };
     const int grid = (int)gridDim.x;
-    // after every thread has read slot[buf] (a barrier between): refill it with the block two
-    // ahead, and load the permutation three ahead
+    // after every thread has read slot[buf] (a barrier between): load the permutation three
+    // ahead and, for mesh leaves, refill the buffer with the block two ahead
     auto refill = [&](int blk, int buf) {
         if (blk + 2 * grid >= nblk) return;
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // reads above, copies below
-        fetch_tri(blk + 2 * grid, buf);
-        if (blk + 3 * grid < nblk) fetch_perm(blk + 3 * grid);
+        if constexpr (!kLate) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // reads above, copies below
+            fetch_tri(blk + 2 * grid, buf);
+        }
+        if (blk + 3 * grid < nblk) {
+            fetch_perm(blk + 3 * grid);
+            if (kLate && t == 0) S.sp2[buf ^ 1] = segs.span(blk + 3 * grid);  // the next iteration's
+        }
+    };
+    // Soup: the block two ahead's gathers into slot[buf] (read by now), group g of it (leaves
+    // 4g .. 4g+3, rows staged in prow).  Issued by threads that the free climb leaves idle: the
+    // 64 copies of a block queue on the copy engine for ~2,300 cycles, a stall that delayed the
+    // whole block's first climb step when every fourth thread issued them after the leaf phase
+    // (tree pass 0.90 -> 0.886 ms on 16.7 M).
+    auto issue_next = [&](int blk, int buf, int g) {
+        if (blk + 2 * grid >= nblk) return;
+        const Span s2 = S.sp2[buf];
+        const int m2 = min(EB, s2.n - s2.b0), ng = (m2 + 3) / 4;
+        if (g == 0) mbar_arrive_tx(&S.bar[buf], 192u * (uint32_t)ng);
+        if (g < ng) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // reads above, copies below
+            const int x = 4 * g;  // a leaf past the segment repeats its group's first row
+            const uint32_t r0 = S.prow[x];
+            gather4_g2s(&S.slot[buf][g][0], &soup_map, r0, x + 1 < m2 ? S.prow[x + 1] : r0,
+                        x + 2 < m2 ? S.prow[x + 2] : r0, x + 3 < m2 ? S.prow[x + 3] : r0, &S.bar[buf]);
+        }
     };
     int buf = 0;
     uint32_t phase = 0;  // bit b: parity of the next phase of S.bar[b] (uniform over the block)
     bool copy_timeout = false;
     if (t < 2) mbar_init(&S.bar[t], 1);
+    if (kLate && t == 0 && (int)blockIdx.x + 2 * grid < nblk) S.sp2[0] = segs.span(blockIdx.x + 2 * grid);
     mbar_init_fence();
     __syncthreads();
     if ((int)blockIdx.x < nblk) {
@@ -311,6 +351,18 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             leaf_hi0 = make_float4(xx, xy, xz, 0.f);
         }
         if (blk + grid < nblk) fetch_keys(blk + grid);
+        if constexpr (kLate) {  // this thread's row of the block two ahead
+            if (blk + 2 * grid < nblk) {
+                const Span s2 = S.sp2[buf];
+                uint32_t row = 0;
+                if (s2.b0 + t < s2.n) {
+                    uint32_t ti = pa;
+                    if (ti >= (uint32_t)s2.n) { bad_perm = true; ti = 0; }
+                    row = (uint32_t)(s2.start + ti);
+                }
+                S.prow[t] = row;
+            }
+        }
         if (n == 1) {  // one leaf, one arrival at node 0: left slot only, f_1 = 1
             if (t == 0) {
                 nodes[0] = make_float4(leaf_lo.x, leaf_lo.y, leaf_lo.z, __int_as_float(-1));
@@ -325,6 +377,8 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             // keeps every thread's wait on this buffer's phase ahead of its next arming.
             __syncthreads();
             refill(blk, buf);
+            if constexpr (kLate)
+                if (t < EB / 4) issue_next(blk, buf, t);
             continue;
         }
         if (k == 0) {  // the root has no parent; slot N-1 and record N-1 stay zero
@@ -417,6 +471,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         // each takes one thread of the first warps and climbs on its own, item in registers,
         // without block barriers (the park / merge handshake works across warps).
         int cur = 0, c = 0;
+        bool issued = false;  // the block two ahead's gathers (uniform)
         for (int guard = 0; guard < 2 * EB; ++guard) {
             __syncthreads();
             const int count = S.cnt[c];
@@ -428,7 +483,10 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
                         lo = nlo;
                         hi = nhi;
                     }
+                } else if (kLate && t >= EB / 2 && t < EB / 2 + EB / 4) {
+                    issue_next(blk, buf, t - EB / 2);  // count <= kFreeClimb <= EB / 2
                 }
+                issued = true;
                 break;
             }
             const int nc = c == 2 ? 0 : c + 1, rc = nc == 2 ? 0 : nc + 1;
@@ -439,6 +497,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
             cur ^= 1;
             c = nc;
         }
+        if (kLate && !issued && t < EB / 4) issue_next(blk, buf, t);
         __syncthreads();
         // a child parked at a split whose sibling never came: the parent straddles the block
         if (t < m - 1) {
@@ -752,8 +811,8 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, cons
 }
 
 // the layout plus the slack that puts it on a 128-byte boundary
-template <int LOG>
-inline size_t leaves_smem_bytes() { return sizeof(ClimbSmem<TreeGeo<LOG>::EB>) + 128; }
+template <int LOG, class Segs, class Leaves>
+inline size_t leaves_smem_bytes() { return sizeof(typename TreeLayout<LOG, Segs, Leaves>::Smem) + 128; }
 
 // The soup as a 2-D tensor of `rows` rows of 12 floats, 48 bytes apart, for the tree pass's
 // tile::gather4 copies: one-row boxes of a whole row, the L2 filling 64 bytes per DRAM request
@@ -790,7 +849,7 @@ void launch_emit_impl(Segs segs, int groups, Leaves lv, const CUtensorMap &soup_
     const int per_sm = ctas_per_sm > 0 && ctas_per_sm < TreeGeo<LOG>::kCtasPerSm ? ctas_per_sm
                                                                                 : TreeGeo<LOG>::kCtasPerSm;
     const int grid = min(groups, sm_count() * per_sm);
-    k_tree_climb<LOG, Segs, Leaves><<<grid, TreeGeo<LOG>::EB, leaves_smem_bytes<LOG>(), s>>>(
+    k_tree_climb<LOG, Segs, Leaves><<<grid, TreeGeo<LOG>::EB, leaves_smem_bytes<LOG, Segs, Leaves>(), s>>>(
         segs, keys, lv, nodes, parents, items, counts, ctl, soup_map);
     if (ev) cudaEventRecord(ev[1], s);
     if (top) {
@@ -827,11 +886,12 @@ cudaError_t prefer_shared(K kernel, size_t bytes) {
 size_t emit_groups(uint32_t n, int log_eb) { return (n + (1u << log_eb) - 1) >> log_eb; }
 
 cudaError_t emit_init() {
-    cudaError_t e = prefer_shared(k_tree_climb<kLogEmitBlock, OneSeg<kLogEmitBlock>>, leaves_smem_bytes<kLogEmitBlock>());
-    if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, ManySegs<8>>, leaves_smem_bytes<8>());
-    if (e == cudaSuccess) e = prefer_shared(k_tree_climb<7, ManySegs<7>>, leaves_smem_bytes<7>());
+    constexpr int L = kLogEmitBlock;
+    cudaError_t e = prefer_shared(k_tree_climb<L, OneSeg<L>>, leaves_smem_bytes<L, OneSeg<L>, SoupLeaves>());
+    if (e == cudaSuccess) e = prefer_shared(k_tree_climb<8, ManySegs<8>>, leaves_smem_bytes<8, ManySegs<8>, SoupLeaves>());
+    if (e == cudaSuccess) e = prefer_shared(k_tree_climb<7, ManySegs<7>>, leaves_smem_bytes<7, ManySegs<7>, SoupLeaves>());
     if (e == cudaSuccess)
-        e = prefer_shared(k_tree_climb<kLogEmitBlock, OneSeg<kLogEmitBlock>, MeshLeaves>, leaves_smem_bytes<kLogEmitBlock>());
+        e = prefer_shared(k_tree_climb<L, OneSeg<L>, MeshLeaves>, leaves_smem_bytes<L, OneSeg<L>, MeshLeaves>());
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_top_group<kLogEmitBlock, OneSegGroups<kLogEmitBlock>>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GroupSmem));
