@@ -192,8 +192,9 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
     // Leaves come in three steps ahead of their block: this thread's permutation entry (its three
     // vertex indices for a mesh) three blocks ahead, its triangle copied into slot[] two blocks
     // ahead, its key one block ahead.  Two buffers, slot[0] and slot[1], serve the copies two
-    // blocks ahead: a block's buffer is refilled right after its own leaf phase has read it, so
-    // the copies of two blocks are in flight while a block climbs.
+    // blocks ahead: a block's buffer is refilled once its own leaf phase has read it (right after
+    // it, or for a one-segment soup during the block's free climb), so the copies of two blocks
+    // are in flight while a block climbs.
     uint32_t pa = 0, pb = 0, pc = 0;
     auto fetch_perm = [&](int blk) {
         const Span sp = segs.span(blk);
