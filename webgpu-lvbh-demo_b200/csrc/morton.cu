@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kCenThreads) k_morton_cen(const float *__restr
     static_assert(R * WARPS * 32 == kSortTile && P * kCenThreads == kDigits, "whole rows and digits");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CenSmem &S = *reinterpret_cast<CenSmem *>(smem_raw);
-    __shared__ uint32_t th[kDigits];
+    __shared__ uint32_t th[2][kDigits];  // a tile's counts, alternating with the buffers
     const uint32_t chunk = blockIdx.x;
     if (chunk == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
         const uint32_t e = *epoch + 1u;
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kCenThreads) k_morton_cen(const float *__restr
         const int b = (int)((tile - t0) & 1u);
         if (tile + 1 < t1) issue(tile + 1, b ^ 1);
         else cp_async_commit();  // an empty group keeps the count below uniform
-        for (int i = threadIdx.x; i < kDigits; i += kCenThreads) th[i] = 0;
+        for (int i = threadIdx.x; i < kDigits; i += kCenThreads) th[b][i] = 0;
         asm volatile("cp.async.wait_group 1;" ::: "memory");  // this tile's pieces (own ones)
         __syncthreads();  // everyone's pieces, and the cleared counts
         bool coherent = false;
@@ -349,18 +349,19 @@ __global__ void __launch_bounds__(kCenThreads) k_morton_cen(const float *__restr
             // repeated digits over consecutive lanes (coherent input) are counted once per run;
             // the warp tests its first row of each tile and keeps the answer for the tile
             if (i == 0) coherent = runs_few(key & (kDigits - 1), valid);
-            if (coherent) add_runs(th, key & (kDigits - 1), valid);
-            else if (valid) atomicAdd(&th[key & (kDigits - 1)], 1u);
+            if (coherent) add_runs(th[b], key & (kDigits - 1), valid);
+            else if (valid) atomicAdd(&th[b][key & (kDigits - 1)], 1u);
         }
         __syncthreads();  // the tile's counts are complete; buffer b is read
         uint32_t *row = tile_hist + (size_t)tile * kDigits + threadIdx.x * P;
 #pragma unroll
         for (int j = 0; j < P; ++j) {
-            const uint32_t c = th[threadIdx.x * P + j];
+            const uint32_t c = th[b][threadIdx.x * P + j];
             row[j] = c;
             acc[j] += c;
         }
-        __syncthreads();  // counts read before the next tile clears them
+        // no barrier here: the next tile counts into th[b ^ 1], which this tile's first barrier
+        // found read, and refills buffer b ^ 1 only, read before this tile's second barrier
     }
     uint32_t *crow = chunk_sum + (size_t)chunk * kDigits + threadIdx.x * P;
 #pragma unroll
