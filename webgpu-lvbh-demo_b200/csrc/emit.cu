@@ -171,7 +171,8 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
                                                     Control *ctl, const __grid_constant__ CUtensorMap soup_map) {
     using G = TreeGeo<LOG>;
     constexpr int EB = G::EB;
-    static_assert(kFreeClimb <= EB / 2, "the free climb leaves threads EB / 2 .. EB / 2 + EB / 4 - 1 idle");
+    constexpr int kFree = kFreeClimb < EB / 2 ? kFreeClimb : EB / 2;  // the free climb leaves threads
+                                                                     // EB / 2 .. 3 EB / 4 - 1 idle
     // the soup gathers of a one-segment build issued late, by threads the free climb leaves idle
     // (a batch keeps them in the refill: its extra state spilled there, 13.6 -> 14.1 ms a batch)
     using Layout = TreeLayout<LOG, Segs, Leaves>;
@@ -487,7 +488,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
                                               __uint_as_float(G::pack(t, t, dval(t - 1), dval(t)))),
                          nlo, nhi);
         append(cont, nlo, nhi, 0, 0);
-        // later steps: the merged parents, compacted.  Once at most kFreeClimb items are left,
+        // later steps: the merged parents, compacted.  Once at most kFree items are left,
         // each takes one thread of the first warps and climbs on its own, item in registers,
         // without block barriers (the park / merge handshake works across warps).
         int cur = 0, c = 0;
@@ -495,7 +496,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
         for (int guard = 0; guard < 2 * EB; ++guard) {
             __syncthreads();
             const int count = S.cnt[c];
-            if (count <= kFreeClimb) {
+            if (count <= kFree) {
                 if (t < count) {
                     float4 lo = qent((cur * 2) * (EB / 2) + t), hi = qent((cur * 2 + 1) * (EB / 2) + t);
                     for (int g2 = 0; g2 < 2 * EB; ++g2) {
@@ -504,7 +505,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
                         hi = nhi;
                     }
                 } else if (kLate && t >= EB / 2 && t < EB / 2 + EB / 4) {
-                    issue_next(blk, buf, t - EB / 2);  // count <= kFreeClimb <= EB / 2
+                    issue_next(blk, buf, t - EB / 2);  // count <= kFree <= EB / 2
                 }
                 issued = true;
                 break;
