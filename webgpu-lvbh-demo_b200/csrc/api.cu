@@ -59,7 +59,7 @@ size_t control_bytes(uint32_t n) {
 size_t arena_bytes(uint32_t cap) {
     const size_t groups = emit_groups(cap);
     return 4 * align_up((size_t)cap * 4) + align_up((size_t)cap * 12) + align_up((size_t)cap * 32) + align_up((size_t)cap) +
-           align_up(groups * kOpenCap * sizeof(OpenItem)) + align_up(2 * groups * sizeof(uint32_t)) +
+           align_up(groups * kOpenCap * sizeof(OpenItem)) + align_up(groups * sizeof(uint32_t)) +
            align_up(sizeof(uint32_t)) + control_bytes(cap);
 }
 
@@ -218,14 +218,14 @@ void free_batch(lvbh_ctx *ctx) {
 
 // Device bytes of the batch scratch for `segs` segments, `tiles` sort tiles and `blocks` tree
 // blocks: segment rows, tile / block / group -> segment maps, bounds, digit counts and
-// look-back words, given bounds, open items, block and group counts.
+// look-back words, given bounds, open items and their per-block counts.
 size_t batch_bytes(uint32_t segs, uint32_t tiles, uint32_t blocks) {
     const size_t rows = align_up((segs + 1ull) * sizeof(SegRow));
     const size_t ord = (size_t)segs * 6 * 4, hist = (size_t)segs * kHistWords * 4;
     const size_t lb = (size_t)kSortPasses * tiles * kDigits * 4;
     return rows + align_up(tiles * 4ull) + 2 * align_up(blocks * 4ull) + align_up(ord + hist + lb) +
            align_up((size_t)segs * 6 * 4) + align_up((size_t)blocks * kOpenCap * sizeof(OpenItem)) +
-           align_up(2 * blocks * 4ull);
+           align_up(blocks * 4ull);
 }
 
 // Batch scratch for up to `segs` segments, `tiles` sort tiles and `blocks` tree blocks.
@@ -262,7 +262,7 @@ int ensure_batch(lvbh_ctx *ctx, uint32_t segs, uint32_t tiles, uint32_t blocks) 
     c += zero;
     ctx->b_bounds = reinterpret_cast<float *>(c); c += bnd;
     ctx->b_items = reinterpret_cast<OpenItem *>(c); c += align_up((size_t)blocks * kOpenCap * sizeof(OpenItem));
-    ctx->b_counts = reinterpret_cast<uint32_t *>(c);  // block counts, then group counts
+    ctx->b_counts = reinterpret_cast<uint32_t *>(c);  // open items per tree block
     char *hc = static_cast<char *>(h);
     ctx->b_host = h;
     ctx->bh_rows = reinterpret_cast<SegRow *>(hc); hc += rows;
@@ -294,7 +294,7 @@ int ensure_arena(lvbh_ctx *ctx, uint32_t n) {
     ctx->pend = reinterpret_cast<float4 *>(c); c += align_up((size_t)cap * 32);
     ctx->pend_d = reinterpret_cast<uint8_t *>(c); c += align_up((size_t)cap);
     ctx->items = reinterpret_cast<OpenItem *>(c); c += align_up(groups * kOpenCap * sizeof(OpenItem));
-    ctx->counts = reinterpret_cast<uint32_t *>(c); c += align_up(2 * groups * sizeof(uint32_t));  // blocks, groups
+    ctx->counts = reinterpret_cast<uint32_t *>(c); c += align_up(groups * sizeof(uint32_t));  // per tree block
     ctx->epoch = reinterpret_cast<uint32_t *>(c); c += align_up(sizeof(uint32_t));
     ctx->ctl = reinterpret_cast<Control *>(c);
     ctx->lookback = reinterpret_cast<uint32_t *>(c + align_up(sizeof(Control)));

@@ -12,7 +12,7 @@ enum : uint32_t {
     ERR_LOOKBACK_TIMEOUT = 2u,  // a decoupled look-back wait exceeded its bound
     ERR_CLIMB = 4u,             // a refit climb exceeded the depth any valid tree has
     ERR_BAD_INDEX = 8u,         // an indexed-mesh vertex index is out of range
-    ERR_COPY_TIMEOUT = 16u,     // a bulk-copy wait (mbarrier) exceeded its bound
+    ERR_COPY_TIMEOUT = 16u,     // a copy wait (mbarrier) exceeded its bound
     ERR_SORT_RANGE = 32u,       // a radix sort scatter target fell outside the array (digit
                                 // counts inconsistent with the keys, e.g. overlapping calls)
 };

@@ -187,8 +187,8 @@ void launch_onesweep_batch(const BatchPlan &bp, const uint32_t *keys_in, const u
                            uint32_t *keys_out, uint32_t *vals_out, int pass,
                            const uint32_t *seg_hist, Control *ctl, uint32_t *lookback,
                            cudaStream_t s);
-// items / counts: bp.blocks * kOpenCap / 2 * bp.blocks entries (block counts, then group
-// counts of the straddling pass's first level).  Errors as launch_emit.
+// items / counts: bp.blocks * kOpenCap / bp.blocks entries (open items per tree block).
+// Errors as launch_emit.
 cudaError_t launch_emit_batch(const BatchPlan &bp, const float4 *tri, const uint32_t *perm,
                               const uint32_t *keys, float4 *otri, float4 *nodes, int32_t *parents,
                               OpenItem *items, uint32_t *counts, uint32_t *arrive, float4 *pend,
