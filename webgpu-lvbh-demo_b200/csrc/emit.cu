@@ -185,6 +185,7 @@ __global__ void __launch_bounds__(TreeGeo<LOG>::EB, TreeGeo<LOG>::kCtasPerSm) k_
     auto tri_row = [&](int b, int x) -> float4 * { return &S.slot[b][x >> 2][(x & 3) * 3]; };
     auto qent = [&](int f) -> float4 & { return (&S.slot[0][0][0])[(f >> 2) * 16 + 12 + (f & 3)]; };
     const int t = threadIdx.x, lane = t & 31;
+    chain_wait();
     // a sort whose look-back gave up left unsorted keys: build nothing from them (uniform)
     if (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT) return;
     const int nblk = segs.blocks();
@@ -712,6 +713,7 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, cons
     GroupSmem &S = *reinterpret_cast<GroupSmem *>(smem_raw);
     const int t = threadIdx.x;
     const int g = blockIdx.x;
+    chain_wait();
     if (ld_relaxed_gpu(&ctl->err) & ERR_LOOKBACK_TIMEOUT) return;  // unsorted keys: nothing to build
     const GroupSpan gs = groups.group(g);
     const int n = gs.n, blk0 = gs.blk0, blk1 = gs.blk1;
@@ -871,21 +873,24 @@ void launch_emit_impl(Segs segs, int groups, Leaves lv, const CUtensorMap &soup_
     const int per_sm = ctas_per_sm > 0 && ctas_per_sm < TreeGeo<LOG>::kCtasPerSm ? ctas_per_sm
                                                                                 : TreeGeo<LOG>::kCtasPerSm;
     const int grid = min(groups, sm_count() * per_sm);
-    k_tree_climb<LOG, Segs, Leaves><<<grid, TreeGeo<LOG>::EB, leaves_smem_bytes<LOG, Segs, Leaves>(), s>>>(
-        segs, keys, lv, nodes, parents, items, counts, ctl, soup_map);
+    // batched builds always chain; a one-mesh build by its size
+    bool chain = true;
+    if constexpr (std::is_same<Segs, OneSeg<LOG>>::value) chain = chain_build((uint32_t)segs.n);
+    launch_chained(chain, k_tree_climb<LOG, Segs, Leaves>, grid, TreeGeo<LOG>::EB, leaves_smem_bytes<LOG, Segs, Leaves>(), s,
+                   segs, keys, lv, nodes, parents, items, counts, ctl, soup_map);
     if (ev) cudaEventRecord(ev[1], s);
     if (top) {
         if constexpr (std::is_same<Segs, OneSeg<LOG>>::value) {
             constexpr int GB = OneSegGroups<LOG>::kBlocks;
             const int ngroups = (groups + GB - 1) / GB;
-            k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(
-                OneSegGroups<LOG>{segs.n}, items, counts, nodes, parents, arrive, pend, pend_d, epoch, ctl);
+            launch_chained(chain, k_top_group<LOG, OneSegGroups<LOG>>, ngroups, kGroupThreads, sizeof(GroupSmem), s,
+                           OneSegGroups<LOG>{segs.n}, items, counts, nodes, parents, arrive, pend, pend_d, epoch, ctl);
         } else if (grp_seg) {
             // batched: the same over groups of 16 blocks that never cross a mesh
             const ManySegGroups<LOG> gr{segs.rows, grp_seg};
             if (ngroups > 0)
-                k_top_group<LOG><<<ngroups, kGroupThreads, sizeof(GroupSmem), s>>>(gr, items, counts, nodes, parents,
-                                                                                   arrive, pend, pend_d, epoch, ctl);
+                launch_chained(chain, k_top_group<LOG, ManySegGroups<LOG>>, ngroups, kGroupThreads, sizeof(GroupSmem), s, gr,
+                               items, counts, nodes, parents, arrive, pend, pend_d, epoch, ctl);
         } else {
             k_emit_top<<<(groups * kTopLanes + 255) / 256, 256, 0, s>>>(segs, items, kOpenCap, counts, nodes,
                                                                          parents, arrive, pend, pend_d,

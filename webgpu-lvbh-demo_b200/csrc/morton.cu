@@ -300,6 +300,7 @@ __global__ void __launch_bounds__(kCenThreads) k_morton_cen(const float *__restr
     CenSmem &S = *reinterpret_cast<CenSmem *>(smem_raw);
     __shared__ uint32_t th[2][kDigits];  // a tile's counts, alternating with the buffers
     const uint32_t chunk = blockIdx.x;
+    chain_wait();
     if (chunk == 0 && threadIdx.x == 0) {  // new arrival epoch for K3c; 0 is never used
         const uint32_t e = *epoch + 1u;
         *epoch = e == 0u ? 1u : e;
@@ -620,9 +621,8 @@ void launch_bounds_cen(const float4 *tri, uint32_t t0, uint32_t t1, float *cen, 
 void launch_morton_cen(const float *cen, uint32_t cen_stride, uint32_t n, Control *ctl, uint32_t *keys,
                        uint32_t *epoch, uint32_t *sort_scratch, cudaStream_t s) {
     if (n == 0) return;
-    k_morton_cen<<<sort_chunks(n), kCenThreads, sizeof(CenSmem), s>>>(cen, cen_stride, n, ctl, keys, epoch,
-                                                                      sort_chunk_tiles(n), sort_scratch,
-                                                                      sort_chunk_sums(sort_scratch, n));
+    launch_chained(chain_build(n), k_morton_cen, sort_chunks(n), kCenThreads, sizeof(CenSmem), s, cen, cen_stride, n, ctl, keys,
+                   epoch, sort_chunk_tiles(n), sort_scratch, sort_chunk_sums(sort_scratch, n));
 }
 
 cudaError_t morton_init() {

@@ -321,6 +321,7 @@ __global__ void __launch_bounds__(T) k_tile_hist(const uint32_t *__restrict__ ke
     constexpr int D = 1 << BITS, P = D / T;
     __shared__ __align__(16) uint32_t h[D];
     const int tid = threadIdx.x, shift = pass * BITS;
+    chain_wait();
     const uint32_t tiles = sort_tiles(n);
     uint32_t acc[P];
 #pragma unroll
@@ -388,6 +389,7 @@ __global__ void __launch_bounds__(kScanThreads) k_chunk_scan(const uint32_t *__r
     __shared__ uint32_t s_wsum[SW];
     __shared__ uint32_t s_base[32];
     __shared__ uint32_t s_part[SW][32];
+    chain_wait();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // digit starts: exclusive scan of the global counts, one digit per thread
     uint32_t g = 0;
@@ -438,6 +440,7 @@ __global__ void __launch_bounds__(T, 4) k_scatter(const uint32_t *__restrict__ k
     // each warp clears its own counts: the ranking below touches only those, so the warp starts it
     // without waiting for the block (a block barrier there cost about 1 us of the three passes)
     for (int i = lane; i < D / 2; i += 32) reinterpret_cast<uint32_t *>(&S.whist[warp][0])[i] = 0;
+    chain_wait();
     const uint32_t tile = blockIdx.x, tile_base = tile * (uint32_t)kSortTile;
     const int shift = pass * BITS;
     const uint32_t wbase = tile_base + warp * (IPT * 32);
@@ -592,11 +595,12 @@ void launch_sort_pass(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t
     uint32_t *chunk_off = chunk_sum + (size_t)chunks * kDigits;
     const uint32_t ct = sort_chunk_tiles(n);
     uint32_t *ghist = &ctl->hist_part[pass][0][0];
+    const bool chain = chain_build(n);
     if (!counted)
-        k_tile_hist<kDigitBits><<<chunks, T, 0, s>>>(keys_in, n, pass, ct, tile_hist, chunk_sum, ghist);
-    k_chunk_scan<kDigitBits><<<kDigits / 32, kScanThreads, 0, s>>>(chunk_sum, chunks, ghist, chunk_off);
-    k_scatter<kDigitBits><<<tiles, T, sizeof(SortSmem<kDigitBits>), s>>>(
-        keys_in, vals_in, keys_out, vals_out, n, pass, tile_hist, chunk_off, ct, ctl);
+        launch_chained(chain, k_tile_hist<kDigitBits>, chunks, T, 0, s, keys_in, n, pass, ct, tile_hist, chunk_sum, ghist);
+    launch_chained(chain, k_chunk_scan<kDigitBits>, kDigits / 32, kScanThreads, 0, s, chunk_sum, chunks, ghist, chunk_off);
+    launch_chained(chain, k_scatter<kDigitBits>, tiles, T, sizeof(SortSmem<kDigitBits>), s, keys_in, vals_in, keys_out,
+                   vals_out, n, pass, tile_hist, chunk_off, ct, ctl);
 }
 
 void launch_onesweep32(const uint32_t *keys_in, const uint32_t *vals_in, uint32_t *keys_out,
