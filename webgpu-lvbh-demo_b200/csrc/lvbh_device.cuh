@@ -79,15 +79,15 @@ __device__ __forceinline__ bool finite3(float4 v) {
 __device__ __forceinline__ void fence_acq_rel_cta() { asm volatile("fence.acq_rel.cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
-// Programmatic dependent launch.  A kernel launched by launch_chained may become resident
-// while the kernel before it on the stream is still finishing; chain_wait blocks until that
-// kernel has completed and its memory is visible (and so, transitively, every earlier one),
-// then lets this kernel's own chained successor start launching.  Every chained kernel calls
-// it before its first access to global memory.  Launched the ordinary way it returns at once.
-__device__ __forceinline__ void chain_wait() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
+// Programmatic dependent launch.  A kernel launched by launch_chained starts launching once
+// every block of the kernel before it on the stream has exited, before that kernel's
+// completion is flushed; chain_wait blocks until the kernel before has completed and its
+// memory is visible (and so, transitively, every earlier one).  Every chained kernel calls it
+// before its first access to global memory.  Launched the ordinary way it returns at once.
+// No kernel signals its dependents early (griddepcontrol.launch_dependents at its start): the
+// waiting blocks that let in cost more than the launch they hid (a 2^20-triangle build 0.235
+// -> 0.250 ms, against 0.232 ms without the early signal).
+__device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // Shared-memory atomic OR with acquire-release semantics at CTA scope: the caller's earlier
 // writes are visible to a thread that later sees its bit, and what the caller reads after it

@@ -118,9 +118,9 @@ struct BatchPlan {
 int sm_count();
 
 // Launches a kernel that begins with chain_wait().  Chained (programmatic stream
-// serialisation), it may become resident while the kernel before it on the stream drains,
-// which saves the launch gap and the ramp-up at each kernel boundary of a build; otherwise it
-// launches in plain stream order.
+// serialisation), its launch overlaps the completion of the kernel before it on the stream,
+// which saves most of the launch gap at each kernel boundary of a build; otherwise it launches
+// in plain stream order.
 template <typename... P, typename... A>
 cudaError_t launch_chained(bool chain, void (*kernel)(P...), dim3 grid, dim3 block, size_t smem,
                            cudaStream_t s, A &&...args) {
@@ -138,10 +138,11 @@ cudaError_t launch_chained(bool chain, void (*kernel)(P...), dim3 grid, dim3 blo
 }
 
 // Whether a one-mesh build of n triangles chains its kernels.  Measured on B200: 4,096 meshes of
-// 64 to 262,144 triangles built one launch sequence each took 383 ms chained against 451 ms;
-// graph-replayed builds up to 2^18 triangles took the same time either way, and from 2^20 on
-// longer chained (0.235 -> 0.250 ms at 2^20, 1.704 -> 1.718 ms at 2^24 triangles).
-constexpr uint32_t kChainMaxTris = 1u << 18;
+// 64 to 262,144 triangles built one launch sequence each took 373 ms chained against 451 ms;
+// graph-replayed builds of clustered triangles took the same time either way up to 2^18 and at
+// 2^21 to 2^23, less chained at 2^20 (0.237 -> 0.232 ms) and a little more at 2^24 (1.7035 ->
+// 1.7066 ms, within the run-to-run spread), so the 16.7 M build keeps plain stream order.
+constexpr uint32_t kChainMaxTris = 1u << 22;
 inline bool chain_build(uint32_t n) { return n <= kChainMaxTris; }
 
 // Server support (api.cu): size a context's scratch for batched builds of up to max_tris
