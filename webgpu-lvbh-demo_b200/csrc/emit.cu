@@ -755,12 +755,22 @@ __global__ void __launch_bounds__(kGroupThreads) k_top_group(Groups groups, cons
         }
         return;
     }
-    for (int b = blk0; b < blk1; ++b) {
-        const int c = S.bstart[b - blk0 + 1] - S.bstart[b - blk0];
-        for (int k = t; k < c; k += kGroupThreads) {
-            const int at = S.bstart[b - blk0] + k;
-            S.it[at] = items[(size_t)b * kOpenCap + k];
-        }
+    // The group's items into shared memory: item `at` of the group is item at - bstart[b] of
+    // block blk0 + b.  Each thread holds at most two, and issues both loads before storing
+    // either (a loop over the blocks waited for one load per block in turn).
+    static_assert(kGroupCap <= 2 * kGroupThreads, "at most two items per thread");
+    auto src = [&](int at) -> const OpenItem & {
+        int b = 0;
+        while (S.bstart[b + 1] <= at) ++b;  // bstart[GB] = total > at: ends at a non-empty block
+        return items[(size_t)(blk0 + b) * kOpenCap + (at - S.bstart[b])];
+    };
+    {
+        const int a0 = t, a1 = t + kGroupThreads;
+        OpenItem i0, i1;
+        if (a0 < total) i0 = src(a0);
+        if (a1 < total) i1 = src(a1);
+        if (a0 < total) S.it[a0] = i0;
+        if (a1 < total) S.it[a1] = i1;
     }
     auto push_out = [&](int i) {
         const int at = atomicAdd(&S.nout, 1);
