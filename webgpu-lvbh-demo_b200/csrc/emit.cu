@@ -51,7 +51,6 @@ namespace {
 // of the persistent grid.  The plain build uses LOG = 8; a batched build may pick LOG = 7.
 template <int LOG>
 struct TreeGeo {
-    static constexpr int kLog = LOG;
     static constexpr int EB = 1 << LOG;
     static constexpr int kCtasPerSm = LOG == 8 ? 4 : 8;
     static_assert(2 * LOG + 14 <= 32, "packed item ranges");

@@ -56,7 +56,6 @@ class RangeAlloc {
   public:
     void reset(size_t cap) {
         free_.clear();
-        cap_ = cap;
         used_ = peak_ = 0;
         if (cap) free_[0] = cap;
     }
@@ -92,13 +91,12 @@ class RangeAlloc {
         }
         free_[off] = bytes;
     }
-    size_t cap() const { return cap_; }
     size_t used() const { return used_; }
     size_t peak() const { return peak_; }
 
   private:
     std::map<size_t, size_t> free_;
-    size_t cap_ = 0, used_ = 0, peak_ = 0;
+    size_t used_ = 0, peak_ = 0;
 };
 
 // Byte layout of the results of `t` triangles: nodes, tris, parents, leaf_index, morton.
